@@ -1,0 +1,266 @@
+/*
+ * pdf.h — C ABI of the B200 projective-dynamics frictional-contact step loop.
+ *
+ * This is the drop-in boundary for the reference's step loop
+ * ("Projective Dynamics with Dry Frictional Contact", SIGGRAPH 2020 code).
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (0 = PDF_OK).  The reference interfaces that each entry point replaces are
+ * cited beside it (paths are relative to the reference project root).
+ *
+ * Ownership: host arrays passed in are copied during the call; the handle owns
+ * all device memory, one CUDA stream and (optionally) a captured CUDA graph.
+ * Threading: a handle is not thread-safe; drive one handle from one host
+ * thread, exactly like the reference's single-threaded main loop
+ * (src/main.cpp:86-114).
+ */
+#ifndef PDF_B200_H
+#define PDF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum pdf_status {
+  PDF_OK = 0,
+  PDF_INVALID_ARG = 1,       /* bad argument or malformed scene / JSON / OBJ */
+  PDF_CUDA_ERROR = 2,        /* a CUDA runtime call failed                  */
+  PDF_NOT_SPD = 3,           /* the global-step matrix is not positive definite */
+  PDF_CAPACITY_EXCEEDED = 4, /* a contact / candidate buffer would overflow  */
+  PDF_DEVICE_TIMEOUT = 5,    /* a bounded device-side wait ran out           */
+  PDF_NAN_DETECTED = 6,      /* non-finite value in inputs or state          */
+  PDF_IO_ERROR = 7,          /* file could not be opened / read              */
+  PDF_NO_DEVICE = 8          /* no usable CUDA device                        */
+};
+
+/* ---- obstacles (include/physics/Obstacle.hpp:64-95) -------------------- */
+enum pdf_obstacle_type {
+  PDF_OBSTACLE_SPHERE = 0,          /* StaticSphere   (src/physics/StaticSphere.cpp:35-47)   */
+  PDF_OBSTACLE_ROTATING_SPHERE = 1, /* RotatingSphere (src/physics/RotatingSphere.cpp:71-93) */
+  PDF_OBSTACLE_PLANE = 2,           /* StaticPlane    (src/physics/StaticPlane.cpp:57-73)    */
+  PDF_OBSTACLE_MESH = 3             /* StaticMesh     (src/physics/StaticMesh.cpp:33-56)     */
+};
+
+typedef struct pdf_obstacle {
+  int32_t type;                 /* pdf_obstacle_type                         */
+  int32_t material;             /* row/column of the friction table          */
+  double center[3];             /* spheres: centre ("Position")               */
+  double radius;                /* spheres: radius                            */
+  double axis[3];               /* rotating sphere: "Rotation Axe"            */
+  double angular_speed;         /* rotating sphere: "Radial Speed" (rad/s)    */
+  double rotation_start_time;   /* rotating sphere: "Rotation Start Time" (s) */
+  double point[3];              /* plane: "Point"                             */
+  double normal[3];             /* plane: "Normal"                            */
+  int32_t n_vertices;           /* mesh obstacle: vertex count                */
+  int32_t n_triangles;          /* mesh obstacle: triangle count              */
+  const double* vertices;       /* mesh obstacle: 3*n_vertices doubles        */
+  const int32_t* triangles;     /* mesh obstacle: 3*n_triangles indices       */
+  double threshold;             /* mesh obstacle: "Threshold"                 */
+} pdf_obstacle;
+
+/* ---- dynamic meshes (include/physics/PhysicMesh.hpp, PhysicParameters) -- */
+typedef struct pdf_mesh_desc {
+  int32_t vertex_offset;        /* first vertex of this mesh in the scene arrays */
+  int32_t n_vertices;
+  int32_t triangle_offset;      /* first triangle of this mesh                   */
+  int32_t n_triangles;          /* triangle indices are scene-global             */
+  double area_density;          /* "Area Density"  (kg/m^2)                      */
+  double bending;               /* "Bending"       (weight of the bending rows)  */
+  double stretching;            /* "Stretching"    (weight of the spring rows)   */
+  int32_t material;             /* "Material Identifier"                         */
+} pdf_mesh_desc;
+
+/* ---- scene (PhysicScene, include/physics/PhysicScene.hpp:38-324) ------- */
+typedef struct pdf_scene_desc {
+  int32_t n_vertices;
+  const double* rest_positions; /* 3N: rest state ("Obj filename")             */
+  const double* positions;      /* 3N: initial state, NULL = rest state         */
+  const double* velocities;     /* 3N: initial velocities, NULL = zero          */
+  int32_t n_triangles;
+  const int32_t* triangles;     /* 3T, scene-global vertex indices, CCW         */
+  int32_t n_meshes;
+  const pdf_mesh_desc* meshes;
+  /* Attachment constraints (src/physics/AttachmentConstraint.cpp:31-51).
+   * The reference has the constraint but no JSON key for it; the JSON reader
+   * here accepts the extension key "Attachments". */
+  int32_t n_pins;
+  const int32_t* pin_vertices;
+  const double* pin_positions;  /* 3*n_pins */
+  const double* pin_weights;    /* n_pins   */
+  int32_t n_obstacles;
+  const pdf_obstacle* obstacles;
+  int32_t n_materials;
+  const double* friction;       /* n_materials^2, row-major ("Friction coefficients") */
+} pdf_scene_desc;
+
+/* ---- parameters (SimulationParameters, include/simulation_building.hpp:34-45) */
+enum pdf_precision {
+  PDF_FP64 = 0,          /* plain FP64 local step and triangular solves        */
+  PDF_FP32_REFINE = 1    /* FP32 local step / solves + FP64-residual refinement */
+};
+enum pdf_warm_start {
+  PDF_WARM_NONE = 0,     /* cold start: v^0 = t_n (SimulationSpeed.cpp:62-76)  */
+  PDF_WARM_MLP = 1       /* learned per-contact warm start of the contact force */
+};
+
+typedef struct pdf_params {
+  double time_step;                 /* "Timestep"                               */
+  int32_t local_global_iterations;  /* "LocalGlobal" (cap when tolerance > 0)   */
+  int32_t self_collision;           /* "Self-collision"                         */
+  double self_collision_tolerance;  /* "Self-collision tolerance"               */
+  double gravity[3];                /* "Gravity"                                */
+  double air_damping;               /* "Air damping" (optional, default 0)      */
+  int32_t precision;                /* pdf_precision                             */
+  double residual_tolerance;        /* > 0: stop PD iterations once the mean
+                                       Alart-Curnier residual is below it       */
+  int32_t warm_start;               /* pdf_warm_start                            */
+  int32_t refine_max;               /* FP32 mode: max refinement sweeps / solve */
+  double refine_tolerance;          /* FP32 mode: relative FP64 residual target */
+  int32_t device;                   /* CUDA device ordinal                       */
+  int32_t contact_capacity;         /* 0 = automatic                             */
+  int32_t use_graph;                /* capture the iteration loop in a CUDA graph */
+} pdf_params;
+
+/* Fills p with the reference defaults (air damping 0, FP64, fixed iterations). */
+void pdf_params_default(pdf_params* p);
+
+/* ---- per-step report --------------------------------------------------- */
+typedef struct pdf_step_report {
+  int32_t n_contacts;               /* obstacle contacts of the last step       */
+  int32_t n_self_contacts;          /* self contacts of the last step           */
+  int32_t n_levels;                 /* self-contact Gauss-Seidel levels         */
+  int32_t iterations;               /* PD iterations run in the last step       */
+  double residual;                  /* mean AC norm after the last iteration    */
+  double residual_max;              /* max AC norm after the last iteration     */
+  double normal_residual;           /* mean |AC_N| (obstacle + self)            */
+  double tangential_residual;       /* mean |AC_T| (obstacle + self)            */
+  double time;                      /* simulated time after the step (s)        */
+  int32_t refine_sweeps;            /* FP32 mode: refinement sweeps, last step  */
+  double solve_residual;            /* FP32 mode: last relative FP64 residual   */
+} pdf_step_report;
+
+typedef struct pdf_stats {
+  /* cumulative device time (ms) per phase since creation, CUDA events */
+  double detection_ms, self_detection_ms, ordering_ms;
+  double rhs_ms, friction_ms, self_friction_ms, solve_ms, step_ms;
+  int64_t steps, iterations;
+  /* one-time set-up */
+  double setup_ms, factor_ms;
+  int64_t factor_nnz;               /* nnz(L) of the Cholesky factor            */
+  int32_t n_supernodes, n_levels;   /* supernodal elimination tree              */
+  int64_t lhs_nnz;                  /* nnz(M + dt^2 A^T A)                      */
+  int32_t n_constraint_rows;        /* rows(A)                                  */
+} pdf_stats;
+
+/* One contact, as the reference's CollisionInfo / SelfCollisionInfo plus
+ * the iterate's local force r and AC residual (SFE:350-423, 590-652). */
+typedef struct pdf_contact {
+  int32_t vertex;                   /* colliding vertex                          */
+  int32_t partner;                  /* self contact: paired vertex; else -1      */
+  int32_t face[3];                  /* self contact: triangle; else -1           */
+  double normal[3];
+  double speed[3];                  /* obstacle velocity at the contact point   */
+  double mu;
+  double force[3];                  /* local-frame contact force r (N, T1, T2)  */
+  double ac;                        /* Alart-Curnier norm of the last iteration */
+} pdf_contact;
+
+/* ---- opaque handles ---------------------------------------------------- */
+typedef struct pdf_handle pdf_handle;
+typedef struct pdf_scene pdf_scene;
+
+/* Scene JSON -> scene.  Replaces getSceneFromJSONDocument
+ * (include/scene_building.hpp:36-39, src/scene_building.cpp:49-75) together with
+ * getJSONDocumentFromFilename (src/jsonHelper.cpp:22-40) and read_obj
+ * (src/geometry/io.cpp:65-121).  OBJ coordinates pass through float like the
+ * reference's tinyobj reader.  Relative OBJ paths resolve against the JSON
+ * file's directory first, then the working directory.  On error *out is NULL
+ * and the message is available from pdf_global_error(). */
+int pdf_scene_load_json(const char* json_path, pdf_scene** out);
+/* Borrowed view of a loaded scene (valid until pdf_scene_free). */
+int pdf_scene_view(const pdf_scene* scene, pdf_scene_desc* out);
+void pdf_scene_free(pdf_scene* scene);
+
+/* Replaces getSimulationParametersFromJSONDocument
+ * (src/simulation_building.cpp:37-78).  Also returns "Frame number" and
+ * "Steps per frame" for the caller's loop (may be NULL). */
+int pdf_params_load_json(const char* json_path, pdf_params* out,
+                         int32_t* frame_number, int32_t* steps_per_frame);
+
+/* Replaces getSimulation(PhysicScene&, const SimulationParameters&)
+ * (src/simulation_building.cpp:80-98) and the constructors it runs
+ * (SimulationFrictionEstimation SFE:31-62, SimulationSpeed.cpp:29-60,
+ * SimulationBase.cpp:46-100): assembles A, the LHS M + dt^2 A^T A, its one-time
+ * Cholesky factor, and uploads everything to the device. */
+int pdf_create(const pdf_scene_desc* scene, const pdf_params* params,
+               pdf_handle** out);
+
+/* Replaces SimulationBase::step() (src/physics/SimulationBase.cpp:103-173),
+ * called nsteps times.  report may be NULL. */
+int pdf_step(pdf_handle* h, int32_t nsteps, pdf_step_report* report);
+
+/* State read-back / overwrite (PhysicScene::getGeneralizedPositions/Speeds,
+ * src/physics/PhysicScene.cpp:233-305).  3N doubles each, either may be NULL. */
+int pdf_get_state(pdf_handle* h, double* q, double* v);
+int pdf_set_state(pdf_handle* h, const double* q, const double* v);
+
+/* Device-resident state (no copies): pointers to the handle's FP64 q and v
+ * (3N each, vertex-major xyz) and the CUDA stream the handle launches on. */
+int pdf_device_state(pdf_handle* h, double** q_dev, double** v_dev,
+                     void** cuda_stream);
+
+/* Contacts of the last step; *n receives the count; out may be NULL to query. */
+int pdf_get_contacts(pdf_handle* h, pdf_contact* out, int32_t capacity,
+                     int32_t* n);
+int pdf_get_self_contacts(pdf_handle* h, pdf_contact* out, int32_t capacity,
+                          int32_t* n);
+/* Self-contact Gauss-Seidel levels (SFE:161-279): level_ptr[n_levels+1],
+ * order[n_self] (indices into pdf_get_self_contacts' order). */
+int pdf_get_self_levels(pdf_handle* h, int32_t* level_ptr, int32_t level_cap,
+                        int32_t* order, int32_t order_cap, int32_t* n_levels);
+
+/* Per-phase statistics; exportStats (SimulationBase.cpp:473-494, SFE:755-770)
+ * as a stats.txt-like text written to path. */
+int pdf_get_stats(pdf_handle* h, pdf_stats* out);
+int pdf_export_stats(pdf_handle* h, const char* path);
+
+/* Per-iteration mean AC residuals of the last step (n <= cap written). */
+int pdf_get_residual_history(pdf_handle* h, double* out, int32_t cap,
+                             int32_t* n);
+
+/* Last error message of this handle (never NULL). */
+const char* pdf_last_error(const pdf_handle* h);
+/* Last error of calls that have no handle (loading, create failures). */
+const char* pdf_global_error(void);
+
+void pdf_destroy(pdf_handle* h);
+
+/* ---- stand-alone detection kernels (bit-exact candidate sets) ---------- */
+/* Vertex-triangle candidates of one mesh: the set
+ * { (v, t) : AABB(t) intersects [x_v - 1.1 tol, x_v + 1.1 tol] } (closed
+ * boxes) that getMeshPotentialTriangleCollision computes with CGAL
+ * box_intersection_d (src/geometry/geometry_util.cpp:284-327), found with a GPU
+ * LBVH over triangles.  Output sorted by (vertex, triangle).  pairs: 2*cap
+ * int32.  Returns PDF_CAPACITY_EXCEEDED (and the true count in *n) if cap is
+ * too small. */
+int pdf_detect_candidates(const double* positions, int32_t n_vertices,
+                          const int32_t* triangles, int32_t n_triangles,
+                          double tolerance, int32_t* pairs, int32_t cap,
+                          int32_t* n, int32_t device);
+
+/* Self collisions of one mesh: candidates, closest-point filter
+ * (geometry_util.cpp:229-262, 506-616) and the greedy node-node pairing
+ * (geometry_util.cpp:94-219) in canonical (vertex, triangle) order.
+ * out: contacts with vertex, partner, face, normal filled. */
+int pdf_detect_self_collisions(const double* positions, int32_t n_vertices,
+                               const int32_t* triangles, int32_t n_triangles,
+                               double tolerance, pdf_contact* out, int32_t cap,
+                               int32_t* n, int32_t device);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PDF_B200_H */
