@@ -88,7 +88,7 @@ class pdf_step_report(C.Structure):
         ("residual", C.c_double), ("residual_max", C.c_double),
         ("normal_residual", C.c_double), ("tangential_residual", C.c_double),
         ("time", C.c_double), ("refine_sweeps", C.c_int32),
-        ("solve_residual", C.c_double),
+        ("solve_residual", C.c_double), ("device_ms", C.c_double),
     ]
 
 
@@ -102,7 +102,8 @@ class pdf_stats(C.Structure):
         ("setup_ms", C.c_double), ("factor_ms", C.c_double),
         ("factor_nnz", C.c_int64), ("n_supernodes", C.c_int32),
         ("n_levels", C.c_int32), ("lhs_nnz", C.c_int64),
-        ("n_constraint_rows", C.c_int32),
+        ("n_constraint_rows", C.c_int32), ("kernel_launches", C.c_int64),
+        ("factor_nnz_true", C.c_int64),
     ]
 
 

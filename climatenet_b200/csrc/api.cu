@@ -1,0 +1,866 @@
+// api.cu — the C ABI (include/pdf.h): handle creation, the step loop and
+// state / contact / statistics read-back.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+#include <fstream>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/pdf.h"
+#include "handle.hpp"
+
+using namespace pdfb;
+
+namespace {
+
+thread_local std::string g_error;
+
+struct CudaFail : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define CK(x)                                                                                  \
+  do {                                                                                         \
+    cudaError_t e_ = (x);                                                                      \
+    if (e_ != cudaSuccess)                                                                     \
+      throw CudaFail(std::string(#x) + ": " + cudaGetErrorString(e_));                         \
+  } while (0)
+
+template <typename T>
+T* dalloc(size_t n) {
+  T* p = nullptr;
+  if (n == 0) n = 1;
+  CK(cudaMalloc((void**)&p, n * sizeof(T)));
+  return p;
+}
+template <typename T>
+T* upload(const std::vector<T>& v) {
+  T* p = dalloc<T>(v.size());
+  if (!v.empty()) CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return p;
+}
+
+constexpr int kThreads = 256;
+inline int blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kThreads - 1) / kThreads); }
+constexpr int kStrideBlocks = 592;  // 4 x 148 SMs for grid-stride kernels
+
+int group_size(int len) {
+  int g = 4;
+  while (g < 32 && g < len) g <<= 1;
+  return g;
+}
+
+// Level-ordered task lists of the supernodal sweeps.
+void build_schedule(pdf_handle* h) {
+  const Factor& f = h->fac;
+  std::vector<std::vector<SweepTask>> fw(f.n_levels), bw(f.n_levels);
+  for (int s = 0; s < f.n_sn; ++s) {
+    const int ns = f.sn_ns[s], nr = f.sn_nr[s], L = f.sn_level[s];
+    const int gf = group_size(ns);
+    const int per_f = 32 / gf;
+    for (int r = 0; r < ns + nr; r += per_f) fw[L].push_back({s, r, std::min(per_f, ns + nr - r), gf});
+    const int gb = group_size(ns / 2 + nr);
+    const int per_b = 32 / gb;
+    for (int c = 0; c < ns; c += per_b) bw[L].push_back({s, c, std::min(per_b, ns - c), gb});
+  }
+  std::vector<SweepTask> fa, ba;
+  h->fwd_off.assign(1, 0);
+  h->bwd_off.assign(1, 0);
+  for (int L = 0; L < f.n_levels; ++L) {
+    fa.insert(fa.end(), fw[L].begin(), fw[L].end());
+    ba.insert(ba.end(), bw[L].begin(), bw[L].end());
+    h->fwd_off.push_back((int)fa.size());
+    h->bwd_off.push_back((int)ba.size());
+  }
+  h->d.fwd_tasks = upload(fa);
+  h->d.bwd_tasks = upload(ba);
+  std::vector<SnInfo> sn(f.n_sn);
+  for (int s = 0; s < f.n_sn; ++s) sn[s] = {f.sn_c0[s], f.sn_ns[s], f.sn_nr[s], 0, f.sn_woff[s], f.sn_roff[s]};
+  h->d.sn = upload(sn);
+  h->d.rows = upload(f.rows);
+  h->n_levels = f.n_levels;
+}
+
+void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
+  auto t0 = std::chrono::steady_clock::now();
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw std::domain_error("no CUDA device");
+  if (p->device < 0 || p->device >= ndev) throw std::invalid_argument("device ordinal out of range");
+  CK(cudaSetDevice(p->device));
+  h->prm = *p;
+  h->fp32 = p->precision == PDF_FP32_REFINE;
+  if (p->precision != PDF_FP64 && p->precision != PDF_FP32_REFINE) throw std::invalid_argument("unknown precision mode");
+  if (sc->n_obstacles > kMaxObstacles) throw std::invalid_argument("at most 8 obstacles are supported");
+  build_model(*sc, *p, h->model);
+  const Model& m = h->model;
+  std::string ferr;
+  if (!factorize(m, p->time_step, 40, h->fac, ferr)) throw std::range_error(ferr);
+  const Factor& f = h->fac;
+  const int N = m.N;
+  CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  for (auto& e : h->ev) CK(cudaEventCreate(&e));
+  DeviceBuffers& d = h->d;
+  d.mass = upload(m.mass);
+  d.ring_ptr = upload(m.ring_ptr);
+  d.ring_idx = upload(m.ring_idx);
+  d.ring_kappa = upload(m.ring_kappa);
+  d.ring_bend = upload(m.ring_bend);
+  d.bend_of = upload(m.bend_of);
+  d.self_bend = upload(m.self_bend);
+  d.bend_ptr = upload(m.bend_ptr);
+  d.bend_idx = upload(m.bend_idx);
+  d.bend_coef = upload(m.bend_coef);
+  d.bend_w = upload(m.bend_w);
+  d.bend_rest = upload(m.bend_rest);
+  d.pin_term = m.has_pins ? upload(m.pin_term) : nullptr;
+  d.ata_ptr = upload(m.ata_ptr);
+  d.ata_col = upload(m.ata_col);
+  d.ata_val = upload(m.ata_val);
+  d.perm = upload(f.perm);
+  d.iperm = upload(f.iperm);
+  std::vector<int> vmat(N);
+  for (int i = 0; i < N; ++i) vmat[i] = m.meshes[m.vmesh[i]].material;
+  d.vmat = upload(vmat);
+  d.friction = upload(m.friction);
+  d.tris = upload(m.tris);
+  DModel& dm = h->dm;
+  dm.N = N;
+  dm.B = (int)m.bend_w.size();
+  dm.mass = d.mass;
+  dm.ring_ptr = d.ring_ptr;
+  dm.ring_idx = d.ring_idx;
+  dm.ring_kappa = d.ring_kappa;
+  dm.ring_bend = d.ring_bend;
+  dm.bend_of = d.bend_of;
+  dm.self_bend = d.self_bend;
+  dm.bend_ptr = d.bend_ptr;
+  dm.bend_idx = d.bend_idx;
+  dm.bend_coef = d.bend_coef;
+  dm.bend_w = d.bend_w;
+  dm.bend_rest = d.bend_rest;
+  dm.pin_term = d.pin_term;
+  dm.ata_ptr = d.ata_ptr;
+  dm.ata_col = d.ata_col;
+  dm.ata_val = d.ata_val;
+  dm.perm = d.perm;
+  dm.iperm = d.iperm;
+  // obstacles
+  h->obs.n = (int)m.obstacles.size();
+  for (int k = 0; k < h->obs.n; ++k) {
+    const pdf_obstacle& o = m.obstacles[k];
+    DObstacle& ob = h->obs.o[k];
+    ob = DObstacle{};
+    ob.type = o.type;
+    ob.material = o.material;
+    for (int c = 0; c < 3; ++c) {
+      ob.c[c] = o.center[c];
+      ob.p[c] = o.point[c];
+    }
+    ob.R = o.radius;
+    // RotatingSphere ctor (RotatingSphere.cpp:29-37): omega * axis.normalized()
+    double ax = o.axis[0], ay = o.axis[1], az = o.axis[2];
+    double an2 = ax * ax + ay * ay + az * az;
+    if (an2 > 0) {
+      double an = std::sqrt(an2);
+      ax /= an;
+      ay /= an;
+      az /= an;
+    }
+    ob.rot[0] = o.angular_speed * ax;
+    ob.rot[1] = o.angular_speed * ay;
+    ob.rot[2] = o.angular_speed * az;
+    // StaticPlane ctor normalises the normal (StaticPlane.cpp:46-53)
+    double nx = o.normal[0], ny = o.normal[1], nz = o.normal[2];
+    double nn2 = nx * nx + ny * ny + nz * nz;
+    if (nn2 > 0) {
+      double nn = std::sqrt(nn2);
+      nx /= nn;
+      ny /= nn;
+      nz /= nn;
+    }
+    ob.n[0] = nx;
+    ob.n[1] = ny;
+    ob.n[2] = nz;
+    // StaticMesh keeps tol^2 and passes sqrt(tol^2) (StaticMesh.cpp:25-31)
+    ob.tol = std::sqrt(o.threshold * o.threshold);
+    if (o.type == PDF_OBSTACLE_MESH) {
+      d.obstacle_v.push_back(upload(m.obstacle_vertices[k]));
+      d.obstacle_t.push_back(upload(m.obstacle_triangles[k]));
+      ob.mv = d.obstacle_v.back();
+      ob.mt = d.obstacle_t.back();
+      ob.n_tri = (int)m.obstacle_triangles[k].size() / 3;
+    }
+    h->host_time_before_start.push_back(o.rotation_start_time);
+  }
+  // state
+  d.q = upload(m.q0);
+  d.v = upload(m.v0);
+  d.tn = dalloc<double>(3 * (size_t)N);
+  d.qk = upload(m.q0);
+  d.cstep = dalloc<double>(3 * (size_t)N);
+  d.bp = dalloc<double>(3 * (size_t)std::max(1, dm.B));
+  // solve
+  build_schedule(h);
+  if (h->fp32) {
+    std::vector<float> w(f.Wr.begin(), f.Wr.end());
+    d.Wr32 = upload(w);
+    std::vector<float> wc(f.Wc.begin(), f.Wc.end());
+    d.Wc32 = upload(wc);
+    d.b32 = dalloc<float>(3 * (size_t)N);
+    d.y32 = dalloc<float>(3 * (size_t)N);
+    d.x32 = dalloc<float>(3 * (size_t)N);
+  } else {
+    d.Wr64 = upload(f.Wr);
+    d.Wc64 = upload(f.Wc);
+    d.b64 = dalloc<double>(3 * (size_t)N);
+    d.y64 = dalloc<double>(3 * (size_t)N);
+    d.x64 = dalloc<double>(3 * (size_t)N);
+  }
+  // contacts
+  const int nobs = std::max(1, h->obs.n);
+  h->cap_contacts = p->contact_capacity > 0 ? p->contact_capacity : nobs * N;
+  h->cap_self = p->contact_capacity > 0 ? p->contact_capacity : 2 * N;
+  DContacts& c = d.c;
+  c.cap = h->cap_contacts;
+  c.slot_cap = N;
+  c.self_cap = h->cap_self;
+  c.n_contacts = dalloc<int>(1);
+  c.n_self = dalloc<int>(1);
+  c.n_levels = dalloc<int>(1);
+  c.n_slots = dalloc<int>(1);
+  CK(cudaMemset(c.n_contacts, 0, sizeof(int)));
+  CK(cudaMemset(c.n_self, 0, sizeof(int)));
+  CK(cudaMemset(c.n_levels, 0, sizeof(int)));
+  CK(cudaMemset(c.n_slots, 0, sizeof(int)));
+  const size_t cc = h->cap_contacts, cs = h->cap_self;
+  c.c_vertex = dalloc<int>(cc);
+  c.c_normal = dalloc<double>(3 * cc);
+  c.c_speed = dalloc<double>(3 * cc);
+  c.c_mu = dalloc<double>(cc);
+  c.c_basis = dalloc<double>(9 * cc);
+  c.c_force = dalloc<double>(3 * cc);
+  CK(cudaMemset(c.c_force, 0, 3 * cc * sizeof(double)));
+  c.c_ac = dalloc<double>(cc);
+  c.c_slot = dalloc<int>(cc);
+  c.s_vertex = dalloc<int>(cs);
+  c.s_partner = dalloc<int>(cs);
+  c.s_face = dalloc<int>(3 * cs);
+  c.s_normal = dalloc<double>(3 * cs);
+  c.s_mu = dalloc<double>(cs);
+  c.s_basis = dalloc<double>(9 * cs);
+  c.s_force = dalloc<double>(3 * cs);
+  CK(cudaMemset(c.s_force, 0, 3 * cs * sizeof(double)));
+  c.s_ac = dalloc<double>(cs);
+  c.s_slota = dalloc<int>(cs);
+  c.s_slotb = dalloc<int>(cs);
+  c.s_remember = dalloc<double>(3 * cs);
+  c.level_ptr = dalloc<int>(cs + 2);
+  c.level_order = dalloc<int>(cs);
+  c.slot_of = dalloc<int>(N);
+  CK(cudaMemset(c.slot_of, 0xff, N * sizeof(int)));
+  c.slot_vertex = dalloc<int>(N);
+  c.f = dalloc<double>(3 * (size_t)N);
+  for (int k = 0; k < 2; ++k) {
+    c.cf[k] = dalloc<double>(3 * (size_t)N);
+    c.sf[k] = dalloc<double>(3 * (size_t)N);
+    CK(cudaMemset(c.cf[k], 0, 3 * (size_t)N * sizeof(double)));
+    CK(cudaMemset(c.sf[k], 0, 3 * (size_t)N * sizeof(double)));
+  }
+  d.newf = dalloc<double>(3 * cs);
+  d.ac_hist = dalloc<double>(4 * (size_t)p->local_global_iterations);
+  if (h->obs.n > 0) {
+    const int nitems = h->obs.n * N;
+    d.flags = dalloc<unsigned char>(nitems);
+    d.sel_idx = dalloc<int>(nitems);
+    thrust::counting_iterator<int> it(0);
+    CK(cub::DeviceSelect::Flagged(nullptr, d.cub_tmp_bytes, it, d.flags, d.sel_idx, c.n_contacts, nitems,
+                                  h->stream));
+    d.cub_tmp = dalloc<char>(d.cub_tmp_bytes);
+  }
+  if (p->self_collision) {
+    int st = self_detect_init(h);
+    if (st != PDF_OK) throw CudaFail("self-collision workspace: " + h->err);
+  }
+  CK(cudaDeviceSynchronize());
+  h->stats.factor_ms = f.factor_ms;
+  h->stats.factor_nnz = f.nnz_w;
+  h->stats.factor_nnz_true = f.nnz_l_true;
+  h->stats.n_supernodes = f.n_sn;
+  h->stats.n_levels = f.n_levels;
+  h->stats.lhs_nnz = (int64_t)m.ata_col.size();
+  h->stats.n_constraint_rows = m.n_rows;
+  h->stats.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// One PD iteration (SimulationBase.cpp:119-157): local step + friction
+// (SFE::computeRhs), global solve (SimulationSpeed::solve), AC residual.
+template <typename T>
+void launch_iteration(pdf_handle* h, int k, T* b, T* y, T* x, const T* Wr, const T* Wc, int mode) {
+  DeviceBuffers& d = h->d;
+  const DModel& dm = h->dm;
+  cudaStream_t st = h->stream;
+  const double dt = h->prm.time_step;
+  const int self_mode = h->prm.self_collision ? 1 : 0;
+  const int cur = k & 1, nxt = 1 - cur;
+  if (dm.B > 0) k_bend_proj<<<blocks_for(dm.B), kThreads, 0, st>>>(dm, d.qk, d.bp);
+  k_vertex_rhs<T><<<blocks_for(dm.N), kThreads, 0, st>>>(dm, d.qk, d.v, d.cstep, d.bp,
+                                                          std::max(h->prm.air_damping, 0.), d.c.slot_of, d.c.f, b,
+                                                          dt, mode);
+  k_friction_obstacle<T><<<kStrideBlocks, kThreads, 0, st>>>(dm, d.c, b, self_mode, cur, nxt);
+  if (self_mode) k_friction_self<T><<<1, 1024, 0, st>>>(dm, d.c, b, d.newf, cur, nxt);
+  for (int L = 0; L < h->n_levels; ++L) {
+    const int nt = h->fwd_off[L + 1] - h->fwd_off[L];
+    if (nt == 0) continue;
+    k_sweep_forward<T><<<(nt + 7) / 8, 256, 0, st>>>(d.fwd_tasks + h->fwd_off[L], nt, d.sn, d.rows, Wr, b, y);
+  }
+  for (int L = h->n_levels - 1; L >= 0; --L) {
+    const int nt = h->bwd_off[L + 1] - h->bwd_off[L];
+    if (nt == 0) continue;
+    k_sweep_backward<T><<<(nt + 7) / 8, 256, 0, st>>>(d.bwd_tasks + h->bwd_off[L], nt, d.sn, d.rows, Wc, y, x,
+                                                       d.perm, d.v, d.qk, d.q, dt, mode);
+  }
+  k_alart_curnier<<<kStrideBlocks, kThreads, 0, st>>>(d.c, d.v, d.ac_hist + 4 * (size_t)k);
+}
+
+// Kernels of this library launched by one PD iteration (CUB's not counted).
+int64_t launches_per_iteration(const pdf_handle* h) {
+  int64_t n = 3 + (h->dm.B > 0 ? 1 : 0) + (h->prm.self_collision ? 1 : 0);
+  for (int L = 0; L < h->n_levels; ++L) {
+    n += (h->fwd_off[L + 1] > h->fwd_off[L]) ? 1 : 0;
+    n += (h->bwd_off[L + 1] > h->bwd_off[L]) ? 1 : 0;
+  }
+  return n;
+}
+
+// Per step outside the iterations: predictor, obstacle flags + materialise,
+// slots (2), slot reset, finalize; self-collision: register reset, per mesh
+// bbox/keys/build/refit/traverse/pair, bases, levels.
+int64_t launches_per_step_extra(const pdf_handle* h) {
+  int64_t n = 1 + (h->obs.n > 0 ? 2 : 0) + 2 + 1 + 1;
+  if (h->prm.self_collision) n += 1 + 6 * (int64_t)h->model.meshes.size() + 1 + 1;
+  return n;
+}
+
+void launch_iterations(pdf_handle* h, int k0, int k1) {
+  DeviceBuffers& d = h->d;
+  for (int k = k0; k < k1; ++k) {
+    if (h->fp32)
+      launch_iteration<float>(h, k, d.b32, d.y32, d.x32, d.Wr32, d.Wc32, 1);
+    else
+      launch_iteration<double>(h, k, d.b64, d.y64, d.x64, d.Wr64, d.Wc64, 0);
+  }
+}
+
+void step_once(pdf_handle* h, bool want_report) {
+  DeviceBuffers& d = h->d;
+  const DModel& dm = h->dm;
+  cudaStream_t st = h->stream;
+  const double dt = h->prm.time_step;
+  const int N = dm.N;
+  const int K = h->prm.local_global_iterations;
+  CK(cudaEventRecord(h->ev[0], st));
+  k_step_init<<<blocks_for(N), kThreads, 0, st>>>(dm, d.q, d.v, d.tn, d.qk, d.cstep, h->prm.gravity[0],
+                                                  h->prm.gravity[1], h->prm.gravity[2], dt);
+  // obstacle detection on the start-of-step positions (SimulationBase.cpp:333-366)
+  if (h->obs.n > 0) {
+    for (int k = 0; k < h->obs.n; ++k) h->obs.o[k].time_before_start = h->host_time_before_start[k];
+    k_obstacle_flags<<<blocks_for(N), kThreads, 0, st>>>(N, d.q, h->obs, d.flags);
+    thrust::counting_iterator<int> it(0);
+    CK(cub::DeviceSelect::Flagged(d.cub_tmp, d.cub_tmp_bytes, it, d.flags, d.sel_idx, d.c.n_contacts,
+                                  h->obs.n * N, st));
+    k_obstacle_materialize<<<kStrideBlocks, kThreads, 0, st>>>(N, d.q, h->obs, d.sel_idx, d.vmat, d.friction,
+                                                               h->model.n_materials, d.c);
+  } else {
+    CK(cudaMemsetAsync(d.c.n_contacts, 0, sizeof(int), st));
+  }
+  CK(cudaEventRecord(h->ev[1], st));
+  if (h->prm.self_collision) {
+    int sst = self_detect_step(h);
+    if (sst != PDF_OK) throw std::overflow_error(h->err);
+  } else {
+    CK(cudaMemsetAsync(d.c.n_self, 0, sizeof(int), st));
+    CK(cudaMemsetAsync(d.c.n_levels, 0, sizeof(int), st));
+  }
+  // compact slots of every vertex touched by a contact (force buffers of SFE:45-60)
+  k_contact_slots<<<kStrideBlocks, kThreads, 0, st>>>(d.c);
+  k_contact_slots_fill<<<kStrideBlocks, kThreads, 0, st>>>(d.c);
+  if (h->prm.self_collision) self_levels_step(h);
+  CK(cudaEventRecord(h->ev[2], st));
+  CK(cudaMemsetAsync(d.ac_hist, 0, 4 * (size_t)K * sizeof(double), st));
+  // iterations
+  if (h->prm.use_graph) {
+    if (!h->graph) {
+      cudaGraph_t g;
+      CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      launch_iterations(h, 0, K);
+      CK(cudaStreamEndCapture(st, &g));
+      CK(cudaGraphInstantiate(&h->graph, g, 0));
+      CK(cudaGraphDestroy(g));
+    }
+    CK(cudaGraphLaunch(h->graph, st));
+  } else {
+    launch_iterations(h, 0, K);
+  }
+  CK(cudaEventRecord(h->ev[3], st));
+  k_contact_slots_reset<<<kStrideBlocks, kThreads, 0, st>>>(d.c);
+  CK(cudaMemsetAsync(d.c.n_slots, 0, sizeof(int), st));
+  k_finalize<<<blocks_for(3 * (int64_t)N), kThreads, 0, st>>>(3 * N, d.qk, d.q);
+  CK(cudaEventRecord(h->ev[4], st));
+  CK(cudaGetLastError());
+  // RotatingSphere::update (RotatingSphere.cpp:39-43)
+  for (auto& t : h->host_time_before_start) t -= dt;
+  h->time += dt;
+  h->stats.steps += 1;
+  h->stats.iterations += K;
+  h->stats.kernel_launches += launches_per_step_extra(h) + K * launches_per_iteration(h);
+  if (want_report) {
+    CK(cudaStreamSynchronize(st));
+    float a, b, cc, dd;
+    CK(cudaEventElapsedTime(&a, h->ev[0], h->ev[1]));
+    CK(cudaEventElapsedTime(&b, h->ev[1], h->ev[2]));
+    CK(cudaEventElapsedTime(&cc, h->ev[2], h->ev[3]));
+    CK(cudaEventElapsedTime(&dd, h->ev[0], h->ev[4]));
+    h->stats.detection_ms += a;
+    h->stats.self_detection_ms += b;
+    h->stats.solve_ms += cc;
+    h->stats.step_ms += dd;
+    int counts[3];
+    CK(cudaMemcpy(&counts[0], d.c.n_contacts, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&counts[1], d.c.n_self, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&counts[2], d.c.n_levels, sizeof(int), cudaMemcpyDeviceToHost));
+    std::vector<double> hist(4 * (size_t)K);
+    CK(cudaMemcpy(hist.data(), d.ac_hist, hist.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    const int nc = counts[0] + counts[1];
+    h->residual_hist.resize(K);
+    for (int k = 0; k < K; ++k) h->residual_hist[k] = nc ? hist[4 * k] / nc : 0.;
+    pdf_step_report& r = h->last;
+    r.n_contacts = counts[0];
+    r.n_self_contacts = counts[1];
+    r.n_levels = counts[2];
+    r.iterations = K;
+    r.residual = nc ? hist[4 * (K - 1)] / nc : 0.;
+    r.residual_max = hist[4 * (K - 1) + 1];
+    r.normal_residual = nc ? hist[4 * (K - 1) + 2] / nc : 0.;
+    r.tangential_residual = nc ? hist[4 * (K - 1) + 3] / nc : 0.;
+    r.time = h->time;
+  }
+}
+
+int fail(pdf_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  g_error = msg;
+  return code;
+}
+
+template <typename F>
+int guarded(pdf_handle* h, F&& fn) {
+  try {
+    return fn();
+  } catch (const CudaFail& e) {
+    return fail(h, PDF_CUDA_ERROR, e.what());
+  } catch (const std::overflow_error& e) {
+    return fail(h, PDF_CAPACITY_EXCEEDED, e.what());
+  } catch (const std::range_error& e) {
+    return fail(h, PDF_NOT_SPD, e.what());
+  } catch (const std::domain_error& e) {
+    return fail(h, PDF_NO_DEVICE, e.what());
+  } catch (const std::invalid_argument& e) {
+    return fail(h, PDF_INVALID_ARG, e.what());
+  } catch (const std::runtime_error& e) {
+    return fail(h, PDF_CUDA_ERROR, e.what());
+  } catch (const std::exception& e) {
+    return fail(h, PDF_INVALID_ARG, e.what());
+  }
+}
+
+void free_handle(pdf_handle* h) {
+  if (!h) return;
+  cudaSetDevice(h->prm.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  self_detect_free(h);
+  DeviceBuffers& d = h->d;
+  void* ptrs[] = {d.mass, d.ring_kappa, d.ring_bend, d.self_bend, d.ring_ptr, d.ring_idx, d.bend_of, d.bend_ptr,
+                  d.bend_idx, d.bend_coef, d.bend_w, d.bend_rest, d.pin_term, d.ata_ptr, d.ata_col, d.ata_val,
+                  d.perm, d.iperm, d.vmat, d.friction, d.tris, d.q, d.v, d.tn, d.qk, d.cstep, d.bp, d.fwd_tasks,
+                  d.bwd_tasks, d.sn, d.rows, d.Wr64, d.Wc64, d.Wr32, d.Wc32, d.b64, d.y64, d.x64, d.b32, d.y32,
+                  d.x32, d.flags, d.sel_idx, d.cub_tmp, d.newf, d.ac_hist, d.c.n_contacts, d.c.c_vertex,
+                  d.c.c_normal, d.c.c_speed, d.c.c_mu, d.c.c_basis, d.c.c_force, d.c.c_ac, d.c.c_slot, d.c.n_self,
+                  d.c.s_vertex, d.c.s_partner, d.c.s_face, d.c.s_normal, d.c.s_mu, d.c.s_basis, d.c.s_force,
+                  d.c.s_ac, d.c.s_slota, d.c.s_slotb, d.c.s_remember, d.c.n_levels, d.c.level_ptr,
+                  d.c.level_order, d.c.slot_of, d.c.n_slots, d.c.slot_vertex, d.c.f, d.c.cf[0], d.c.cf[1],
+                  d.c.sf[0], d.c.sf[1]};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (auto p : d.obstacle_v) cudaFree(p);
+  for (auto p : d.obstacle_t) cudaFree(p);
+  for (auto& e : h->ev)
+    if (e) cudaEventDestroy(e);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+void fill_contact(pdf_contact& o, int vertex, int partner, const int* face, const double* n, const double* sp,
+                  double mu, const double* f, double ac) {
+  o.vertex = vertex;
+  o.partner = partner;
+  for (int k = 0; k < 3; ++k) {
+    o.face[k] = face ? face[k] : -1;
+    o.normal[k] = n[k];
+    o.speed[k] = sp ? sp[k] : 0.;
+    o.force[k] = f[k];
+  }
+  o.mu = mu;
+  o.ac = ac;
+}
+
+}  // namespace
+
+namespace pdfb {
+void set_global_error(const std::string& msg) { g_error = msg; }
+}  // namespace pdfb
+
+extern "C" {
+
+void pdf_params_default(pdf_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->time_step = 1e-3;
+  p->local_global_iterations = 20;
+  p->gravity[2] = -9.81;
+  p->precision = PDF_FP64;
+  p->refine_max = 4;
+  p->refine_tolerance = 1e-10;
+  p->use_graph = 1;
+}
+
+const char* pdf_global_error(void) { return g_error.c_str(); }
+const char* pdf_last_error(const pdf_handle* h) { return h ? h->err.c_str() : g_error.c_str(); }
+
+int pdf_create(const pdf_scene_desc* scene, const pdf_params* params, pdf_handle** out) {
+  if (!out) return fail(nullptr, PDF_INVALID_ARG, "null output handle");
+  *out = nullptr;
+  if (!scene || !params) return fail(nullptr, PDF_INVALID_ARG, "null scene or parameters");
+  pdf_handle* h = new pdf_handle();
+  int st = guarded(h, [&] {
+    create_impl(h, scene, params);
+    return PDF_OK;
+  });
+  if (st != PDF_OK) {
+    g_error = h->err;
+    free_handle(h);
+    return st;
+  }
+  *out = h;
+  return PDF_OK;
+}
+
+int pdf_step(pdf_handle* h, int32_t nsteps, pdf_step_report* report) {
+  if (!h || nsteps < 0) return fail(h, PDF_INVALID_ARG, "invalid handle or step count");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    CK(cudaEventRecord(h->ev[5], h->stream));
+    for (int s = 0; s < nsteps; ++s) step_once(h, (s == nsteps - 1) || h->prm.self_collision);
+    CK(cudaEventRecord(h->ev[6], h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]));
+    h->last.device_ms = ms;
+    if (report) *report = h->last;
+    return PDF_OK;
+  });
+}
+
+int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms_out, double* bytes_out) {
+  if (!h || reps <= 0 || phase < 0 || phase > 3) return fail(h, PDF_INVALID_ARG, "invalid phase timing request");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    DeviceBuffers& d = h->d;
+    const DModel& dm = h->dm;
+    cudaStream_t st = h->stream;
+    const double dt = h->prm.time_step;
+    const Factor& f = h->fac;
+    const double s = h->fp32 ? 4. : 8.;
+    const double N = dm.N;
+    double bytes = 0;
+    int64_t idx_rows = (int64_t)f.rows.size();
+    if (phase == 0) {
+      // 2 [l s + idx_bytes(L)] + 2 (2 * 3 s N) + FP64 epilogue (q read; v, q^k written)
+      bytes = 2. * ((double)f.nnz_w * s + 4. * (double)idx_rows) + 2. * (2. * 3. * s * N) + 72. * N;
+    } else if (phase == 1) {
+      // 4*3sN + E (8 + s) + sum_b [(r_b + 1)(4 + s) + s], s = 8 (FP64 local step)
+      const double E = (double)h->model.ring_idx.size() / 2.;
+      double bsum = 0;
+      for (size_t b = 0; b + 1 < h->model.bend_ptr.size(); ++b)
+        bsum += (h->model.bend_ptr[b + 1] - h->model.bend_ptr[b]) * 12. + 8.;
+      bytes = 4. * 24. * N + E * 16. + bsum;
+    }
+    // phase 0 works on a saved right-hand side restored between repetitions
+    double* save64 = nullptr;
+    float* save32 = nullptr;
+    if (phase == 0) {
+      if (h->fp32) {
+        save32 = dalloc<float>(3 * (size_t)dm.N);
+        CK(cudaMemcpyAsync(save32, d.b32, 3 * (size_t)dm.N * sizeof(float), cudaMemcpyDeviceToDevice, st));
+      } else {
+        save64 = dalloc<double>(3 * (size_t)dm.N);
+        CK(cudaMemcpyAsync(save64, d.b64, 3 * (size_t)dm.N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      }
+    }
+    std::vector<double> vsave(3 * (size_t)dm.N), qsave(3 * (size_t)dm.N);
+    CK(cudaMemcpyAsync(vsave.data(), d.v, vsave.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(qsave.data(), d.qk, qsave.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    double total = 0;
+    for (int r = 0; r < reps; ++r) {
+      if (phase == 0) {
+        if (h->fp32)
+          CK(cudaMemcpyAsync(d.b32, save32, 3 * (size_t)dm.N * sizeof(float), cudaMemcpyDeviceToDevice, st));
+        else
+          CK(cudaMemcpyAsync(d.b64, save64, 3 * (size_t)dm.N * sizeof(double), cudaMemcpyDeviceToDevice, st));
+      }
+      CK(cudaEventRecord(h->ev[5], st));
+      if (phase == 0) {
+        for (int L = 0; L < h->n_levels; ++L) {
+          const int nt = h->fwd_off[L + 1] - h->fwd_off[L];
+          if (!nt) continue;
+          if (h->fp32)
+            k_sweep_forward<float><<<(nt + 7) / 8, 256, 0, st>>>(d.fwd_tasks + h->fwd_off[L], nt, d.sn, d.rows,
+                                                                 d.Wr32, d.b32, d.y32);
+          else
+            k_sweep_forward<double><<<(nt + 7) / 8, 256, 0, st>>>(d.fwd_tasks + h->fwd_off[L], nt, d.sn, d.rows,
+                                                                  d.Wr64, d.b64, d.y64);
+        }
+        for (int L = h->n_levels - 1; L >= 0; --L) {
+          const int nt = h->bwd_off[L + 1] - h->bwd_off[L];
+          if (!nt) continue;
+          if (h->fp32)
+            k_sweep_backward<float><<<(nt + 7) / 8, 256, 0, st>>>(d.bwd_tasks + h->bwd_off[L], nt, d.sn, d.rows,
+                                                                  d.Wc32, d.y32, d.x32, d.perm, d.v, d.qk, d.q,
+                                                                  dt, 1);
+          else
+            k_sweep_backward<double><<<(nt + 7) / 8, 256, 0, st>>>(d.bwd_tasks + h->bwd_off[L], nt, d.sn, d.rows,
+                                                                   d.Wc64, d.y64, d.x64, d.perm, d.v, d.qk, d.q,
+                                                                   dt, 0);
+        }
+      } else if (phase == 1) {
+        if (dm.B > 0) k_bend_proj<<<blocks_for(dm.B), kThreads, 0, st>>>(dm, d.qk, d.bp);
+        if (h->fp32)
+          k_vertex_rhs<float><<<blocks_for(dm.N), kThreads, 0, st>>>(dm, d.qk, d.v, d.cstep, d.bp,
+                                                                     std::max(h->prm.air_damping, 0.), d.c.slot_of,
+                                                                     d.c.f, d.b32, dt, 1);
+        else
+          k_vertex_rhs<double><<<blocks_for(dm.N), kThreads, 0, st>>>(dm, d.qk, d.v, d.cstep, d.bp,
+                                                                      std::max(h->prm.air_damping, 0.),
+                                                                      d.c.slot_of, d.c.f, d.b64, dt, 0);
+      } else if (phase == 2) {
+        if (h->fp32)
+          k_friction_obstacle<float><<<kStrideBlocks, kThreads, 0, st>>>(dm, d.c, d.b32, 0, 0, 1);
+        else
+          k_friction_obstacle<double><<<kStrideBlocks, kThreads, 0, st>>>(dm, d.c, d.b64, 0, 0, 1);
+      } else {
+        if (h->obs.n > 0) {
+          k_obstacle_flags<<<blocks_for(dm.N), kThreads, 0, st>>>(dm.N, d.q, h->obs, d.flags);
+          thrust::counting_iterator<int> it(0);
+          CK(cub::DeviceSelect::Flagged(d.cub_tmp, d.cub_tmp_bytes, it, d.flags, d.sel_idx, d.c.n_contacts,
+                                        h->obs.n * dm.N, st));
+        }
+        if (h->prm.self_collision) {
+          int sst = self_detect_step(h);
+          if (sst != PDF_OK) throw std::overflow_error(h->err);
+        }
+      }
+      CK(cudaEventRecord(h->ev[6], st));
+      CK(cudaEventSynchronize(h->ev[6]));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]));
+      total += ms;
+    }
+    CK(cudaMemcpyAsync(d.v, vsave.data(), vsave.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(d.qk, qsave.data(), qsave.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    if (save64) cudaFree(save64);
+    if (save32) cudaFree(save32);
+    if (ms_out) *ms_out = total / reps;
+    if (bytes_out) *bytes_out = bytes;
+    return PDF_OK;
+  });
+}
+
+int pdf_get_state(pdf_handle* h, double* q, double* v) {
+  if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
+  return guarded(h, [&]() -> int {
+    const size_t n = 3 * (size_t)h->dm.N * sizeof(double);
+    CK(cudaStreamSynchronize(h->stream));
+    if (q) CK(cudaMemcpy(q, h->d.q, n, cudaMemcpyDeviceToHost));
+    if (v) CK(cudaMemcpy(v, h->d.v, n, cudaMemcpyDeviceToHost));
+    return PDF_OK;
+  });
+}
+
+int pdf_set_state(pdf_handle* h, const double* q, const double* v) {
+  if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
+  return guarded(h, [&]() -> int {
+    const size_t n3 = 3 * (size_t)h->dm.N;
+    for (size_t i = 0; i < n3; ++i)
+      if ((q && !std::isfinite(q[i])) || (v && !std::isfinite(v[i])))
+        return fail(h, PDF_NAN_DETECTED, "non-finite value in the state passed to pdf_set_state");
+    CK(cudaStreamSynchronize(h->stream));
+    if (q) CK(cudaMemcpy(h->d.q, q, n3 * sizeof(double), cudaMemcpyHostToDevice));
+    if (v) CK(cudaMemcpy(h->d.v, v, n3 * sizeof(double), cudaMemcpyHostToDevice));
+    return PDF_OK;
+  });
+}
+
+int pdf_device_state(pdf_handle* h, double** q_dev, double** v_dev, void** stream) {
+  if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
+  if (q_dev) *q_dev = h->d.q;
+  if (v_dev) *v_dev = h->d.v;
+  if (stream) *stream = (void*)h->stream;
+  return PDF_OK;
+}
+
+int pdf_get_contacts(pdf_handle* h, pdf_contact* out, int32_t cap, int32_t* n) {
+  if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
+  return guarded(h, [&]() -> int {
+    CK(cudaStreamSynchronize(h->stream));
+    int C = 0;
+    CK(cudaMemcpy(&C, h->d.c.n_contacts, sizeof(int), cudaMemcpyDeviceToHost));
+    if (n) *n = C;
+    if (!out) return PDF_OK;
+    const int m = std::min(C, cap);
+    std::vector<int> vx(m);
+    std::vector<double> nr(3 * m), sp(3 * m), mu(m), fo(3 * m), ac(m);
+    const DContacts& c = h->d.c;
+    if (m > 0) {
+      CK(cudaMemcpy(vx.data(), c.c_vertex, m * sizeof(int), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(nr.data(), c.c_normal, 3 * m * sizeof(double), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(sp.data(), c.c_speed, 3 * m * sizeof(double), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(mu.data(), c.c_mu, m * sizeof(double), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(fo.data(), c.c_force, 3 * m * sizeof(double), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(ac.data(), c.c_ac, m * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    for (int k = 0; k < m; ++k)
+      fill_contact(out[k], vx[k], -1, nullptr, &nr[3 * k], &sp[3 * k], mu[k], &fo[3 * k], ac[k]);
+    return C > cap ? fail(h, PDF_CAPACITY_EXCEEDED, "contact buffer too small") : PDF_OK;
+  });
+}
+
+int pdf_get_self_contacts(pdf_handle* h, pdf_contact* out, int32_t cap, int32_t* n) {
+  if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
+  return guarded(h, [&]() -> int {
+    CK(cudaStreamSynchronize(h->stream));
+    int S = 0;
+    CK(cudaMemcpy(&S, h->d.c.n_self, sizeof(int), cudaMemcpyDeviceToHost));
+    if (n) *n = S;
+    if (!out) return PDF_OK;
+    const int m = std::min(S, cap);
+    std::vector<int> vx(m), pa(m), fa(3 * m);
+    std::vector<double> nr(3 * m), mu(m), fo(3 * m), ac(m);
+    const DContacts& c = h->d.c;
+    if (m > 0) {
+      CK(cudaMemcpy(vx.data(), c.s_vertex, m * sizeof(int), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(pa.data(), c.s_partner, m * sizeof(int), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(fa.data(), c.s_face, 3 * m * sizeof(int), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(nr.data(), c.s_normal, 3 * m * sizeof(double), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(mu.data(), c.s_mu, m * sizeof(double), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(fo.data(), c.s_force, 3 * m * sizeof(double), cudaMemcpyDeviceToHost));
+      CK(cudaMemcpy(ac.data(), c.s_ac, m * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+    for (int k = 0; k < m; ++k)
+      fill_contact(out[k], vx[k], pa[k], &fa[3 * k], &nr[3 * k], nullptr, mu[k], &fo[3 * k], ac[k]);
+    return S > cap ? fail(h, PDF_CAPACITY_EXCEEDED, "self-contact buffer too small") : PDF_OK;
+  });
+}
+
+int pdf_get_self_levels(pdf_handle* h, int32_t* level_ptr, int32_t level_cap, int32_t* order, int32_t order_cap,
+                        int32_t* n_levels) {
+  if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
+  return guarded(h, [&]() -> int {
+    CK(cudaStreamSynchronize(h->stream));
+    int nl = 0, S = 0;
+    CK(cudaMemcpy(&nl, h->d.c.n_levels, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&S, h->d.c.n_self, sizeof(int), cudaMemcpyDeviceToHost));
+    if (n_levels) *n_levels = nl;
+    if (level_ptr && level_cap > 0)
+      CK(cudaMemcpy(level_ptr, h->d.c.level_ptr, std::min(level_cap, nl + 1) * sizeof(int), cudaMemcpyDeviceToHost));
+    if (order && order_cap > 0 && S > 0)
+      CK(cudaMemcpy(order, h->d.c.level_order, std::min(order_cap, S) * sizeof(int), cudaMemcpyDeviceToHost));
+    return PDF_OK;
+  });
+}
+
+int pdf_get_stats(pdf_handle* h, pdf_stats* out) {
+  if (!h || !out) return fail(h, PDF_INVALID_ARG, "null argument");
+  *out = h->stats;
+  return PDF_OK;
+}
+
+int pdf_export_stats(pdf_handle* h, const char* path) {
+  if (!h || !path) return fail(h, PDF_INVALID_ARG, "null argument");
+  std::ofstream of(path);
+  if (!of) return fail(h, PDF_IO_ERROR, std::string("cannot open ") + path);
+  const pdf_stats& s = h->stats;
+  auto section = [&](const char* name, double value, int64_t number) {
+    of << name << "\n";
+    if (number == 0)
+      of << "\t(No data)\n";
+    else
+      of << "\t Number      : " << number << "\n\t Mean value  : " << value / (double)number << "\n";
+    of << "\n-------------------\n\n";
+  };
+  of << "LHS computation time (µs)\n\t Value : " << 1e3 * (s.setup_ms - s.factor_ms) << "\n\n-------------------\n\n";
+  of << "Cholesky computation time (µs)\n\t Value : " << 1e3 * s.factor_ms << "\n\n-------------------\n\n";
+  section("Collision detection time (µs)", 1e3 * s.detection_ms, s.steps);
+  section("Self collision detection time (µs)", 1e3 * s.self_detection_ms, s.steps);
+  section("Iteration time (µs)", 1e3 * s.solve_ms, s.iterations);
+  section("Step time (µs)", 1e3 * s.step_ms, s.steps);
+  return PDF_OK;
+}
+
+int pdf_get_residual_history(pdf_handle* h, double* out, int32_t cap, int32_t* n) {
+  if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
+  if (n) *n = (int)h->residual_hist.size();
+  if (out)
+    for (int i = 0; i < (int)h->residual_hist.size() && i < cap; ++i) out[i] = h->residual_hist[i];
+  return PDF_OK;
+}
+
+void pdf_destroy(pdf_handle* h) { free_handle(h); }
+
+int pdf_detect_candidates(const double* positions, int32_t n_vertices, const int32_t* triangles, int32_t n_triangles,
+                          double tolerance, int32_t* pairs, int32_t cap, int32_t* n, int32_t device) {
+  std::string err;
+  int st = PDF_OK;
+  try {
+    st = standalone_candidates(positions, n_vertices, triangles, n_triangles, tolerance, pairs, cap, n, device, err);
+  } catch (const std::exception& e) {
+    err = e.what();
+    st = PDF_CUDA_ERROR;
+  }
+  if (st != PDF_OK) g_error = err;
+  return st;
+}
+
+int pdf_detect_self_collisions(const double* positions, int32_t n_vertices, const int32_t* triangles,
+                               int32_t n_triangles, double tolerance, pdf_contact* out, int32_t cap, int32_t* n,
+                               int32_t device) {
+  std::string err;
+  int st = PDF_OK;
+  try {
+    st = standalone_self(positions, n_vertices, triangles, n_triangles, tolerance, out, cap, n, device, err);
+  } catch (const std::exception& e) {
+    err = e.what();
+    st = PDF_CUDA_ERROR;
+  }
+  if (st != PDF_OK) g_error = err;
+  return st;
+}
+
+}  // extern "C"

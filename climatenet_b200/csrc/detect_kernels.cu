@@ -1,0 +1,142 @@
+// detect_kernels.cu — obstacle detection and contact bookkeeping.
+// Compiled with --fmad=false so that every multiply and add rounds separately,
+// exactly like the reference compiled for plain x86-64: detection decisions
+// (inside / outside, closest-point region) must come out bit-identical.
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+#include "geometry.cuh"
+#include "kernels.hpp"
+
+namespace pdfb {
+
+// Per (obstacle, vertex) flag, obstacle-major so that a stable compaction gives
+// the reference's order (obstacles in scene order, vertices ascending:
+// PhysicScene::getCollisionsInfoExceptFor PhysicScene.cpp:115-181 and
+// Obstacle::checkCollision Obstacle.cpp:24-45).
+__global__ void k_obstacle_flags(int N, const double* __restrict__ q, DObstacles obs, unsigned char* __restrict__ flags) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N) return;
+  const double3 x = ld3(q, i);
+  for (int o = 0; o < obs.n; ++o) {
+    const DObstacle& ob = obs.o[o];
+    bool hit = false;
+    if (ob.type == 0 || ob.type == 1) {
+      // Sphere::isInside Sphere.cpp:93-98 (hard-coded 1 cm margin)
+      const double3 r = x - make_double3(ob.c[0], ob.c[1], ob.c[2]);
+      hit = sqrt(dot3(r, r)) < ob.R + 1e-2;
+    } else if (ob.type == 2) {
+      // StaticPlane::checkCollision StaticPlane.cpp:57-73 (hard-coded 1.5 cm)
+      const double d = dot3(x - make_double3(ob.p[0], ob.p[1], ob.p[2]), make_double3(ob.n[0], ob.n[1], ob.n[2]));
+      hit = d < 1.5e-2;
+    } else {
+      int tri;
+      double3 cp;
+      hit = mesh_obstacle_closest(x, ob.mv, ob.mt, ob.n_tri, ob.tol, &tri, &cp);
+    }
+    flags[(int64_t)o * N + i] = hit ? 1 : 0;
+  }
+}
+
+// contact basis, computeBasis SFE:91-105
+__device__ void write_basis(double* B, double3 n) {
+  double3 t = cross3(n, make_double3(1., 0., 0.));
+  if (sqrt(dot3(t, t)) < 1.e-15) t = cross3(n, make_double3(0., 1., 0.));
+  t = normalized3(t);
+  const double3 bt = normalized3(cross3(n, t));
+  B[0] = n.x;
+  B[1] = n.y;
+  B[2] = n.z;
+  B[3] = t.x;
+  B[4] = t.y;
+  B[5] = t.z;
+  B[6] = bt.x;
+  B[7] = bt.y;
+  B[8] = bt.z;
+}
+
+__global__ void k_obstacle_materialize(int N, const double* __restrict__ q, DObstacles obs, const int* __restrict__ idx,
+                                       const int* __restrict__ vmat, const double* __restrict__ friction, int n_mat,
+                                       DContacts c) {
+  const int C = *c.n_contacts;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C; k += gridDim.x * blockDim.x) {
+    const int o = idx[k] / N, i = idx[k] % N;
+    const DObstacle& ob = obs.o[o];
+    const double3 x = ld3(q, i);
+    double3 nrm, sp = make_double3(0., 0., 0.);
+    if (ob.type == 0 || ob.type == 1) {
+      // Sphere::project Sphere.cpp:104-113
+      const double3 ctr = make_double3(ob.c[0], ob.c[1], ob.c[2]);
+      nrm = normalized3(x - ctr);
+      const double3 cp = ctr + ob.R * nrm;
+      if (ob.type == 1 && ob.time_before_start < 0) {
+        // RotatingSphere::checkCollision RotatingSphere.cpp:71-93: omega x (p - c)
+        sp = cross3(make_double3(ob.rot[0], ob.rot[1], ob.rot[2]), cp - ctr);
+      }
+    } else if (ob.type == 2) {
+      nrm = make_double3(ob.n[0], ob.n[1], ob.n[2]);
+    } else {
+      int tri;
+      double3 cp;
+      mesh_obstacle_closest(x, ob.mv, ob.mt, ob.n_tri, ob.tol, &tri, &cp);
+      const double3 a = ld3(ob.mv, ob.mt[3 * tri]), b = ld3(ob.mv, ob.mt[3 * tri + 1]), cc = ld3(ob.mv, ob.mt[3 * tri + 2]);
+      nrm = normalized3(cross3(b - a, cc - a));  // Mesh::getTriangleNormal Mesh.cpp:120-126
+    }
+    c.c_vertex[k] = i;
+    st3(c.c_normal, k, nrm);
+    st3(c.c_speed, k, sp);
+    c.c_mu[k] = friction[(int64_t)vmat[i] * n_mat + ob.material];
+    write_basis(c.c_basis + 9 * (int64_t)k, nrm);
+  }
+}
+
+// Involved-vertex slots: every contact vertex, self-contact vertex and partner
+// gets a compact slot for the per-contact force buffers.
+__device__ __forceinline__ void claim_slot(DContacts& c, int v) {
+  if (atomicCAS(c.slot_of + v, -1, -2) == -1) {
+    const int s = atomicAdd(c.n_slots, 1);
+    if (s < c.slot_cap) {
+      c.slot_vertex[s] = v;
+      c.slot_of[v] = s;
+    }
+  }
+}
+
+__global__ void k_contact_slots(DContacts c) {
+  const int C = *c.n_contacts, S = *c.n_self;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C + S; k += gridDim.x * blockDim.x) {
+    if (k < C) {
+      claim_slot(c, c.c_vertex[k]);
+    } else {
+      claim_slot(c, c.s_vertex[k - C]);
+      claim_slot(c, c.s_partner[k - C]);
+    }
+  }
+}
+
+__global__ void k_contact_slots_fill(DContacts c) {
+  const int C = *c.n_contacts, S = *c.n_self;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C + S; k += gridDim.x * blockDim.x) {
+    if (k < C) {
+      c.c_slot[k] = c.slot_of[c.c_vertex[k]];
+    } else {
+      c.s_slota[k - C] = c.slot_of[c.s_vertex[k - C]];
+      c.s_slotb[k - C] = c.slot_of[c.s_partner[k - C]];
+      st3(c.s_remember, k - C, make_double3(0., 0., 0.));
+    }
+  }
+  const int ns = min(*c.n_slots, c.slot_cap);
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < 3 * ns; s += gridDim.x * blockDim.x) {
+    c.cf[0][s] = 0.;
+    c.cf[1][s] = 0.;
+    c.sf[0][s] = 0.;
+    c.sf[1][s] = 0.;
+  }
+}
+
+__global__ void k_contact_slots_reset(DContacts c) {
+  const int ns = min(*c.n_slots, c.slot_cap);
+  for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < ns; s += gridDim.x * blockDim.x) c.slot_of[c.slot_vertex[s]] = -1;
+}
+
+}  // namespace pdfb

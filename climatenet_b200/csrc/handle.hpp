@@ -1,0 +1,85 @@
+// handle.hpp — the state behind a pdf_handle (host orchestration of the
+// device step loop).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/pdf.h"
+#include "factor.hpp"
+#include "kernels.hpp"
+#include "model.hpp"
+
+namespace pdfb {
+
+struct DeviceBuffers {
+  // model tables
+  double *mass = nullptr, *ring_kappa = nullptr, *ring_bend = nullptr, *self_bend = nullptr;
+  int *ring_ptr = nullptr, *ring_idx = nullptr, *bend_of = nullptr, *bend_ptr = nullptr, *bend_idx = nullptr;
+  double *bend_coef = nullptr, *bend_w = nullptr, *bend_rest = nullptr, *pin_term = nullptr;
+  int *ata_ptr = nullptr, *ata_col = nullptr;
+  double* ata_val = nullptr;
+  int *perm = nullptr, *iperm = nullptr, *vmat = nullptr;
+  double* friction = nullptr;
+  int* tris = nullptr;  // 3T scene-global
+  std::vector<double*> obstacle_v;
+  std::vector<int*> obstacle_t;
+  // state
+  double *q = nullptr, *v = nullptr, *tn = nullptr, *qk = nullptr, *cstep = nullptr, *bp = nullptr;
+  // solve
+  SweepTask *fwd_tasks = nullptr, *bwd_tasks = nullptr;
+  SnInfo* sn = nullptr;
+  int* rows = nullptr;
+  double *Wr64 = nullptr, *Wc64 = nullptr;
+  float *Wr32 = nullptr, *Wc32 = nullptr;
+  double *b64 = nullptr, *y64 = nullptr, *x64 = nullptr;
+  float *b32 = nullptr, *y32 = nullptr, *x32 = nullptr;
+  // contacts
+  DContacts c{};
+  unsigned char* flags = nullptr;
+  int* sel_idx = nullptr;
+  void* cub_tmp = nullptr;
+  size_t cub_tmp_bytes = 0;
+  double* newf = nullptr;
+  double* ac_hist = nullptr;  // 4 per iteration
+  // self-collision detection scratch (selfdetect.cu)
+  void* self_ws = nullptr;
+};
+
+}  // namespace pdfb
+
+struct pdf_handle {
+  pdfb::Model model;
+  pdfb::Factor fac;
+  pdf_params prm{};
+  pdfb::DeviceBuffers d;
+  pdfb::DModel dm{};
+  pdfb::DObstacles obs{};
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[8] = {};
+  cudaGraphExec_t graph = nullptr;
+  int graph_iters = 0;
+  std::vector<int> fwd_off, bwd_off;  // task offsets per level
+  int n_levels = 0;
+  int cap_contacts = 0, cap_self = 0;
+  double time = 0.;
+  std::string err;
+  pdf_step_report last{};
+  pdf_stats stats{};
+  std::vector<double> residual_hist;
+  std::vector<double> host_time_before_start;
+  bool fp32 = false;
+};
+
+namespace pdfb {
+// selfdetect.cu
+int self_detect_init(pdf_handle* h);
+int self_detect_step(pdf_handle* h);  // self contacts of the step (detection + pairing)
+void self_levels_step(pdf_handle* h); // breadth-first Gauss-Seidel levels (after slots)
+void self_detect_free(pdf_handle* h);
+int standalone_candidates(const double* pos, int nv, const int* tris, int nt, double tol, int* pairs, int cap,
+                          int* n, int device, std::string& err);
+int standalone_self(const double* pos, int nv, const int* tris, int nt, double tol, pdf_contact* out, int cap,
+                    int* n, int device, std::string& err);
+}  // namespace pdfb

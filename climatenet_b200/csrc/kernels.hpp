@@ -1,0 +1,66 @@
+// kernels.hpp — declarations of the device kernels and their launch records.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+
+namespace pdfb {
+
+// One warp's share of a supernodal sweep: `count` consecutive rows (forward)
+// or columns (backward) starting at `first`, g lanes per row/column.
+struct SweepTask {
+  int sn, first, count, g;
+};
+struct SnInfo {
+  int c0, ns, nr, pad;
+  int64_t woff, roff;
+};
+
+// Analytic and mesh obstacles, passed by value.
+constexpr int kMaxObstacles = 8;
+struct DObstacle {
+  int type, material, n_tri, pad;
+  double c[3], R;
+  double rot[3], time_before_start;
+  double p[3], n[3];
+  double tol;
+  const double* mv;
+  const int* mt;
+};
+struct DObstacles {
+  int n;
+  DObstacle o[kMaxObstacles];
+};
+
+__global__ void k_step_init(DModel m, const double* q, double* v, double* tn, double* qk, double* cstep, double gx,
+                            double gy, double gz, double dt);
+__global__ void k_bend_proj(DModel m, const double* qk, double* bp);
+template <typename T>
+__global__ void k_vertex_rhs(DModel m, const double* qk, const double* v, const double* cstep, const double* bp,
+                             double air_damping, const int* slot_of, double* fslot, T* b, double dt,
+                             int residual_mode);
+template <typename T>
+__global__ void k_friction_obstacle(DModel m, DContacts c, T* b, int self_mode, int cur, int nxt);
+template <typename T>
+__global__ void k_friction_self(DModel m, DContacts c, T* b, double* newf, int cur, int nxt);
+__global__ void k_alart_curnier(DContacts c, const double* v, double* acc);
+__global__ void k_finalize(int n3, const double* qk, double* q);
+
+template <typename T>
+__global__ void k_sweep_forward(const SweepTask* tasks, int ntasks, const SnInfo* sn, const int* rows, const T* W,
+                                T* b, T* y);
+template <typename T>
+__global__ void k_sweep_backward(const SweepTask* tasks, int ntasks, const SnInfo* sn, const int* rows, const T* W,
+                                 const T* y, T* x, const int* perm, double* v, double* qk, const double* q, double dt,
+                                 int mode);
+
+// detection (detect_kernels.cu, compiled without FMA contraction)
+__global__ void k_obstacle_flags(int N, const double* q, DObstacles obs, unsigned char* flags);
+__global__ void k_obstacle_materialize(int N, const double* q, DObstacles obs, const int* idx, const int* vmat,
+                                       const double* friction, int n_mat, DContacts c);
+__global__ void k_contact_slots(DContacts c);
+__global__ void k_contact_slots_fill(DContacts c);
+__global__ void k_contact_slots_reset(DContacts c);
+
+}  // namespace pdfb

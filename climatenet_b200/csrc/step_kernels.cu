@@ -1,0 +1,333 @@
+// step_kernels.cu — device kernels of one projective-dynamics step:
+// predictor, local step (projections + right-hand side), per-contact
+// Coulomb/Signorini projection, self-contact Gauss-Seidel levels,
+// Alart-Curnier residual.  Reference citations are relative to the reference
+// project root ("SFE" = src/physics/SimulationFrictionEstimation.cpp).
+#include <cuda_runtime.h>
+
+#include "device.cuh"
+#include "kernels.hpp"
+
+namespace pdfb {
+
+// ---------------------------------------------------------------------------
+// Predictor and per-step constant (SimulationSpeed::initializeStep,
+// SimulationSpeed.cpp:62-76; external force SimulationBase.cpp:266-287 with the
+// gravity functor m g of simulation_building.cpp:86-92; t_n :294-301).
+// c = M t_n - dt A^T A q_n + dt * (attachment part of A^T p), which is the
+// part of SimulationSpeed::computeRhs (:238-278) that is constant over a step.
+__global__ void k_step_init(DModel m, const double* __restrict__ q, double* __restrict__ v,
+                            double* __restrict__ tn, double* __restrict__ qk, double* __restrict__ cstep,
+                            double gx, double gy, double gz, double dt) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.N) return;
+  const double mi = m.mass[i];
+  const double g[3] = {gx, gy, gz};
+  double ax = 0, ay = 0, az = 0;
+  for (int k = m.ata_ptr[i]; k < m.ata_ptr[i + 1]; ++k) {
+    const double a = m.ata_val[k];
+    const int j = m.ata_col[k];
+    ax += a * q[3 * (int64_t)j];
+    ay += a * q[3 * (int64_t)j + 1];
+    az += a * q[3 * (int64_t)j + 2];
+  }
+  const double ataq[3] = {ax, ay, az};
+  for (int c = 0; c < 3; ++c) {
+    const int64_t d = 3 * (int64_t)i + c;
+    const double f = mi * g[c];
+    const double t = v[d] + dt * ((1. / mi) * f);
+    tn[d] = t;
+    v[d] = t;
+    qk[d] = q[d] + dt * t;
+    double cc = mi * t - dt * ataq[c];
+    if (m.pin_term) cc += dt * m.pin_term[d];
+    cstep[d] = cc;
+  }
+}
+
+// Bending projections (BendingConstraint::addConstraintProjection,
+// BendingConstraint.cpp:106-138): p_b = sqrt(b) * (rest/|L x|) L x, or 0 when
+// |L x| <= 1e-25, with L x the mean-value Laplacian at the current iterate.
+__global__ void k_bend_proj(DModel m, const double* __restrict__ qk, double* __restrict__ bp) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= m.B) return;
+  double3 lb = make_double3(0., 0., 0.);
+  for (int k = m.bend_ptr[b]; k < m.bend_ptr[b + 1]; ++k) lb = lb + m.bend_coef[k] * ld3(qk, m.bend_idx[k]);
+  const double n = sqrt(dot3(lb, lb));
+  double3 p = make_double3(0., 0., 0.);
+  if (n > 1e-25) {
+    const double s = m.bend_rest[b] / n;
+    lb = make_double3(lb.x * s, lb.y * s, lb.z * s);
+    p = m.bend_w[b] * lb;
+  }
+  st3(bp, b, p);
+}
+
+// Vertex-centric local step + right-hand side (SimulationBase::computeProjections
+// SimulationBase.cpp:314-323, SpringConstraint.cpp:57-69, SimulationSpeed::computeRhs
+// SimulationSpeed.cpp:238-278):
+//   rhs_i = c_i + dt * ( sum_j kappa_ij normalize(q_i - q_j)          springs
+//                        + sum_{rows b containing i} A[b,i] p_b        bending
+//                        - d_i v_i )                                   damping
+// Vertex i gathers from its 1-ring, so no atomics are needed.  Output goes
+// straight to the solve's pivot order.  At contact vertices (slot >= 0) the
+// force estimate f = rhs - dt^2 (A^T A v)_i of SFE:337-347 is written too.
+// Residual mode (FP32 solves) writes r = rhs - (M + dt^2 A^T A) v instead.
+template <typename T>
+__global__ void k_vertex_rhs(DModel m, const double* __restrict__ qk, const double* __restrict__ v,
+                             const double* __restrict__ cstep, const double* __restrict__ bp,
+                             double air_damping, const int* __restrict__ slot_of,
+                             double* __restrict__ fslot, T* __restrict__ b, double dt, int residual_mode) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m.N) return;
+  const double3 qi = ld3(qk, i);
+  double3 acc = make_double3(0., 0., 0.);
+  const int bo = m.bend_of[i];
+  if (bo >= 0) acc = acc + m.self_bend[i] * ld3(bp, bo);
+  for (int s = m.ring_ptr[i]; s < m.ring_ptr[i + 1]; ++s) {
+    const int j = m.ring_idx[s];
+    const double3 e = normalized3(qi - ld3(qk, j));
+    acc = acc + m.ring_kappa[s] * e;
+    const int bj = m.bend_of[j];
+    if (bj >= 0) acc = acc + m.ring_bend[s] * ld3(bp, bj);
+  }
+  const double3 vi = ld3(v, i);
+  const int slot = slot_of[i];
+  // air damping is switched off at every contact vertex (SimulationBase.cpp:347-396)
+  const double di = slot >= 0 ? 0. : air_damping;
+  const double3 c = ld3(cstep, i);
+  const double3 rhs = make_double3(c.x + dt * (acc.x - di * vi.x), c.y + dt * (acc.y - di * vi.y),
+                                   c.z + dt * (acc.z - di * vi.z));
+  double3 out = rhs;
+  if (residual_mode || slot >= 0) {
+    double ax = 0, ay = 0, az = 0;
+    for (int k = m.ata_ptr[i]; k < m.ata_ptr[i + 1]; ++k) {
+      const double a = m.ata_val[k];
+      const int j = m.ata_col[k];
+      ax += a * v[3 * (int64_t)j];
+      ay += a * v[3 * (int64_t)j + 1];
+      az += a * v[3 * (int64_t)j + 2];
+    }
+    const double dt2 = dt * dt;
+    const double3 f = make_double3(rhs.x - dt2 * ax, rhs.y - dt2 * ay, rhs.z - dt2 * az);
+    if (slot >= 0) st3(fslot, slot, f);
+    if (residual_mode) {
+      const double mi = m.mass[i];
+      out = make_double3(f.x - mi * vi.x, f.y - mi * vi.y, f.z - mi * vi.z);
+    }
+  }
+  const int64_t p = m.iperm[i];
+  b[3 * p] = (T)out.x;
+  b[3 * p + 1] = (T)out.y;
+  b[3 * p + 2] = (T)out.z;
+}
+
+template __global__ void k_vertex_rhs<double>(DModel, const double*, const double*, const double*, const double*,
+                                              double, const int*, double*, double*, double, int);
+template __global__ void k_vertex_rhs<float>(DModel, const double*, const double*, const double*, const double*,
+                                             double, const int*, double*, float*, double, int);
+
+__device__ __forceinline__ void atomic_add3(double* p, double3 g) {
+  atomicAdd(p, g.x);
+  atomicAdd(p + 1, g.y);
+  atomicAdd(p + 2, g.z);
+}
+__device__ __forceinline__ void atomic_add3(float* p, double3 g) {
+  atomicAdd(p, (float)g.x);
+  atomicAdd(p + 1, (float)g.y);
+  atomicAdd(p + 2, (float)g.z);
+}
+
+__device__ __forceinline__ double3 basis_t(const double* B, double3 v) {
+  // B^T v with B stored by columns (n, t, b)
+  return make_double3(B[0] * v.x + B[1] * v.y + B[2] * v.z, B[3] * v.x + B[4] * v.y + B[5] * v.z,
+                      B[6] * v.x + B[7] * v.y + B[8] * v.z);
+}
+__device__ __forceinline__ double3 basis_v(const double* B, double3 r) {
+  // B r : component i = (B(i,0) r0 + B(i,1) r1) + B(i,2) r2
+  return make_double3(B[0] * r.x + B[3] * r.y + B[6] * r.z, B[1] * r.x + B[4] * r.y + B[7] * r.z,
+                      B[2] * r.x + B[5] * r.y + B[8] * r.z);
+}
+
+// Friction-cone projection shared by obstacle and self contacts (SFE:376-394,
+// 503-520): r = -forceLoc, tangential part clamped to mu r_N.
+__device__ __forceinline__ double3 cone_project(double3 fl, double mu) {
+  double3 r = make_double3(-fl.x, -fl.y, -fl.z);
+  const double rtn = sqrt(r.y * r.y + r.z * r.z);
+  if (rtn > mu * r.x) {
+    r.y *= mu * r.x / rtn;
+    r.z *= mu * r.x / rtn;
+  }
+  return r;
+}
+
+// Obstacle contacts (SFE:350-423).  One thread per contact.
+template <typename T>
+__global__ void k_friction_obstacle(DModel m, DContacts c, T* __restrict__ b, int self_mode, int cur, int nxt) {
+  const int C = *c.n_contacts;
+  const int S = self_mode ? *c.n_self : 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C; k += gridDim.x * blockDim.x) {
+    const int vid = c.c_vertex[k];
+    const int slot = c.c_slot[k];
+    const double* B = c.c_basis + 9 * (int64_t)k;
+    double3 f = ld3(c.f, slot);
+    if (self_mode) f = f + ld3(c.sf[cur], slot);
+    const double mv = m.mass[vid];
+    const double3 sp = ld3(c.c_speed, k);
+    const double3 fl = basis_t(B, make_double3(f.x - mv * sp.x, f.y - mv * sp.y, f.z - mv * sp.z));
+    if (fl.x > 0.) continue;  // take-off: the stored local force keeps its old value
+    const double3 r = cone_project(fl, c.c_mu[k]);
+    st3(c.c_force, k, r);
+    const double3 g = basis_v(B, r);
+    if (!self_mode || S == 0) atomic_add3(b + 3 * (int64_t)m.iperm[vid], g);
+    if (self_mode) st3(c.cf[nxt], slot, g);
+  }
+}
+template __global__ void k_friction_obstacle<double>(DModel, DContacts, double*, int, int, int);
+template __global__ void k_friction_obstacle<float>(DModel, DContacts, float*, int, int, int);
+
+// Self contacts (SFE:431-587).  One CTA walks the breadth-first levels in
+// order; inside a level every contact is estimated from the buffers as they
+// stood before the level (compute phase), then the previous forces are removed
+// and the new ones added (update phase).  At the end the contact and
+// self-contact forces are added to the right-hand side and the buffer that
+// becomes "next" is cleared.
+template <typename T>
+__global__ void k_friction_self(DModel m, DContacts c, T* __restrict__ b, double* __restrict__ newf, int cur,
+                                int nxt) {
+  const int S = *c.n_self;
+  const int C = *c.n_contacts;
+  const int nl = *c.n_levels;
+  if (S > 0) {
+    for (int l = 0; l < nl; ++l) {
+      const int l0 = c.level_ptr[l], l1 = c.level_ptr[l + 1];
+      for (int i = l0 + threadIdx.x; i < l1; i += blockDim.x) {
+        const int sc = c.level_order[i];
+        const int sa = c.s_slota[sc], sb = c.s_slotb[sc];
+        const int va = c.s_vertex[sc], vb = c.s_partner[sc];
+        const double* Bm = c.s_basis + 9 * (int64_t)sc;
+        const double mA = m.mass[va], mB = m.mass[vb];
+        const double3 rem = ld3(c.s_remember, sc);
+        const double3 fA = ld3(c.f, sa) + ld3(c.cf[nxt], sa) + ld3(c.sf[cur], sa) + ld3(c.sf[nxt], sa) - rem;
+        const double3 fB = ld3(c.f, sb) + ld3(c.cf[nxt], sb) + ld3(c.sf[cur], sb) + ld3(c.sf[nxt], sb) + rem;
+        const double ia = 1. / mA, ib = 1. / mB;
+        const double3 fl = basis_t(Bm, make_double3(ia * fA.x - ib * fB.x, ia * fA.y - ib * fB.y, ia * fA.z - ib * fB.z));
+        double3 g = make_double3(0., 0., 0.);
+        if (!(fl.x > 0.)) {
+          double3 r = cone_project(fl, c.s_mu[sc]);
+          const double sc2 = (mA * mB) / (mA + mB);
+          r = make_double3(sc2 * r.x, sc2 * r.y, sc2 * r.z);
+          st3(c.s_force, sc, r);
+          g = basis_v(Bm, r);
+        }
+        st3(newf, sc, g);
+      }
+      __syncthreads();
+      for (int i = l0 + threadIdx.x; i < l1; i += blockDim.x) {
+        const int sc = c.level_order[i];
+        const int sa = c.s_slota[sc], sb = c.s_slotb[sc];
+        const double3 prev = ld3(c.s_remember, sc);
+        const double3 g = ld3(newf, sc);
+        atomicAdd(c.sf[cur] + 3 * sa, -prev.x);
+        atomicAdd(c.sf[cur] + 3 * sa + 1, -prev.y);
+        atomicAdd(c.sf[cur] + 3 * sa + 2, -prev.z);
+        atomicAdd(c.sf[cur] + 3 * sb, prev.x);
+        atomicAdd(c.sf[cur] + 3 * sb + 1, prev.y);
+        atomicAdd(c.sf[cur] + 3 * sb + 2, prev.z);
+        atomicAdd(c.sf[nxt] + 3 * sa, g.x);
+        atomicAdd(c.sf[nxt] + 3 * sa + 1, g.y);
+        atomicAdd(c.sf[nxt] + 3 * sa + 2, g.z);
+        atomicAdd(c.sf[nxt] + 3 * sb, -g.x);
+        atomicAdd(c.sf[nxt] + 3 * sb + 1, -g.y);
+        atomicAdd(c.sf[nxt] + 3 * sb + 2, -g.z);
+        st3(c.s_remember, sc, g);
+      }
+      __syncthreads();
+    }
+    const int ns = *c.n_slots;
+    for (int s = threadIdx.x; s < ns; s += blockDim.x) {
+      const double3 g = ld3(c.cf[nxt], s) + ld3(c.sf[nxt], s);
+      const int64_t p = m.iperm[c.slot_vertex[s]];
+      atomic_add3(b + 3 * p, g);
+    }
+    __syncthreads();
+  }
+  (void)C;
+  // buffer swap: the old "current" buffers become "next" and start from zero
+  if (S > 0 || C > 0) {
+    const int ns = *c.n_slots;
+    for (int s = threadIdx.x; s < 3 * ns; s += blockDim.x) {
+      c.cf[cur][s] = 0.;
+      c.sf[cur][s] = 0.;
+    }
+  }
+}
+template __global__ void k_friction_self<double>(DModel, DContacts, double*, double*, int, int);
+template __global__ void k_friction_self<float>(DModel, DContacts, float*, double*, int, int);
+
+// Alart-Curnier residual with rho = 1 (coulomb_util.cpp:92-152) for every
+// contact after the solve (SFE:590-652).  acc[4] += {sum |AC|, max |AC|,
+// sum |AC_N|, sum |AC_T|}.
+__device__ __forceinline__ double dmax0(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double dmin0(double a, double b) { return (b < a) ? b : a; }
+
+__device__ double ac_norm(double3 u, double3 r, double mu, double* an, double* at) {
+  const double N = dmax0(0., r.x - u.x) - r.x;
+  const double dx = r.y - u.y, dy = r.z - u.z;
+  const double dn = sqrt(dx * dx + dy * dy);
+  const double radius = dmax0(0., mu * r.x / dn);
+  const double mm = dmin0(1., radius);
+  const double tx = dx * mm - r.y, ty = dy * mm - r.z;
+  *an = fabs(N);
+  *at = sqrt(tx * tx + ty * ty);
+  return sqrt(N * N + tx * tx + ty * ty);
+}
+
+__device__ __forceinline__ void atomic_max_pos(double* addr, double val) {
+  // valid for non-negative doubles: their bit patterns order like int64
+  atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(val));
+}
+
+__global__ void k_alart_curnier(DContacts c, const double* __restrict__ v, double* __restrict__ acc) {
+  const int C = *c.n_contacts, S = *c.n_self;
+  double s = 0, mx = 0, sn = 0, st = 0;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C + S; k += gridDim.x * blockDim.x) {
+    double an, at, n;
+    if (k < C) {
+      const double* B = c.c_basis + 9 * (int64_t)k;
+      const double3 u = basis_t(B, ld3(v, c.c_vertex[k]) - ld3(c.c_speed, k));
+      n = ac_norm(u, ld3(c.c_force, k), c.c_mu[k], &an, &at);
+      c.c_ac[k] = n;
+    } else {
+      const int q = k - C;
+      const double* B = c.s_basis + 9 * (int64_t)q;
+      const double3 u = basis_t(B, ld3(v, c.s_vertex[q]) - ld3(v, c.s_partner[q]));
+      n = ac_norm(u, ld3(c.s_force, q), c.s_mu[q], &an, &at);
+      c.s_ac[q] = n;
+    }
+    s += n;
+    mx = fmax(mx, n);
+    sn += an;
+    st += at;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s += __shfl_xor_sync(0xffffffffu, s, o);
+    sn += __shfl_xor_sync(0xffffffffu, sn, o);
+    st += __shfl_xor_sync(0xffffffffu, st, o);
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0 && (C + S) > 0) {
+    atomicAdd(acc, s);
+    atomic_max_pos(acc + 1, mx);
+    atomicAdd(acc + 2, sn);
+    atomicAdd(acc + 3, st);
+  }
+}
+
+// End of step (SFE::updateScene SFE:64-87): q <- q^K.
+__global__ void k_finalize(int n3, const double* __restrict__ qk, double* __restrict__ q) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < n3) q[d] = qk[d];
+}
+
+}  // namespace pdfb

@@ -1,0 +1,237 @@
+"""ctypes binding of the B200 step-loop library (climatenet_b200/_build/libpdf_b200.so).
+
+There is no fallback: if the library is missing or no CUDA device is usable,
+every call raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_build", "libpdf_b200.so")
+_lib = None
+
+
+class PdfError(RuntimeError):
+    """A pdf_* call returned a non-zero status."""
+
+    def __init__(self, status, msg):
+        super().__init__("%s: %s" % (abi.STATUS_NAMES.get(status, status), msg))
+        self.status = status
+
+
+def lib():
+    """Load (once) and return the native library; raise if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("climatenet_b200 native library not built: %s (run __graft_entry__.build())"
+                          % LIB_PATH)
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    i32 = C.c_int32
+    L.pdf_params_default.argtypes = [C.POINTER(abi.pdf_params)]
+    L.pdf_global_error.restype = C.c_char_p
+    L.pdf_last_error.argtypes = [vp]
+    L.pdf_last_error.restype = C.c_char_p
+    L.pdf_scene_load_json.argtypes = [C.c_char_p, C.POINTER(vp)]
+    L.pdf_scene_view.argtypes = [vp, C.POINTER(abi.pdf_scene_desc)]
+    L.pdf_scene_free.argtypes = [vp]
+    L.pdf_params_load_json.argtypes = [C.c_char_p, C.POINTER(abi.pdf_params), C.POINTER(i32), C.POINTER(i32)]
+    L.pdf_create.argtypes = [C.POINTER(abi.pdf_scene_desc), C.POINTER(abi.pdf_params), C.POINTER(vp)]
+    L.pdf_step.argtypes = [vp, i32, C.POINTER(abi.pdf_step_report)]
+    L.pdf_get_state.argtypes = [vp, vp, vp]
+    L.pdf_set_state.argtypes = [vp, vp, vp]
+    L.pdf_device_state.argtypes = [vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)]
+    L.pdf_get_contacts.argtypes = [vp, vp, i32, C.POINTER(i32)]
+    L.pdf_get_self_contacts.argtypes = [vp, vp, i32, C.POINTER(i32)]
+    L.pdf_get_self_levels.argtypes = [vp, vp, i32, vp, i32, C.POINTER(i32)]
+    L.pdf_get_stats.argtypes = [vp, C.POINTER(abi.pdf_stats)]
+    L.pdf_export_stats.argtypes = [vp, C.c_char_p]
+    L.pdf_get_residual_history.argtypes = [vp, vp, i32, C.POINTER(i32)]
+    L.pdf_time_phase.argtypes = [vp, i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.pdf_destroy.argtypes = [vp]
+    L.pdf_detect_candidates.argtypes = [vp, i32, vp, i32, C.c_double, vp, i32, C.POINTER(i32), i32]
+    L.pdf_detect_self_collisions.argtypes = [vp, i32, vp, i32, C.c_double, vp, i32, C.POINTER(i32), i32]
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _check(status, handle=None):
+    if status != 0:
+        L = lib()
+        msg = L.pdf_last_error(handle) if handle else L.pdf_global_error()
+        raise PdfError(status, (msg or b"").decode())
+
+
+class LoadedScene:
+    """A scene read from the reference's JSON format (getSceneFromJSONDocument)."""
+
+    def __init__(self, path):
+        h = C.c_void_p()
+        _check(lib().pdf_scene_load_json(os.fsencode(path), C.byref(h)))
+        self.h = h
+        self._desc = abi.pdf_scene_desc()
+        _check(lib().pdf_scene_view(self.h, C.byref(self._desc)))
+
+    def desc(self):
+        return self._desc
+
+    @property
+    def n_vertices(self):
+        return self._desc.n_vertices
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().pdf_scene_free(self.h)
+            self.h = None
+
+
+def load_params(path):
+    """getSimulationParametersFromJSONDocument: (pdf_params, frames, steps per frame)."""
+    p = abi.pdf_params()
+    fr = C.c_int32()
+    spf = C.c_int32()
+    _check(lib().pdf_params_load_json(os.fsencode(path), C.byref(p), C.byref(fr), C.byref(spf)))
+    return p, fr.value, spf.value
+
+
+class Simulation:
+    """One simulation handle; the drop-in for SimulationBase (step, exportStats)."""
+
+    def __init__(self, scene, params):
+        L = lib()
+        self._scene = scene
+        self._desc = scene.desc()
+        self.params = params
+        h = C.c_void_p()
+        _check(L.pdf_create(C.byref(self._desc), C.byref(params), C.byref(h)))
+        self.h = h
+        self.n = self._desc.n_vertices
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().pdf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def step(self, n=1):
+        rep = abi.pdf_step_report()
+        _check(lib().pdf_step(self.h, n, C.byref(rep)), self.h)
+        return rep
+
+    def state(self):
+        q = np.empty((self.n, 3))
+        v = np.empty((self.n, 3))
+        _check(lib().pdf_get_state(self.h, _ptr(q), _ptr(v)), self.h)
+        return q, v
+
+    def set_state(self, q=None, v=None):
+        qa = None if q is None else np.ascontiguousarray(q, dtype=np.float64)
+        va = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
+        _check(lib().pdf_set_state(self.h, None if qa is None else _ptr(qa),
+                                   None if va is None else _ptr(va)), self.h)
+
+    def device_state(self):
+        q = C.c_void_p()
+        v = C.c_void_p()
+        s = C.c_void_p()
+        _check(lib().pdf_device_state(self.h, C.byref(q), C.byref(v), C.byref(s)), self.h)
+        return q.value, v.value, s.value
+
+    def _contacts(self, fn):
+        n = C.c_int32()
+        _check(fn(self.h, None, 0, C.byref(n)), self.h)
+        arr = (abi.pdf_contact * max(1, n.value))()
+        _check(fn(self.h, arr, n.value, C.byref(n)), self.h)
+        return abi.contacts_to_numpy(arr, n.value)
+
+    def contacts(self):
+        return self._contacts(lib().pdf_get_contacts)
+
+    def self_contacts(self):
+        return self._contacts(lib().pdf_get_self_contacts)
+
+    def self_levels(self):
+        nl = C.c_int32()
+        _check(lib().pdf_get_self_levels(self.h, None, 0, None, 0, C.byref(nl)), self.h)
+        ns = self.self_contacts()["vertex"].shape[0]
+        ptr = np.zeros(nl.value + 1, dtype=np.int32)
+        order = np.zeros(max(1, ns), dtype=np.int32)
+        _check(lib().pdf_get_self_levels(self.h, _ptr(ptr), nl.value + 1, _ptr(order), ns, C.byref(nl)),
+               self.h)
+        return ptr, order[:ns]
+
+    def stats(self):
+        s = abi.pdf_stats()
+        _check(lib().pdf_get_stats(self.h, C.byref(s)), self.h)
+        return s
+
+    def export_stats(self, path):
+        _check(lib().pdf_export_stats(self.h, os.fsencode(path)), self.h)
+
+    exportStats = export_stats
+
+    def time_phase(self, phase, reps=10):
+        """(ms per repetition, algorithmic bytes) of one phase run in isolation."""
+        ms = C.c_double()
+        by = C.c_double()
+        _check(lib().pdf_time_phase(self.h, phase, reps, C.byref(ms), C.byref(by)), self.h)
+        return ms.value, by.value
+
+    def residual_history(self):
+        n = C.c_int32()
+        lib().pdf_get_residual_history(self.h, None, 0, C.byref(n))
+        out = np.zeros(max(1, n.value))
+        lib().pdf_get_residual_history(self.h, _ptr(out), n.value, C.byref(n))
+        return out[:n.value]
+
+
+def getSceneFromJSONFileName(path):
+    """Mirror of getSceneFromJSONFileName (src/scene_building.cpp:41-47)."""
+    return LoadedScene(path)
+
+
+def getSimulationParametersFromJSONFileName(path):
+    """Mirror of getSimulationParametersFromJSONFileName (src/simulation_building.cpp:29-35)."""
+    return load_params(path)[0]
+
+
+def getSimulation(scene, params):
+    """Mirror of getSimulation (src/simulation_building.cpp:80-98)."""
+    return Simulation(scene, params)
+
+
+def detect_candidates(positions, triangles, tolerance, device=0, cap=None):
+    """Vertex-triangle box candidates of one mesh, sorted (vertex, triangle)."""
+    pos = np.ascontiguousarray(positions, dtype=np.float64)
+    tris = np.ascontiguousarray(triangles, dtype=np.int32)
+    n = C.c_int32()
+    if cap is None:
+        cap = 64 * len(pos) + 1024
+    out = np.zeros((cap, 2), dtype=np.int32)
+    _check(lib().pdf_detect_candidates(_ptr(pos), len(pos), _ptr(tris), len(tris), tolerance,
+                                       _ptr(out), cap, C.byref(n), device))
+    return out[:n.value]
+
+
+def detect_self_collisions(positions, triangles, tolerance, device=0):
+    """Self collisions (greedy node-node pairing) of one mesh."""
+    pos = np.ascontiguousarray(positions, dtype=np.float64)
+    tris = np.ascontiguousarray(triangles, dtype=np.int32)
+    n = C.c_int32()
+    cap = 2 * len(pos) + 16
+    arr = (abi.pdf_contact * cap)()
+    _check(lib().pdf_detect_self_collisions(_ptr(pos), len(pos), _ptr(tris), len(tris), tolerance,
+                                            arr, cap, C.byref(n), device))
+    return abi.contacts_to_numpy(arr, n.value)

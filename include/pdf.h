@@ -140,6 +140,8 @@ typedef struct pdf_step_report {
   double time;                      /* simulated time after the step (s)        */
   int32_t refine_sweeps;            /* FP32 mode: refinement sweeps, last step  */
   double solve_residual;            /* FP32 mode: last relative FP64 residual   */
+  double device_ms;                 /* device time of the whole pdf_step call,
+                                       CUDA events on the handle's stream      */
 } pdf_step_report;
 
 typedef struct pdf_stats {
@@ -153,6 +155,8 @@ typedef struct pdf_stats {
   int32_t n_supernodes, n_levels;   /* supernodal elimination tree              */
   int64_t lhs_nnz;                  /* nnz(M + dt^2 A^T A)                      */
   int32_t n_constraint_rows;        /* rows(A)                                  */
+  int64_t kernel_launches;          /* this library's kernels launched so far   */
+  int64_t factor_nnz_true;          /* structural nnz(L) without padding        */
 } pdf_stats;
 
 /* One contact, as the reference's CollisionInfo / SelfCollisionInfo plus
@@ -230,6 +234,16 @@ int pdf_export_stats(pdf_handle* h, const char* path);
 /* Per-iteration mean AC residuals of the last step (n <= cap written). */
 int pdf_get_residual_history(pdf_handle* h, double* out, int32_t cap,
                              int32_t* n);
+
+/* Times one phase of the PD iteration in isolation on the handle's stream:
+ * reps back-to-back launches bracketed by CUDA events, average device time per
+ * repetition in *ms.  Phases: 0 = global solve (forward + backward supernodal
+ * sweeps), 1 = local step (projections + right-hand side), 2 = contact
+ * projection, 3 = detection (obstacles and self-collision).  The state is not
+ * advanced in a meaningful way; call it before or after a measured run.
+ * *bytes receives the algorithmic bytes one repetition must move. */
+int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms,
+                   double* bytes);
 
 /* Last error message of this handle (never NULL). */
 const char* pdf_last_error(const pdf_handle* h);

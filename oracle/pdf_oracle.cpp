@@ -931,8 +931,10 @@ static void step(Sim& s) {
   for (; it < s.prm.local_global_iterations; ++it) {
     /* SFE::computeRhs SFE:307-588 */
     rhs_base(s, s.q.data(), s.tn.data(), s.vnext.data(), s.qnext.data(), s.rhs.data());
-    s.c_local_forces.resize(C, {0, 0, 0});
-    s.s_local_forces.resize(S, {0, 0, 0});
+    /* SFE:334-335 resize: slots keep whatever an earlier step left there
+     * (storage only ever grows; never-used slots hold zero). */
+    if ((int)s.c_local_forces.size() < C) s.c_local_forces.resize(C, {0, 0, 0});
+    if ((int)s.s_local_forces.size() < S) s.s_local_forces.resize(S, {0, 0, 0});
     if (!((C == 0) && (!self || S == 0))) {
       /* forces = rhs - dt^2 A^T A v  (SFE:337-347) */
       std::vector<double> atav(3 * (size_t)N);
