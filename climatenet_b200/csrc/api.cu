@@ -63,10 +63,11 @@ void build_schedule(pdf_handle* h) {
   std::vector<std::vector<SweepTask>> fw(f.n_levels), bw(f.n_levels);
   for (int s = 0; s < f.n_sn; ++s) {
     const int ns = f.sn_ns[s], nr = f.sn_nr[s], L = f.sn_level[s];
-    const int gf = group_size(ns);
+    // about two elements per lane: g = pow2 >= half the typical row/column length
+    const int gf = group_size(ns / 2);
     const int per_f = 32 / gf;
     for (int r = 0; r < ns + nr; r += per_f) fw[L].push_back({s, r, std::min(per_f, ns + nr - r), gf});
-    const int gb = group_size(ns / 2 + nr);
+    const int gb = group_size((ns / 2 + nr) / 2);
     const int per_b = 32 / gb;
     for (int c = 0; c < ns; c += per_b) bw[L].push_back({s, c, std::min(per_b, ns - c), gb});
   }
@@ -299,6 +300,35 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   h->stats.setup_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
+// Local step: bending projections + vertex right-hand side (or residual).
+template <typename T>
+void launch_local(pdf_handle* h, T* b, int mode) {
+  DeviceBuffers& d = h->d;
+  const DModel& dm = h->dm;
+  cudaStream_t st = h->stream;
+  if (dm.B > 0) k_bend_proj<<<blocks_for(dm.B), kThreads, 0, st>>>(dm, d.qk, d.bp);
+  launch_vertex_rhs<T>(blocks_for(dm.N), kThreads, st, dm, d.qk, d.v, d.cstep, d.bp,
+                       std::max(h->prm.air_damping, 0.), d.c.slot_of, d.c.f, b, h->prm.time_step, mode);
+}
+
+// Global solve: forward sweep over the levels bottom-up, backward top-down.
+template <typename T>
+void launch_solve(pdf_handle* h, T* b, T* y, T* x, const T* Wr, const T* Wc, int mode) {
+  DeviceBuffers& d = h->d;
+  cudaStream_t st = h->stream;
+  for (int L = 0; L < h->n_levels; ++L) {
+    const int nt = h->fwd_off[L + 1] - h->fwd_off[L];
+    if (nt == 0) continue;
+    launch_sweep_forward<T>(st, d.fwd_tasks + h->fwd_off[L], nt, d.sn, d.rows, Wr, b, y, h->dm.N);
+  }
+  for (int L = h->n_levels - 1; L >= 0; --L) {
+    const int nt = h->bwd_off[L + 1] - h->bwd_off[L];
+    if (nt == 0) continue;
+    launch_sweep_backward<T>(st, d.bwd_tasks + h->bwd_off[L], nt, d.sn, d.rows, Wc, y, x, d.perm, d.v, d.qk, d.q,
+                             h->prm.time_step, mode, h->dm.N);
+  }
+}
+
 // One PD iteration (SimulationBase.cpp:119-157): local step + friction
 // (SFE::computeRhs), global solve (SimulationSpeed::solve), AC residual.
 template <typename T>
@@ -306,26 +336,12 @@ void launch_iteration(pdf_handle* h, int k, T* b, T* y, T* x, const T* Wr, const
   DeviceBuffers& d = h->d;
   const DModel& dm = h->dm;
   cudaStream_t st = h->stream;
-  const double dt = h->prm.time_step;
   const int self_mode = h->prm.self_collision ? 1 : 0;
   const int cur = k & 1, nxt = 1 - cur;
-  if (dm.B > 0) k_bend_proj<<<blocks_for(dm.B), kThreads, 0, st>>>(dm, d.qk, d.bp);
-  k_vertex_rhs<T><<<blocks_for(dm.N), kThreads, 0, st>>>(dm, d.qk, d.v, d.cstep, d.bp,
-                                                          std::max(h->prm.air_damping, 0.), d.c.slot_of, d.c.f, b,
-                                                          dt, mode);
-  k_friction_obstacle<T><<<kStrideBlocks, kThreads, 0, st>>>(dm, d.c, b, self_mode, cur, nxt);
-  if (self_mode) k_friction_self<T><<<1, 1024, 0, st>>>(dm, d.c, b, d.newf, cur, nxt);
-  for (int L = 0; L < h->n_levels; ++L) {
-    const int nt = h->fwd_off[L + 1] - h->fwd_off[L];
-    if (nt == 0) continue;
-    k_sweep_forward<T><<<(nt + 7) / 8, 256, 0, st>>>(d.fwd_tasks + h->fwd_off[L], nt, d.sn, d.rows, Wr, b, y);
-  }
-  for (int L = h->n_levels - 1; L >= 0; --L) {
-    const int nt = h->bwd_off[L + 1] - h->bwd_off[L];
-    if (nt == 0) continue;
-    k_sweep_backward<T><<<(nt + 7) / 8, 256, 0, st>>>(d.bwd_tasks + h->bwd_off[L], nt, d.sn, d.rows, Wc, y, x,
-                                                       d.perm, d.v, d.qk, d.q, dt, mode);
-  }
+  launch_local<T>(h, b, mode);
+  launch_friction_obstacle<T>(kStrideBlocks, kThreads, st, dm, d.c, b, self_mode, cur, nxt);
+  if (self_mode) launch_friction_self<T>(1, 1024, st, dm, d.c, b, d.newf, cur, nxt);
+  launch_solve<T>(h, b, y, x, Wr, Wc, mode);
   k_alart_curnier<<<kStrideBlocks, kThreads, 0, st>>>(d.c, d.v, d.ac_hist + 4 * (size_t)k);
 }
 
@@ -585,7 +601,6 @@ int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms_out, d
     DeviceBuffers& d = h->d;
     const DModel& dm = h->dm;
     cudaStream_t st = h->stream;
-    const double dt = h->prm.time_step;
     const Factor& f = h->fac;
     const double s = h->fp32 ? 4. : 8.;
     const double N = dm.N;
@@ -627,43 +642,20 @@ int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms_out, d
       }
       CK(cudaEventRecord(h->ev[5], st));
       if (phase == 0) {
-        for (int L = 0; L < h->n_levels; ++L) {
-          const int nt = h->fwd_off[L + 1] - h->fwd_off[L];
-          if (!nt) continue;
-          if (h->fp32)
-            k_sweep_forward<float><<<(nt + 7) / 8, 256, 0, st>>>(d.fwd_tasks + h->fwd_off[L], nt, d.sn, d.rows,
-                                                                 d.Wr32, d.b32, d.y32);
-          else
-            k_sweep_forward<double><<<(nt + 7) / 8, 256, 0, st>>>(d.fwd_tasks + h->fwd_off[L], nt, d.sn, d.rows,
-                                                                  d.Wr64, d.b64, d.y64);
-        }
-        for (int L = h->n_levels - 1; L >= 0; --L) {
-          const int nt = h->bwd_off[L + 1] - h->bwd_off[L];
-          if (!nt) continue;
-          if (h->fp32)
-            k_sweep_backward<float><<<(nt + 7) / 8, 256, 0, st>>>(d.bwd_tasks + h->bwd_off[L], nt, d.sn, d.rows,
-                                                                  d.Wc32, d.y32, d.x32, d.perm, d.v, d.qk, d.q,
-                                                                  dt, 1);
-          else
-            k_sweep_backward<double><<<(nt + 7) / 8, 256, 0, st>>>(d.bwd_tasks + h->bwd_off[L], nt, d.sn, d.rows,
-                                                                   d.Wc64, d.y64, d.x64, d.perm, d.v, d.qk, d.q,
-                                                                   dt, 0);
-        }
-      } else if (phase == 1) {
-        if (dm.B > 0) k_bend_proj<<<blocks_for(dm.B), kThreads, 0, st>>>(dm, d.qk, d.bp);
         if (h->fp32)
-          k_vertex_rhs<float><<<blocks_for(dm.N), kThreads, 0, st>>>(dm, d.qk, d.v, d.cstep, d.bp,
-                                                                     std::max(h->prm.air_damping, 0.), d.c.slot_of,
-                                                                     d.c.f, d.b32, dt, 1);
+          launch_solve<float>(h, d.b32, d.y32, d.x32, d.Wr32, d.Wc32, 1);
         else
-          k_vertex_rhs<double><<<blocks_for(dm.N), kThreads, 0, st>>>(dm, d.qk, d.v, d.cstep, d.bp,
-                                                                      std::max(h->prm.air_damping, 0.),
-                                                                      d.c.slot_of, d.c.f, d.b64, dt, 0);
+          launch_solve<double>(h, d.b64, d.y64, d.x64, d.Wr64, d.Wc64, 0);
+      } else if (phase == 1) {
+        if (h->fp32)
+          launch_local<float>(h, d.b32, 1);
+        else
+          launch_local<double>(h, d.b64, 0);
       } else if (phase == 2) {
         if (h->fp32)
-          k_friction_obstacle<float><<<kStrideBlocks, kThreads, 0, st>>>(dm, d.c, d.b32, 0, 0, 1);
+          launch_friction_obstacle<float>(kStrideBlocks, kThreads, st, dm, d.c, d.b32, 0, 0, 1);
         else
-          k_friction_obstacle<double><<<kStrideBlocks, kThreads, 0, st>>>(dm, d.c, d.b64, 0, 0, 1);
+          launch_friction_obstacle<double>(kStrideBlocks, kThreads, st, dm, d.c, d.b64, 0, 0, 1);
       } else {
         if (h->obs.n > 0) {
           k_obstacle_flags<<<blocks_for(dm.N), kThreads, 0, st>>>(dm.N, d.q, h->obs, d.flags);

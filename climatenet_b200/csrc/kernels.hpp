@@ -36,24 +36,31 @@ struct DObstacles {
 __global__ void k_step_init(DModel m, const double* q, double* v, double* tn, double* qk, double* cstep, double gx,
                             double gy, double gz, double dt);
 __global__ void k_bend_proj(DModel m, const double* qk, double* bp);
-template <typename T>
-__global__ void k_vertex_rhs(DModel m, const double* qk, const double* v, const double* cstep, const double* bp,
-                             double air_damping, const int* slot_of, double* fslot, T* b, double dt,
-                             int residual_mode);
-template <typename T>
-__global__ void k_friction_obstacle(DModel m, DContacts c, T* b, int self_mode, int cur, int nxt);
-template <typename T>
-__global__ void k_friction_self(DModel m, DContacts c, T* b, double* newf, int cur, int nxt);
 __global__ void k_alart_curnier(DContacts c, const double* v, double* acc);
 __global__ void k_finalize(int n3, const double* qk, double* q);
 
+// Templated kernels are launched through host wrappers defined (and
+// instantiated for float and double) next to the kernels, so that every
+// launch goes through the translation unit that registers the kernel.
 template <typename T>
-__global__ void k_sweep_forward(const SweepTask* tasks, int ntasks, const SnInfo* sn, const int* rows, const T* W,
-                                T* b, T* y);
+void launch_vertex_rhs(dim3 grid, dim3 block, cudaStream_t st, DModel m, const double* qk, const double* v,
+                       const double* cstep, const double* bp, double air_damping, const int* slot_of, double* fslot,
+                       T* b, double dt, int residual_mode);
 template <typename T>
-__global__ void k_sweep_backward(const SweepTask* tasks, int ntasks, const SnInfo* sn, const int* rows, const T* W,
-                                 const T* y, T* x, const int* perm, double* v, double* qk, const double* q, double dt,
-                                 int mode);
+void launch_friction_obstacle(dim3 grid, dim3 block, cudaStream_t st, DModel m, DContacts c, T* b, int self_mode,
+                              int cur, int nxt);
+template <typename T>
+void launch_friction_self(dim3 grid, dim3 block, cudaStream_t st, DModel m, DContacts c, T* b, double* newf, int cur,
+                          int nxt);
+// Solve vectors b, y, x are three planes of n values (x, y, z components) in
+// pivot order.
+template <typename T>
+void launch_sweep_forward(cudaStream_t st, const SweepTask* tasks, int ntasks, const SnInfo* sn, const int* rows,
+                          const T* W, T* b, T* y, int n);
+template <typename T>
+void launch_sweep_backward(cudaStream_t st, const SweepTask* tasks, int ntasks, const SnInfo* sn, const int* rows,
+                           const T* W, const T* y, T* x, const int* perm, double* v, double* qk, const double* q,
+                           double dt, int mode, int n);
 
 // detection (detect_kernels.cu, compiled without FMA contraction)
 __global__ void k_obstacle_flags(int N, const double* q, DObstacles obs, unsigned char* flags);

@@ -460,11 +460,11 @@ __global__ void k_levels(DContacts c, int* deg, int* uf, int* dist, int* seed, i
   if (tid == 0) maxlvl = 0;
   for (int l = tid; l < cap_levels + 1; l += nth) lcount[l] = 0;
   __syncthreads();
-  for (int e = tid; e < S; e += nth) {
-    const int l = min(dist[c.s_slota[e]], dist[c.s_slotb[e]]);
-    elev[e] = l;
-    atomicMax(&maxlvl, l);
-  }
+  for (int e = tid; e < S; e += nth) elev[e] = min(dist[c.s_slota[e]], dist[c.s_slotb[e]]);
+  // the reference opens one level per breadth-first frontier, including the
+  // last frontier that finds no new edge: levels = max reached distance + 1
+  for (int s = tid; s < V; s += nth)
+    if (dist[s] < INF) atomicMax(&maxlvl, dist[s]);
   __syncthreads();
   const int nl = min(maxlvl + 1, cap_levels);
   for (int e = tid; e < S; e += nth) atomicAdd(lcount + min(elev[e], nl - 1), 1);

@@ -117,25 +117,32 @@ __global__ void k_vertex_rhs(DModel m, const double* __restrict__ qk, const doub
     }
   }
   const int64_t p = m.iperm[i];
-  b[3 * p] = (T)out.x;
-  b[3 * p + 1] = (T)out.y;
-  b[3 * p + 2] = (T)out.z;
+  b[p] = (T)out.x;
+  b[p + m.N] = (T)out.y;
+  b[p + 2 * (int64_t)m.N] = (T)out.z;
 }
 
-template __global__ void k_vertex_rhs<double>(DModel, const double*, const double*, const double*, const double*,
-                                              double, const int*, double*, double*, double, int);
-template __global__ void k_vertex_rhs<float>(DModel, const double*, const double*, const double*, const double*,
-                                             double, const int*, double*, float*, double, int);
-
-__device__ __forceinline__ void atomic_add3(double* p, double3 g) {
-  atomicAdd(p, g.x);
-  atomicAdd(p + 1, g.y);
-  atomicAdd(p + 2, g.z);
+template <typename T>
+void launch_vertex_rhs(dim3 grid, dim3 block, cudaStream_t st, DModel m, const double* qk, const double* v,
+                       const double* cstep, const double* bp, double air_damping, const int* slot_of, double* fslot,
+                       T* b, double dt, int residual_mode) {
+  k_vertex_rhs<T><<<grid, block, 0, st>>>(m, qk, v, cstep, bp, air_damping, slot_of, fslot, b, dt, residual_mode);
 }
-__device__ __forceinline__ void atomic_add3(float* p, double3 g) {
-  atomicAdd(p, (float)g.x);
-  atomicAdd(p + 1, (float)g.y);
-  atomicAdd(p + 2, (float)g.z);
+template void launch_vertex_rhs<double>(dim3, dim3, cudaStream_t, DModel, const double*, const double*, const double*,
+                                        const double*, double, const int*, double*, double*, double, int);
+template void launch_vertex_rhs<float>(dim3, dim3, cudaStream_t, DModel, const double*, const double*, const double*,
+                                       const double*, double, const int*, double*, float*, double, int);
+
+// Adds g into entry p of the three planes (stride n) of a solve vector.
+__device__ __forceinline__ void atomic_add3(double* b, int64_t p, int n, double3 g) {
+  atomicAdd(b + p, g.x);
+  atomicAdd(b + p + n, g.y);
+  atomicAdd(b + p + 2 * (int64_t)n, g.z);
+}
+__device__ __forceinline__ void atomic_add3(float* b, int64_t p, int n, double3 g) {
+  atomicAdd(b + p, (float)g.x);
+  atomicAdd(b + p + n, (float)g.y);
+  atomicAdd(b + p + 2 * (int64_t)n, (float)g.z);
 }
 
 __device__ __forceinline__ double3 basis_t(const double* B, double3 v) {
@@ -179,12 +186,17 @@ __global__ void k_friction_obstacle(DModel m, DContacts c, T* __restrict__ b, in
     const double3 r = cone_project(fl, c.c_mu[k]);
     st3(c.c_force, k, r);
     const double3 g = basis_v(B, r);
-    if (!self_mode || S == 0) atomic_add3(b + 3 * (int64_t)m.iperm[vid], g);
+    if (!self_mode || S == 0) atomic_add3(b, m.iperm[vid], m.N, g);
     if (self_mode) st3(c.cf[nxt], slot, g);
   }
 }
-template __global__ void k_friction_obstacle<double>(DModel, DContacts, double*, int, int, int);
-template __global__ void k_friction_obstacle<float>(DModel, DContacts, float*, int, int, int);
+template <typename T>
+void launch_friction_obstacle(dim3 grid, dim3 block, cudaStream_t st, DModel m, DContacts c, T* b, int self_mode,
+                              int cur, int nxt) {
+  k_friction_obstacle<T><<<grid, block, 0, st>>>(m, c, b, self_mode, cur, nxt);
+}
+template void launch_friction_obstacle<double>(dim3, dim3, cudaStream_t, DModel, DContacts, double*, int, int, int);
+template void launch_friction_obstacle<float>(dim3, dim3, cudaStream_t, DModel, DContacts, float*, int, int, int);
 
 // Self contacts (SFE:431-587).  One CTA walks the breadth-first levels in
 // order; inside a level every contact is estimated from the buffers as they
@@ -248,7 +260,7 @@ __global__ void k_friction_self(DModel m, DContacts c, T* __restrict__ b, double
     for (int s = threadIdx.x; s < ns; s += blockDim.x) {
       const double3 g = ld3(c.cf[nxt], s) + ld3(c.sf[nxt], s);
       const int64_t p = m.iperm[c.slot_vertex[s]];
-      atomic_add3(b + 3 * p, g);
+      atomic_add3(b, p, m.N, g);
     }
     __syncthreads();
   }
@@ -262,8 +274,13 @@ __global__ void k_friction_self(DModel m, DContacts c, T* __restrict__ b, double
     }
   }
 }
-template __global__ void k_friction_self<double>(DModel, DContacts, double*, double*, int, int);
-template __global__ void k_friction_self<float>(DModel, DContacts, float*, double*, int, int);
+template <typename T>
+void launch_friction_self(dim3 grid, dim3 block, cudaStream_t st, DModel m, DContacts c, T* b, double* newf, int cur,
+                          int nxt) {
+  k_friction_self<T><<<grid, block, 0, st>>>(m, c, b, newf, cur, nxt);
+}
+template void launch_friction_self<double>(dim3, dim3, cudaStream_t, DModel, DContacts, double*, double*, int, int);
+template void launch_friction_self<float>(dim3, dim3, cudaStream_t, DModel, DContacts, float*, double*, int, int);
 
 // Alart-Curnier residual with rho = 1 (coulomb_util.cpp:92-152) for every
 // contact after the solve (SFE:590-652).  acc[4] += {sum |AC|, max |AC|,

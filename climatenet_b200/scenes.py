@@ -199,7 +199,8 @@ def workload(cfg, n_override=None):
         return s, dict(time_step=2.5e-3, iterations=20, self_collision=True, self_tol=1e-3), 400
     if cfg == 3:
         n = n_override or 500
-        s = cloth_on_sphere(n=n, side=2.0, z=0.05, mu=0.5, sphere_center=(0, 0, -0.5),
+        # 5 mm above the sphere top: inside the 1 cm contact margin from step 0
+        s = cloth_on_sphere(n=n, side=2.0, z=0.005, mu=0.5, sphere_center=(0, 0, -0.5),
                             sphere_radius=0.5, rotating=1.0)
         return s, dict(time_step=2e-3, iterations=20, self_collision=True, self_tol=2e-3), 300
     if cfg == 5:
