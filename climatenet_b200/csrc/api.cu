@@ -51,42 +51,38 @@ constexpr int kThreads = 256;
 inline int blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kThreads - 1) / kThreads); }
 constexpr int kStrideBlocks = 592;  // 4 x 148 SMs for grid-stride kernels
 
-int group_size(int len) {
-  int g = 4;
-  while (g < 32 && g < len) g <<= 1;
-  return g;
-}
+// Work items of one sweep are at most 32 x kChunk elements.
+constexpr int kChunk = 256;
 
-// Level-ordered task lists of the supernodal sweeps.
+// Work-item lists of the two sweeps in elimination-tree order (forward:
+// levels bottom-up, backward: top-down), one item per tile and chunk.
 void build_schedule(pdf_handle* h) {
   const Factor& f = h->fac;
-  std::vector<std::vector<SweepTask>> fw(f.n_levels), bw(f.n_levels);
-  for (int s = 0; s < f.n_sn; ++s) {
-    const int ns = f.sn_ns[s], nr = f.sn_nr[s], L = f.sn_level[s];
-    // about two elements per lane: g = pow2 >= half the typical row/column length
-    const int gf = group_size(ns / 2);
-    const int per_f = 32 / gf;
-    for (int r = 0; r < ns + nr; r += per_f) fw[L].push_back({s, r, std::min(per_f, ns + nr - r), gf});
-    const int gb = group_size((ns / 2 + nr) / 2);
-    const int per_b = 32 / gb;
-    for (int c = 0; c < ns; c += per_b) bw[L].push_back({s, c, std::min(per_b, ns - c), gb});
-  }
   std::vector<SweepTask> fa, ba;
-  h->fwd_off.assign(1, 0);
-  h->bwd_off.assign(1, 0);
-  for (int L = 0; L < f.n_levels; ++L) {
-    fa.insert(fa.end(), fw[L].begin(), fw[L].end());
-    ba.insert(ba.end(), bw[L].begin(), bw[L].end());
-    h->fwd_off.push_back((int)fa.size());
-    h->bwd_off.push_back((int)ba.size());
-  }
-  h->d.fwd_tasks = upload(fa);
-  h->d.bwd_tasks = upload(ba);
-  std::vector<SnInfo> sn(f.n_sn);
-  for (int s = 0; s < f.n_sn; ++s) sn[s] = {f.sn_c0[s], f.sn_ns[s], f.sn_nr[s], 0, f.sn_woff[s], f.sn_roff[s]};
+  std::vector<SnInfo> sn;
+  build_sweep_tasks(f, kChunk, fa, ba, sn);
+  h->d.ftasks = upload(fa);
+  h->d.btasks = upload(ba);
+  h->d.nf = (int)fa.size();
+  h->d.nb = (int)ba.size();
   h->d.sn = upload(sn);
   h->d.rows = upload(f.rows);
   h->n_levels = f.n_levels;
+  // dependency counters start at zero, the solve counter at one
+  SweepSync& sy = h->d.sync;
+  sy.queue = dalloc<int>(2);
+  sy.epoch = dalloc<unsigned long long>(1);
+  sy.fdone = dalloc<unsigned long long>(f.n_sn);
+  sy.fchild = dalloc<unsigned long long>(f.n_sn);
+  sy.bdone = dalloc<unsigned long long>(f.n_sn);
+  sy.err = dalloc<int>(1);
+  CK(cudaMemset(sy.queue, 0, 2 * sizeof(int)));
+  const unsigned long long one = 1ULL;
+  CK(cudaMemcpy(sy.epoch, &one, sizeof(one), cudaMemcpyHostToDevice));
+  CK(cudaMemset(sy.fdone, 0, f.n_sn * sizeof(unsigned long long)));
+  CK(cudaMemset(sy.fchild, 0, f.n_sn * sizeof(unsigned long long)));
+  CK(cudaMemset(sy.bdone, 0, f.n_sn * sizeof(unsigned long long)));
+  CK(cudaMemset(sy.err, 0, sizeof(int)));
 }
 
 void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
@@ -210,19 +206,19 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   // solve
   build_schedule(h);
   if (h->fp32) {
-    std::vector<float> w(f.Wr.begin(), f.Wr.end());
-    d.Wr32 = upload(w);
-    std::vector<float> wc(f.Wc.begin(), f.Wc.end());
-    d.Wc32 = upload(wc);
+    d.Wf32 = upload(std::vector<float>(f.Wf.begin(), f.Wf.end()));
+    d.Wb32 = upload(std::vector<float>(f.Wb.begin(), f.Wb.end()));
     d.b32 = dalloc<float>(3 * (size_t)N);
     d.y32 = dalloc<float>(3 * (size_t)N);
     d.x32 = dalloc<float>(3 * (size_t)N);
+    launch_solve_prep<float>(h->stream, N, d.x32, d.y32, d.sync);
   } else {
-    d.Wr64 = upload(f.Wr);
-    d.Wc64 = upload(f.Wc);
+    d.Wf64 = upload(f.Wf);
+    d.Wb64 = upload(f.Wb);
     d.b64 = dalloc<double>(3 * (size_t)N);
     d.y64 = dalloc<double>(3 * (size_t)N);
     d.x64 = dalloc<double>(3 * (size_t)N);
+    launch_solve_prep<double>(h->stream, N, d.x64, d.y64, d.sync);
   }
   // contacts
   const int nobs = std::max(1, h->obs.n);
@@ -311,28 +307,19 @@ void launch_local(pdf_handle* h, T* b, int mode) {
                        std::max(h->prm.air_damping, 0.), d.c.slot_of, d.c.f, b, h->prm.time_step, mode);
 }
 
-// Global solve: forward sweep over the levels bottom-up, backward top-down.
+// Global solve: one persistent forward and one backward sweep, then the
+// write-back of v and q^k (which also clears x, y for the next solve).
 template <typename T>
-void launch_solve(pdf_handle* h, T* b, T* y, T* x, const T* Wr, const T* Wc, int mode) {
+void launch_solve(pdf_handle* h, T* b, T* y, T* x, const T* Wf, const T* Wb, int mode) {
   DeviceBuffers& d = h->d;
-  cudaStream_t st = h->stream;
-  for (int L = 0; L < h->n_levels; ++L) {
-    const int nt = h->fwd_off[L + 1] - h->fwd_off[L];
-    if (nt == 0) continue;
-    launch_sweep_forward<T>(st, d.fwd_tasks + h->fwd_off[L], nt, d.sn, d.rows, Wr, b, y, h->dm.N);
-  }
-  for (int L = h->n_levels - 1; L >= 0; --L) {
-    const int nt = h->bwd_off[L + 1] - h->bwd_off[L];
-    if (nt == 0) continue;
-    launch_sweep_backward<T>(st, d.bwd_tasks + h->bwd_off[L], nt, d.sn, d.rows, Wc, y, x, d.perm, d.v, d.qk, d.q,
-                             h->prm.time_step, mode, h->dm.N);
-  }
+  launch_solve_sweeps<T>(h->stream, d.ftasks, d.nf, d.btasks, d.nb, d.sn, d.rows, Wf, Wb, b, y, x, h->dm.N, d.sync);
+  launch_solve_post<T>(h->stream, h->dm.N, d.perm, x, y, d.v, d.qk, d.q, h->prm.time_step, mode, d.sync);
 }
 
 // One PD iteration (SimulationBase.cpp:119-157): local step + friction
 // (SFE::computeRhs), global solve (SimulationSpeed::solve), AC residual.
 template <typename T>
-void launch_iteration(pdf_handle* h, int k, T* b, T* y, T* x, const T* Wr, const T* Wc, int mode) {
+void launch_iteration(pdf_handle* h, int k, T* b, T* y, T* x, const T* Wf, const T* Wb, int mode) {
   DeviceBuffers& d = h->d;
   const DModel& dm = h->dm;
   cudaStream_t st = h->stream;
@@ -341,18 +328,14 @@ void launch_iteration(pdf_handle* h, int k, T* b, T* y, T* x, const T* Wr, const
   launch_local<T>(h, b, mode);
   launch_friction_obstacle<T>(kStrideBlocks, kThreads, st, dm, d.c, b, self_mode, cur, nxt);
   if (self_mode) launch_friction_self<T>(1, 1024, st, dm, d.c, b, d.newf, cur, nxt);
-  launch_solve<T>(h, b, y, x, Wr, Wc, mode);
+  launch_solve<T>(h, b, y, x, Wf, Wb, mode);
   k_alart_curnier<<<kStrideBlocks, kThreads, 0, st>>>(d.c, d.v, d.ac_hist + 4 * (size_t)k);
 }
 
-// Kernels of this library launched by one PD iteration (CUB's not counted).
+// Kernels of this library launched by one PD iteration (CUB's not counted):
+// [bending], vertex rhs, friction, [self friction], forward, backward, post, AC.
 int64_t launches_per_iteration(const pdf_handle* h) {
-  int64_t n = 3 + (h->dm.B > 0 ? 1 : 0) + (h->prm.self_collision ? 1 : 0);
-  for (int L = 0; L < h->n_levels; ++L) {
-    n += (h->fwd_off[L + 1] > h->fwd_off[L]) ? 1 : 0;
-    n += (h->bwd_off[L + 1] > h->bwd_off[L]) ? 1 : 0;
-  }
-  return n;
+  return 6 + (h->dm.B > 0 ? 1 : 0) + (h->prm.self_collision ? 1 : 0);
 }
 
 // Per step outside the iterations: predictor, obstacle flags + materialise,
@@ -368,9 +351,9 @@ void launch_iterations(pdf_handle* h, int k0, int k1) {
   DeviceBuffers& d = h->d;
   for (int k = k0; k < k1; ++k) {
     if (h->fp32)
-      launch_iteration<float>(h, k, d.b32, d.y32, d.x32, d.Wr32, d.Wc32, 1);
+      launch_iteration<float>(h, k, d.b32, d.y32, d.x32, d.Wf32, d.Wb32, 1);
     else
-      launch_iteration<double>(h, k, d.b64, d.y64, d.x64, d.Wr64, d.Wc64, 0);
+      launch_iteration<double>(h, k, d.b64, d.y64, d.x64, d.Wf64, d.Wb64, 0);
   }
 }
 
@@ -505,8 +488,9 @@ void free_handle(pdf_handle* h) {
   DeviceBuffers& d = h->d;
   void* ptrs[] = {d.mass, d.ring_kappa, d.ring_bend, d.self_bend, d.ring_ptr, d.ring_idx, d.bend_of, d.bend_ptr,
                   d.bend_idx, d.bend_coef, d.bend_w, d.bend_rest, d.pin_term, d.ata_ptr, d.ata_col, d.ata_val,
-                  d.perm, d.iperm, d.vmat, d.friction, d.tris, d.q, d.v, d.tn, d.qk, d.cstep, d.bp, d.fwd_tasks,
-                  d.bwd_tasks, d.sn, d.rows, d.Wr64, d.Wc64, d.Wr32, d.Wc32, d.b64, d.y64, d.x64, d.b32, d.y32,
+                  d.perm, d.iperm, d.vmat, d.friction, d.tris, d.q, d.v, d.tn, d.qk, d.cstep, d.bp, d.ftasks,
+                  d.btasks, d.sn, d.rows, d.Wf64, d.Wb64, d.Wf32, d.Wb32, d.sync.queue, d.sync.epoch,
+                  d.sync.fdone, d.sync.fchild, d.sync.bdone, d.sync.err, d.b64, d.y64, d.x64, d.b32, d.y32,
                   d.x32, d.flags, d.sel_idx, d.cub_tmp, d.newf, d.ac_hist, d.c.n_contacts, d.c.c_vertex,
                   d.c.c_normal, d.c.c_speed, d.c.c_mu, d.c.c_basis, d.c.c_force, d.c.c_ac, d.c.c_slot, d.c.n_self,
                   d.c.s_vertex, d.c.s_partner, d.c.s_face, d.c.s_normal, d.c.s_mu, d.c.s_basis, d.c.s_force,
@@ -590,6 +574,9 @@ int pdf_step(pdf_handle* h, int32_t nsteps, pdf_step_report* report) {
     CK(cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]));
     h->last.device_ms = ms;
     if (report) *report = h->last;
+    int derr = 0;
+    CK(cudaMemcpy(&derr, h->d.sync.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (derr) return fail(h, PDF_DEVICE_TIMEOUT, "a supernodal sweep gave up waiting for a dependency");
     return PDF_OK;
   });
 }
@@ -607,8 +594,10 @@ int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms_out, d
     double bytes = 0;
     int64_t idx_rows = (int64_t)f.rows.size();
     if (phase == 0) {
-      // 2 [l s + idx_bytes(L)] + 2 (2 * 3 s N) + FP64 epilogue (q read; v, q^k written)
-      bytes = 2. * ((double)f.nnz_w * s + 4. * (double)idx_rows) + 2. * (2. * 3. * s * N) + 72. * N;
+      // 2 [l s + idx_bytes(L)] + 2 (2 * 3 s N) + FP64 write-back (q read; v, q^k
+      // written), with l = structural nnz(L) (padding and explicit zeros of the
+      // stored tiles are not counted)
+      bytes = 2. * ((double)f.nnz_l_true * s + 4. * (double)idx_rows) + 2. * (2. * 3. * s * N) + 72. * N;
     } else if (phase == 1) {
       // 4*3sN + E (8 + s) + sum_b [(r_b + 1)(4 + s) + s], s = 8 (FP64 local step)
       const double E = (double)h->model.ring_idx.size() / 2.;
@@ -643,9 +632,9 @@ int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms_out, d
       CK(cudaEventRecord(h->ev[5], st));
       if (phase == 0) {
         if (h->fp32)
-          launch_solve<float>(h, d.b32, d.y32, d.x32, d.Wr32, d.Wc32, 1);
+          launch_solve<float>(h, d.b32, d.y32, d.x32, d.Wf32, d.Wb32, 1);
         else
-          launch_solve<double>(h, d.b64, d.y64, d.x64, d.Wr64, d.Wc64, 0);
+          launch_solve<double>(h, d.b64, d.y64, d.x64, d.Wf64, d.Wb64, 0);
       } else if (phase == 1) {
         if (h->fp32)
           launch_local<float>(h, d.b32, 1);
@@ -825,6 +814,23 @@ int pdf_get_residual_history(pdf_handle* h, double* out, int32_t cap, int32_t* n
 }
 
 void pdf_destroy(pdf_handle* h) { free_handle(h); }
+
+int pdf_factor_check(const pdf_scene_desc* scene, const pdf_params* params, const double* b, double* x) {
+  if (!scene || !params || !b || !x) return fail(nullptr, PDF_INVALID_ARG, "null argument");
+  try {
+    Model m;
+    build_model(*scene, *params, m);
+    Factor f;
+    std::string err;
+    if (!factorize(m, params->time_step, 40, f, err)) return fail(nullptr, PDF_NOT_SPD, err);
+    std::vector<double> bv(b, b + 3 * (size_t)m.N), xv;
+    if (!emulate_sweeps(f, kChunk, bv, xv, err)) return fail(nullptr, PDF_INVALID_ARG, err);
+    std::copy(xv.begin(), xv.end(), x);
+  } catch (const std::exception& e) {
+    return fail(nullptr, PDF_INVALID_ARG, e.what());
+  }
+  return PDF_OK;
+}
 
 int pdf_detect_candidates(const double* positions, int32_t n_vertices, const int32_t* triangles, int32_t n_triangles,
                           double tolerance, int32_t* pairs, int32_t cap, int32_t* n, int32_t device) {

@@ -156,8 +156,7 @@ bool factorize(const Model& m, double dt, int leaf_size, Factor& f, std::string&
   f.nnz_w = f.sn_woff[S];
   f.rows.resize(f.sn_roff[S]);
   for (int s = 0; s < S; ++s) std::copy(R[s].begin(), R[s].end(), f.rows.begin() + f.sn_roff[s]);
-  f.Wr.assign(f.nnz_w, 0.);
-  f.Wc.assign(f.nnz_w, 0.);
+  std::vector<double> Wr(f.nnz_w, 0.);  // packed row-major W_s (intermediate)
 
   // ---- numeric: multifrontal, level by level ---------------------------
   const double dt2 = std::pow(dt, 2);
@@ -242,20 +241,13 @@ bool factorize(const Model& m, double dt, int leaf_size, Factor& f, std::string&
     // row-major copy: rows i < ns hold X[i][0..i]; rows ns+r hold P[r][0..ns)
 #pragma omp parallel for schedule(dynamic, 8) if (inner_parallel)
     for (int i = 0; i < mdim; ++i) {
-      double* wr = &f.Wr[wo + w_rowstart(i, ns)];
+      double* wr = &Wr[wo + w_rowstart(i, ns)];
       if (i < ns) {
         for (int j = 0; j <= i; ++j) wr[j] = X[(size_t)j * ns + i];
       } else {
         const double* Fi = &F[(size_t)i * mdim];
         for (int j = 0; j < ns; ++j) wr[j] = dotn(Fi + j, &X[(size_t)j * ns + j], ns - j);
       }
-    }
-    // column-major copy from the row-major one
-#pragma omp parallel for schedule(dynamic, 8) if (inner_parallel)
-    for (int j = 0; j < ns; ++j) {
-      double* wc = &f.Wc[wo + w_colstart(j, ns, nr)];
-      for (int i = j; i < ns; ++i) wc[i - j] = f.Wr[wo + w_rowstart(i, ns) + j];
-      for (int r = 0; r < nr; ++r) wc[ns - j + r] = f.Wr[wo + w_rowstart(ns + r, ns) + j];
     }
   };
 
@@ -274,6 +266,56 @@ bool factorize(const Model& m, double dt, int leaf_size, Factor& f, std::string&
   if (failed) {
     err = "global-step matrix M + dt^2 A^T A is not positive definite";
     return false;
+  }
+  // ---- tiled copies for the device sweeps (layout in factor.hpp) --------
+  f.sn_btile0.assign(S + 1, 0);
+  for (int s = 0; s < S; ++s) f.sn_btile0[s + 1] = f.sn_btile0[s] + (f.sn_ns[s] + kTile - 1) / kTile;
+  {
+    // forward tiles cover rows of W_s (ns + nr rows): more tiles than the
+    // backward ones (ns columns); give every supernode both counts
+    std::vector<int64_t> ft0(S + 1, 0);
+    for (int s = 0; s < S; ++s) ft0[s + 1] = ft0[s] + (f.sn_ns[s] + f.sn_nr[s] + kTile - 1) / kTile;
+    const int64_t nft = ft0[S], nbt = f.sn_btile0[S];
+    f.ftile_off.assign(nft + 1, 0);
+    f.btile_off.assign(nbt + 1, 0);
+    for (int s = 0; s < S; ++s) {
+      const int64_t ns = f.sn_ns[s], nr = f.sn_nr[s];
+      for (int64_t t = 0; t < ft0[s + 1] - ft0[s]; ++t) {
+        const int64_t w = std::min(ns, kTile * t + kTile);
+        f.ftile_off[ft0[s] + t + 1] = f.ftile_off[ft0[s] + t] + kTile * w;
+      }
+      for (int64_t t = 0; t < f.sn_btile0[s + 1] - f.sn_btile0[s]; ++t) {
+        const int64_t hgt = ns - kTile * t + nr;
+        f.btile_off[f.sn_btile0[s] + t + 1] = f.btile_off[f.sn_btile0[s] + t] + kTile * hgt;
+      }
+    }
+    f.sn_ftile0 = ft0;
+    f.Wf.assign(f.ftile_off[nft], 0.);
+    f.Wb.assign(f.btile_off[nbt], 0.);
+    f.tiled_w = std::max(f.ftile_off[nft], f.btile_off[nbt]);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int s = 0; s < S; ++s) {
+      const int64_t ns = f.sn_ns[s], nr = f.sn_nr[s], wo = f.sn_woff[s];
+      auto wval = [&](int64_t i, int64_t j) -> double {  // W_s(i, j), zero above D^-1's diagonal
+        if (i < ns) return j <= i ? Wr[wo + w_rowstart(i, ns) + j] : 0.;
+        if (i < ns + nr) return Wr[wo + w_rowstart(i, ns) + j];
+        return 0.;
+      };
+      for (int64_t t = 0; t < ft0[s + 1] - ft0[s]; ++t) {
+        double* T = &f.Wf[f.ftile_off[ft0[s] + t]];
+        const int64_t w = std::min(ns, kTile * t + kTile);
+        for (int64_t j = 0; j < w; ++j)
+          for (int64_t l = 0; l < kTile; ++l) T[kTile * j + l] = wval(kTile * t + l, j);
+      }
+      for (int64_t t = 0; t < f.sn_btile0[s + 1] - f.sn_btile0[s]; ++t) {
+        double* T = &f.Wb[f.btile_off[f.sn_btile0[s] + t]];
+        const int64_t j0 = kTile * t, hgt = ns - j0 + nr;
+        for (int64_t i = 0; i < hgt; ++i) {
+          const int64_t row = i < ns - j0 ? j0 + i : ns + (i - (ns - j0));
+          for (int64_t l = 0; l < kTile; ++l) T[kTile * i + l] = (j0 + l < ns) ? wval(row, j0 + l) : 0.;
+        }
+      }
+    }
   }
   // structural nnz(L): sum over rows k of |reach of A(0:k, k) in the
   // elimination tree| plus the diagonal (row-subtree counting)
@@ -308,6 +350,112 @@ bool factorize(const Model& m, double dt, int leaf_size, Factor& f, std::string&
   }
   f.nnz_l_true = nnz_true;
   f.factor_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_start).count();
+  return true;
+}
+
+void build_sweep_tasks(const Factor& f, int chunk, std::vector<SweepTask>& fa, std::vector<SweepTask>& ba,
+                       std::vector<SnInfo>& sn) {
+  std::vector<std::vector<int>> by_level(f.n_levels);
+  for (int s = 0; s < f.n_sn; ++s) by_level[f.sn_level[s]].push_back(s);
+  sn.assign(f.n_sn, SnInfo{});
+  for (int s = 0; s < f.n_sn; ++s) {
+    sn[s].c0 = f.sn_c0[s];
+    sn[s].ns = f.sn_ns[s];
+    sn[s].nr = f.sn_nr[s];
+    sn[s].parent = f.sn_parent[s];
+    sn[s].roff = f.sn_roff[s];
+  }
+  for (int s = 0; s < f.n_sn; ++s)
+    if (f.sn_parent[s] >= 0) sn[f.sn_parent[s]].nchild++;
+  fa.clear();
+  ba.clear();
+  for (int L = 0; L < f.n_levels; ++L)
+    for (int s : by_level[L]) {
+      const int ns = f.sn_ns[s];
+      for (int64_t t = f.sn_ftile0[s]; t < f.sn_ftile0[s + 1]; ++t) {
+        const int tl = (int)(t - f.sn_ftile0[s]);
+        const int w = std::min(ns, kTile * tl + kTile);
+        for (int a = 0; a < w; a += chunk) fa.push_back({s, tl, a, std::min(w, a + chunk), f.ftile_off[t]});
+      }
+    }
+  for (int L = f.n_levels - 1; L >= 0; --L)
+    for (int s : by_level[L]) {
+      const int ns = f.sn_ns[s], nr = f.sn_nr[s];
+      for (int64_t t = f.sn_btile0[s]; t < f.sn_btile0[s + 1]; ++t) {
+        const int tl = (int)(t - f.sn_btile0[s]);
+        const int hgt = ns - kTile * tl + nr;
+        for (int a = 0; a < hgt; a += chunk) ba.push_back({s, tl, a, std::min(hgt, a + chunk), f.btile_off[t]});
+      }
+    }
+  for (const auto& t : fa) sn[t.sn].ntf++;
+  for (const auto& t : ba) sn[t.sn].ntb++;
+}
+
+bool emulate_sweeps(const Factor& f, int chunk, const std::vector<double>& bin, std::vector<double>& xout,
+                    std::string& err) {
+  const int64_t n = f.N;
+  std::vector<SweepTask> fa, ba;
+  std::vector<SnInfo> sn;
+  build_sweep_tasks(f, chunk, fa, ba, sn);
+  std::vector<double> b(3 * n), y(3 * n, 0.), x(3 * n, 0.);
+  for (int64_t k = 0; k < n; ++k)
+    for (int c = 0; c < 3; ++c) b[k + c * n] = bin[3 * (size_t)f.perm[k] + c];
+  auto chk = [&](int64_t i, int64_t lim, const char* what) {
+    if (i < 0 || i >= lim) {
+      err = std::string("index out of range in ") + what;
+      return false;
+    }
+    return true;
+  };
+  const int64_t nWf = (int64_t)f.Wf.size(), nWb = (int64_t)f.Wb.size(), nrows = (int64_t)f.rows.size();
+  for (const SweepTask& tk : fa) {
+    const SnInfo& s = sn[tk.sn];
+    for (int l = 0; l < kTile; ++l) {
+      const int row = tk.tile * kTile + l;
+      double acc[3] = {0, 0, 0};
+      for (int j = tk.a0; j < tk.a1; ++j) {
+        const int64_t wi = tk.off + (int64_t)j * kTile + l;
+        if (!chk(wi, nWf, "forward tile") || !chk(s.c0 + j, n, "forward vector")) return false;
+        for (int c = 0; c < 3; ++c) acc[c] += f.Wf[wi] * b[s.c0 + j + c * n];
+      }
+      if (row < s.ns) {
+        for (int c = 0; c < 3; ++c) y[s.c0 + row + c * n] += acc[c];
+      } else if (row < s.ns + s.nr) {
+        if (!chk(s.roff + row - s.ns, nrows, "forward rows")) return false;
+        const int64_t r = f.rows[s.roff + row - s.ns];
+        if (!chk(r, n, "forward scatter")) return false;
+        for (int c = 0; c < 3; ++c) b[r + c * n] -= acc[c];
+      }
+    }
+  }
+  for (const SweepTask& tk : ba) {
+    const SnInfo& s = sn[tk.sn];
+    const int j0t = tk.tile * kTile, nd = s.ns - j0t;
+    for (int l = 0; l < kTile; ++l) {
+      const int col = j0t + l;
+      double acc[3] = {0, 0, 0};
+      for (int i = tk.a0; i < tk.a1; ++i) {
+        const int64_t wi = tk.off + (int64_t)i * kTile + l;
+        if (!chk(wi, nWb, "backward tile")) return false;
+        double v[3];
+        if (i < nd) {
+          if (!chk(s.c0 + j0t + i, n, "backward y")) return false;
+          for (int c = 0; c < 3; ++c) v[c] = y[s.c0 + j0t + i + c * n];
+        } else {
+          if (!chk(s.roff + i - nd, nrows, "backward rows")) return false;
+          const int64_t r = f.rows[s.roff + i - nd];
+          if (!chk(r, n, "backward gather")) return false;
+          for (int c = 0; c < 3; ++c) v[c] = -x[r + c * n];
+        }
+        for (int c = 0; c < 3; ++c) acc[c] += f.Wb[wi] * v[c];
+      }
+      if (col < s.ns)
+        for (int c = 0; c < 3; ++c) x[s.c0 + col + c * n] += acc[c];
+    }
+  }
+  xout.assign(3 * n, 0.);
+  for (int64_t k = 0; k < n; ++k)
+    for (int c = 0; c < 3; ++c) xout[3 * (size_t)f.perm[k] + c] = x[k + c * n];
   return true;
 }
 

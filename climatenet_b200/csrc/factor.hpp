@@ -17,9 +17,15 @@
 //    b_R -= (L_R D^-1) b_s and the backward sweep x_s = W_s^T [y_s ; -x_R]:
 //    both are plain matrix-vector products with no dependency inside a
 //    supernode, so a supernode can be split across any number of warps.
-//  * W_s is stored twice: row-major (forward, one warp group per row) and
-//    column-major (backward, one warp group per column); each sweep reads its
-//    copy exactly once with coalesced loads.
+//  * W_s is stored twice in 32-lane tiles, one copy per sweep, so that a warp
+//    streams a tile with one coalesced 32-element load per step:
+//      forward tile t  = rows [32t, 32t+32) of W_s, columns 0..w_t-1
+//                        (w_t = min(ns, 32t+32): the zero upper part of D^-1
+//                        is not stored beyond the tile's diagonal block);
+//                        element (row 32t+l, col j) at off + 32 j + l;
+//      backward tile t = columns [32t, 32t+32) of W_s, rows 32t..ns-1 of D^-1
+//                        then the nr rows of L_R D^-1 (h_t = ns - 32t + nr);
+//                        element (local row i, col 32t+l) at off + 32 i + l.
 #pragma once
 #include <cstdint>
 #include <string>
@@ -29,6 +35,8 @@
 
 namespace pdfb {
 
+constexpr int kTile = 32;
+
 struct Factor {
   int N = 0;
   std::vector<int> perm, iperm;  // perm[k] = vertex at pivot position k
@@ -36,16 +44,48 @@ struct Factor {
   std::vector<int> sn_c0, sn_ns, sn_nr, sn_parent, sn_level;
   std::vector<int64_t> sn_roff;  // offset into rows
   std::vector<int> rows;         // R_s, permuted indices, ascending
-  std::vector<int64_t> sn_woff;  // offset of W_s (same for both copies)
-  std::vector<double> Wr, Wc;    // packed W_s, row-major / column-major
+  std::vector<int64_t> sn_woff;  // offset of W_s in the packed row-major form
+  // tiled copies (see above); forward tiles of supernode s are
+  // [sn_ftile0[s], sn_ftile0[s+1]), backward tiles [sn_btile0[s], sn_btile0[s+1])
+  std::vector<int64_t> sn_ftile0, sn_btile0;
+  std::vector<int64_t> ftile_off, btile_off;  // per tile, +1 sentinel
+  std::vector<double> Wf, Wb;
   int n_levels = 0;
   int64_t nnz_w = 0;             // sum ns(ns+1)/2 + nr ns
   int64_t nnz_l_true = 0;        // structural nnz of L (diagonal included)
+  int64_t tiled_w = 0;           // stored elements per tiled copy (with padding)
   double factor_ms = 0;
 };
 
 // Returns false (and sets err) if the matrix is not positive definite.
 bool factorize(const Model& m, double dt, int leaf_size, Factor& f, std::string& err);
+
+// One warp's work item of a supernodal sweep: tile `tile` of supernode `sn`
+// (rows 32 tile.. of W_s for the forward sweep, columns for the backward one),
+// restricted to the chunk [a0, a1) of columns (forward) or local rows
+// (backward); `off` is the tile's offset in the tiled W copy.
+struct SweepTask {
+  int sn, tile, a0, a1;
+  int64_t off;
+};
+struct SnInfo {
+  int c0, ns, nr, parent;
+  int64_t roff;
+  int nchild, ntf, ntb, pad;  // children, forward / backward work items
+};
+
+// Work items of both sweeps in elimination-tree order (forward: levels
+// bottom-up; backward: top-down), at most 32 x chunk elements each, and the
+// per-supernode dependency record.
+void build_sweep_tasks(const Factor& f, int chunk, std::vector<SweepTask>& fwd, std::vector<SweepTask>& bwd,
+                       std::vector<SnInfo>& sn);
+
+// Host emulation of the two device sweeps on the tiled layout (same work
+// items, same index arithmetic, every index bounds-checked): solves
+// (M + dt^2 A^T A) x = b for three right-hand sides given vertex-major (3N),
+// result vertex-major.  Returns false with err on an out-of-range index.
+bool emulate_sweeps(const Factor& f, int chunk, const std::vector<double>& b, std::vector<double>& x,
+                    std::string& err);
 
 // W column offset inside a supernode: column j starts at colstart(j).
 inline int64_t w_colstart(int64_t j, int64_t ns, int64_t nr) { return j * (ns + nr) - j * (j - 1) / 2; }

@@ -28,11 +28,13 @@ struct DeviceBuffers {
   // state
   double *q = nullptr, *v = nullptr, *tn = nullptr, *qk = nullptr, *cstep = nullptr, *bp = nullptr;
   // solve
-  SweepTask *fwd_tasks = nullptr, *bwd_tasks = nullptr;
+  SweepTask *ftasks = nullptr, *btasks = nullptr;
+  int nf = 0, nb = 0;  // work items per sweep
   SnInfo* sn = nullptr;
   int* rows = nullptr;
-  double *Wr64 = nullptr, *Wc64 = nullptr;
-  float *Wr32 = nullptr, *Wc32 = nullptr;
+  double *Wf64 = nullptr, *Wb64 = nullptr;  // tiled factor copies (forward / backward)
+  float *Wf32 = nullptr, *Wb32 = nullptr;
+  SweepSync sync{};
   double *b64 = nullptr, *y64 = nullptr, *x64 = nullptr;
   float *b32 = nullptr, *y32 = nullptr, *x32 = nullptr;
   // contacts
@@ -60,7 +62,6 @@ struct pdf_handle {
   cudaEvent_t ev[8] = {};
   cudaGraphExec_t graph = nullptr;
   int graph_iters = 0;
-  std::vector<int> fwd_off, bwd_off;  // task offsets per level
   int n_levels = 0;
   int cap_contacts = 0, cap_self = 0;
   double time = 0.;

@@ -4,17 +4,18 @@
 #include <cuda_runtime.h>
 
 #include "device.cuh"
+#include "factor.hpp"
 
 namespace pdfb {
 
-// One warp's share of a supernodal sweep: `count` consecutive rows (forward)
-// or columns (backward) starting at `first`, g lanes per row/column.
-struct SweepTask {
-  int sn, first, count, g;
-};
-struct SnInfo {
-  int c0, ns, nr, pad;
-  int64_t woff, roff;
+// Work queues (2 ints), solve counter and cumulative completion counters.
+struct SweepSync {
+  int* queue;
+  unsigned long long* epoch;
+  unsigned long long* fdone;   // per supernode: forward work items finished
+  unsigned long long* fchild;  // per supernode: children whose forward finished
+  unsigned long long* bdone;   // per supernode: backward work items finished
+  int* err;                    // set when a dependency wait gives up
 };
 
 // Analytic and mesh obstacles, passed by value.
@@ -53,14 +54,16 @@ template <typename T>
 void launch_friction_self(dim3 grid, dim3 block, cudaStream_t st, DModel m, DContacts c, T* b, double* newf, int cur,
                           int nxt);
 // Solve vectors b, y, x are three planes of n values (x, y, z components) in
-// pivot order.
+// pivot order.  y and x must be zero before a solve (k_solve_post / prep).
 template <typename T>
-void launch_sweep_forward(cudaStream_t st, const SweepTask* tasks, int ntasks, const SnInfo* sn, const int* rows,
-                          const T* W, T* b, T* y, int n);
+void launch_solve_sweeps(cudaStream_t st, const SweepTask* ftasks, int nf, const SweepTask* btasks, int nb,
+                         const SnInfo* sn, const int* rows, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
+                         SweepSync sy);
 template <typename T>
-void launch_sweep_backward(cudaStream_t st, const SweepTask* tasks, int ntasks, const SnInfo* sn, const int* rows,
-                           const T* W, const T* y, T* x, const int* perm, double* v, double* qk, const double* q,
-                           double dt, int mode, int n);
+void launch_solve_post(cudaStream_t st, int n, const int* perm, T* x, T* y, double* v, double* qk, const double* q,
+                       double dt, int mode, SweepSync sy);
+template <typename T>
+void launch_solve_prep(cudaStream_t st, int n, T* x, T* y, SweepSync sy);
 
 // detection (detect_kernels.cu, compiled without FMA contraction)
 __global__ void k_obstacle_flags(int N, const double* q, DObstacles obs, unsigned char* flags);

@@ -1,19 +1,26 @@
-// sweep_kernels.cu — level-scheduled supernodal triangular sweeps for three
-// right-hand sides (x, y, z), replacing the three Eigen::SimplicialLLT::solve
-// calls of SimulationSpeed::solve (src/physics/SimulationSpeed.cpp:171-187).
+// sweep_kernels.cu — supernodal triangular sweeps for three right-hand sides
+// (x, y, z), replacing the three Eigen::SimplicialLLT::solve calls of
+// SimulationSpeed::solve (src/physics/SimulationSpeed.cpp:171-187).
 //
 // Each supernode s (columns [c0, c0+ns), rows R_s) carries
-// W_s = [D^-1 ; L_R D^-1] (see factor.hpp).  A sweep over one elimination-tree
-// level is one launch; a warp owns a task of consecutive rows (forward) or
-// columns (backward) of one supernode, with g lanes cooperating on each
-// row/column so that short rows do not idle a whole warp.  Warps walk the
-// level's task list with a grid stride, so the grid stays a few CTAs per SM.
-//   forward : y_s = D^-1 b_s ; b_R -= (L_R D^-1) b_s      (atomics into b_R)
-//   backward: x_s = W_s^T [y_s ; -x_R]                    (gather from ancestors)
-// Both read their copy of W once, coalesced (row-major for forward,
-// column-major for backward).  The three right-hand sides are stored as three
-// planes of n values (structure of arrays), so every vector access of a lane
-// group is contiguous.
+// W_s = [D^-1 ; L_R D^-1] (see factor.hpp) in 32-lane tiles.  A sweep is ONE
+// persistent launch: warps take work items from a queue in elimination-tree
+// order and wait (bounded spin) only for the supernodes they depend on, so
+// independent subtrees and tree levels overlap instead of being separated by
+// kernel boundaries.
+//   forward : y_s = D^-1 b_s ; b_R -= (L_R D^-1) b_s   (a work item: one row tile
+//             x one column chunk; partial sums land in y / b_R with atomics);
+//             s may start once all its children are complete.
+//   backward: x_s = W_s^T [y_s ; -x_R]                 (a work item: one column
+//             tile x one row chunk; partial sums land in x with atomics);
+//             s may start once its parent is complete.
+// Every element of W is read once per sweep with one coalesced 32-lane load;
+// the vector entries a tile needs are loaded 32 at a time and broadcast by
+// warp shuffles.  Vectors that other warps update during the sweep are read
+// through L2 (ld.global.cg) so that no stale L1 line is used.
+// Completion counters are cumulative over solves: supernode s has finished
+// solve number e when its counter reaches e * (work items of s).  A wait that
+// exceeds kMaxSpins sets the error flag and gives up instead of hanging.
 #include <cuda_runtime.h>
 
 #include "device.cuh"
@@ -21,159 +28,247 @@
 
 namespace pdfb {
 
-template <typename T>
-__device__ __forceinline__ void group_reduce(T& a, T& b, T& c, int g) {
-  for (int o = g >> 1; o > 0; o >>= 1) {
-    a += __shfl_xor_sync(0xffffffffu, a, o);
-    b += __shfl_xor_sync(0xffffffffu, b, o);
-    c += __shfl_xor_sync(0xffffffffu, c, o);
+constexpr int kMaxSpins = 1 << 22;
+
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long* p) {
+  return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+
+__device__ __forceinline__ float ldcg(const float* p) { return __ldcg(p); }
+__device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
+
+// lane 0 waits until *ctr >= target; false (and error flag set) on timeout
+__device__ __forceinline__ bool wait_counter(const unsigned long long* ctr, unsigned long long target, int* err) {
+  int spins = 0;
+  while (ld_volatile_u64(ctr) < target) {
+    if (++spins > kMaxSpins) {
+      atomicExch(err, 1);
+      return false;
+    }
+    __nanosleep(64);
   }
+  __threadfence();
+  return true;
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_sweep_forward(const SweepTask* __restrict__ tasks, int ntasks,
                                                        const SnInfo* __restrict__ sn, const int* __restrict__ rows,
-                                                       const T* __restrict__ W, T* __restrict__ b,
-                                                       T* __restrict__ y, int n) {
+                                                       const T* __restrict__ W, T* b, T* y, int n, SweepSync sy) {
   const int lane = threadIdx.x & 31;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < ntasks; w += nwarps) {
-    const SweepTask t = tasks[w];
-    const SnInfo s = sn[t.sn];
-    const int g = t.g;
-    const int grp = lane / g, sub = lane % g;
-    const int row = t.first + grp;
-    const bool active = grp < t.count;
+  const unsigned long long ep = *reinterpret_cast<const volatile unsigned long long*>(sy.epoch);
+  while (true) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(sy.queue + 0, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= ntasks) return;
+    const SweepTask tk = tasks[t];
+    const SnInfo s = sn[tk.sn];
+    int ok = 1;
+    if (lane == 0 && s.nchild > 0) ok = wait_counter(sy.fchild + tk.sn, ep * (unsigned long long)s.nchild, sy.err);
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    const int row = tk.tile * kTile + lane;
     T ax = 0, ay = 0, az = 0;
-    if (active) {
-      const int len = row < s.ns ? row + 1 : s.ns;
-      const int64_t base = s.woff + (row < s.ns ? (int64_t)row * (row + 1) / 2
-                                                : (int64_t)s.ns * (s.ns + 1) / 2 + (int64_t)(row - s.ns) * s.ns);
-      const T* wr = W + base;
+    if (ok) {
       const T* bx = b + s.c0;
       const T* by = bx + n;
       const T* bz = by + n;
-      int j = sub;
-      for (; j + 3 * g < len; j += 4 * g) {
-        const T w0 = wr[j], w1 = wr[j + g], w2 = wr[j + 2 * g], w3 = wr[j + 3 * g];
-        ax += w0 * bx[j] + w1 * bx[j + g] + w2 * bx[j + 2 * g] + w3 * bx[j + 3 * g];
-        ay += w0 * by[j] + w1 * by[j + g] + w2 * by[j + 2 * g] + w3 * by[j + 3 * g];
-        az += w0 * bz[j] + w1 * bz[j + g] + w2 * bz[j + 2 * g] + w3 * bz[j + 3 * g];
+      for (int j0 = tk.a0; j0 < tk.a1; j0 += 32) {
+        const int jl = j0 + lane;
+        T vx = 0, vy = 0, vz = 0;
+        if (jl < tk.a1) {
+          vx = ldcg(bx + jl);
+          vy = ldcg(by + jl);
+          vz = ldcg(bz + jl);
+        }
+        const int m = min(32, tk.a1 - j0);
+        const T* wp = W + tk.off + (int64_t)j0 * kTile + lane;
+        int u = 0;
+        for (; u + 4 <= m; u += 4) {
+          const T w0 = __ldg(wp + u * kTile), w1 = __ldg(wp + (u + 1) * kTile);
+          const T w2 = __ldg(wp + (u + 2) * kTile), w3 = __ldg(wp + (u + 3) * kTile);
+          ax += w0 * __shfl_sync(0xffffffffu, vx, u) + w1 * __shfl_sync(0xffffffffu, vx, u + 1) +
+                w2 * __shfl_sync(0xffffffffu, vx, u + 2) + w3 * __shfl_sync(0xffffffffu, vx, u + 3);
+          ay += w0 * __shfl_sync(0xffffffffu, vy, u) + w1 * __shfl_sync(0xffffffffu, vy, u + 1) +
+                w2 * __shfl_sync(0xffffffffu, vy, u + 2) + w3 * __shfl_sync(0xffffffffu, vy, u + 3);
+          az += w0 * __shfl_sync(0xffffffffu, vz, u) + w1 * __shfl_sync(0xffffffffu, vz, u + 1) +
+                w2 * __shfl_sync(0xffffffffu, vz, u + 2) + w3 * __shfl_sync(0xffffffffu, vz, u + 3);
+        }
+        for (; u < m; ++u) {
+          const T w = __ldg(wp + u * kTile);
+          ax += w * __shfl_sync(0xffffffffu, vx, u);
+          ay += w * __shfl_sync(0xffffffffu, vy, u);
+          az += w * __shfl_sync(0xffffffffu, vz, u);
+        }
       }
-      for (; j < len; j += g) {
-        const T wv = wr[j];
-        ax += wv * bx[j];
-        ay += wv * by[j];
-        az += wv * bz[j];
-      }
-    }
-    group_reduce(ax, ay, az, g);
-    if (active && sub == 0) {
       if (row < s.ns) {
         const int64_t o = (int64_t)s.c0 + row;
-        y[o] = ax;
-        y[o + n] = ay;
-        y[o + 2 * (int64_t)n] = az;
-      } else {
+        atomicAdd(y + o, ax);
+        atomicAdd(y + o + n, ay);
+        atomicAdd(y + o + 2 * (int64_t)n, az);
+      } else if (row < s.ns + s.nr) {
         const int64_t r = rows[s.roff + row - s.ns];
         atomicAdd(b + r, -ax);
         atomicAdd(b + r + n, -ay);
         atomicAdd(b + r + 2 * (int64_t)n, -az);
       }
     }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) {
+      const unsigned long long done = atomicAdd(sy.fdone + tk.sn, 1ULL) + 1ULL;
+      if (done == ep * (unsigned long long)s.ntf && s.parent >= 0) {
+        __threadfence();
+        atomicAdd(sy.fchild + s.parent, 1ULL);
+      }
+    }
   }
 }
 
-// mode 0: v[perm] = x (direct FP64 solve); mode 1: v[perm] += x (increment).
 template <typename T>
 __global__ void __launch_bounds__(256) k_sweep_backward(const SweepTask* __restrict__ tasks, int ntasks,
                                                         const SnInfo* __restrict__ sn, const int* __restrict__ rows,
-                                                        const T* __restrict__ W, const T* __restrict__ y,
-                                                        T* __restrict__ x, const int* __restrict__ perm,
-                                                        double* __restrict__ v, double* __restrict__ qk,
-                                                        const double* __restrict__ q, double dt, int mode, int n) {
+                                                        const T* __restrict__ W, const T* __restrict__ y, T* x, int n,
+                                                        SweepSync sy) {
   const int lane = threadIdx.x & 31;
-  const int nwarps = (gridDim.x * blockDim.x) >> 5;
-  for (int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < ntasks; w += nwarps) {
-    const SweepTask t = tasks[w];
-    const SnInfo s = sn[t.sn];
-    const int g = t.g;
-    const int grp = lane / g, sub = lane % g;
-    const int col = t.first + grp;
-    const bool active = grp < t.count;
+  const unsigned long long ep = *reinterpret_cast<const volatile unsigned long long*>(sy.epoch);
+  while (true) {
+    int t = 0;
+    if (lane == 0) t = atomicAdd(sy.queue + 1, 1);
+    t = __shfl_sync(0xffffffffu, t, 0);
+    if (t >= ntasks) return;
+    const SweepTask tk = tasks[t];
+    const SnInfo s = sn[tk.sn];
+    int ok = 1;
+    if (lane == 0 && s.parent >= 0)
+      ok = wait_counter(sy.bdone + s.parent, ep * (unsigned long long)sn[s.parent].ntb, sy.err);
+    ok = __shfl_sync(0xffffffffu, ok, 0);
+    const int j0t = tk.tile * kTile;
+    const int col = j0t + lane;
+    const int nd = s.ns - j0t;  // local rows belonging to D^-1
     T ax = 0, ay = 0, az = 0;
-    if (active) {
-      const int nd = s.ns - col;  // entries of D^-1 in this column
-      const int len = nd + s.nr;
-      const int64_t base = s.woff + (int64_t)col * (s.ns + s.nr) - (int64_t)col * (col - 1) / 2;
-      const T* wc = W + base;
-      const T* yx = y + s.c0 + col;
-      const T* yy = yx + n;
-      const T* yz = yy + n;
-      int k = sub;
-      for (; k < nd; k += g) {
-        const T wv = wc[k];
-        ax += wv * yx[k];
-        ay += wv * yy[k];
-        az += wv * yz[k];
+    if (ok) {
+      for (int i0 = tk.a0; i0 < tk.a1; i0 += 32) {
+        const int il = i0 + lane;
+        T vx = 0, vy = 0, vz = 0;
+        if (il < tk.a1) {
+          if (il < nd) {
+            const int64_t o = (int64_t)s.c0 + j0t + il;
+            vx = y[o];
+            vy = y[o + n];
+            vz = y[o + 2 * (int64_t)n];
+          } else {
+            const int64_t r = rows[s.roff + il - nd];
+            vx = -ldcg(x + r);
+            vy = -ldcg(x + r + n);
+            vz = -ldcg(x + r + 2 * (int64_t)n);
+          }
+        }
+        const int m = min(32, tk.a1 - i0);
+        const T* wp = W + tk.off + (int64_t)i0 * kTile + lane;
+        int u = 0;
+        for (; u + 4 <= m; u += 4) {
+          const T w0 = __ldg(wp + u * kTile), w1 = __ldg(wp + (u + 1) * kTile);
+          const T w2 = __ldg(wp + (u + 2) * kTile), w3 = __ldg(wp + (u + 3) * kTile);
+          ax += w0 * __shfl_sync(0xffffffffu, vx, u) + w1 * __shfl_sync(0xffffffffu, vx, u + 1) +
+                w2 * __shfl_sync(0xffffffffu, vx, u + 2) + w3 * __shfl_sync(0xffffffffu, vx, u + 3);
+          ay += w0 * __shfl_sync(0xffffffffu, vy, u) + w1 * __shfl_sync(0xffffffffu, vy, u + 1) +
+                w2 * __shfl_sync(0xffffffffu, vy, u + 2) + w3 * __shfl_sync(0xffffffffu, vy, u + 3);
+          az += w0 * __shfl_sync(0xffffffffu, vz, u) + w1 * __shfl_sync(0xffffffffu, vz, u + 1) +
+                w2 * __shfl_sync(0xffffffffu, vz, u + 2) + w3 * __shfl_sync(0xffffffffu, vz, u + 3);
+        }
+        for (; u < m; ++u) {
+          const T w = __ldg(wp + u * kTile);
+          ax += w * __shfl_sync(0xffffffffu, vx, u);
+          ay += w * __shfl_sync(0xffffffffu, vy, u);
+          az += w * __shfl_sync(0xffffffffu, vz, u);
+        }
       }
-      const int* rr = rows + s.roff - nd;
-      for (; k < len; k += g) {
-        const T wv = wc[k];
-        const int64_t r = rr[k];
-        ax -= wv * x[r];
-        ay -= wv * x[r + n];
-        az -= wv * x[r + 2 * (int64_t)n];
+      if (col < s.ns) {
+        const int64_t o = (int64_t)s.c0 + col;
+        atomicAdd(x + o, ax);
+        atomicAdd(x + o + n, ay);
+        atomicAdd(x + o + 2 * (int64_t)n, az);
       }
     }
-    group_reduce(ax, ay, az, g);
-    if (active && sub == 0) {
-      const int64_t pc = (int64_t)s.c0 + col;
-      x[pc] = ax;
-      x[pc + n] = ay;
-      x[pc + 2 * (int64_t)n] = az;
-      const int64_t vtx = perm[pc];
-      double vx = (double)ax, vy = (double)ay, vz = (double)az;
-      if (mode == 1) {
-        vx += v[3 * vtx];
-        vy += v[3 * vtx + 1];
-        vz += v[3 * vtx + 2];
-      }
-      v[3 * vtx] = vx;
-      v[3 * vtx + 1] = vy;
-      v[3 * vtx + 2] = vz;
-      qk[3 * vtx] = q[3 * vtx] + dt * vx;
-      qk[3 * vtx + 1] = q[3 * vtx + 1] + dt * vy;
-      qk[3 * vtx + 2] = q[3 * vtx + 2] + dt * vz;
-    }
+    __threadfence();
+    __syncwarp();
+    if (lane == 0) atomicAdd(sy.bdone + tk.sn, 1ULL);
   }
 }
 
-// At most kSweepCtasPerSm CTAs of 8 warps per SM; warps stride over tasks.
+// After the backward sweep: v[perm] = x (mode 0) or v[perm] += x (mode 1),
+// q^k = q_n + dt v; x and y are cleared for the next solve; one thread
+// rewinds the work queues and advances the solve counter.
+template <typename T>
+__global__ void k_solve_post(int n, const int* __restrict__ perm, T* x, T* y, double* __restrict__ v,
+                             double* __restrict__ qk, const double* __restrict__ q, double dt, int mode, SweepSync sy) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int64_t vtx = perm[k];
+    double vv[3];
+    for (int c = 0; c < 3; ++c) {
+      const int64_t o = k + (int64_t)c * n;
+      vv[c] = (double)x[o];
+      x[o] = 0;
+      y[o] = 0;
+    }
+    for (int c = 0; c < 3; ++c) {
+      double val = vv[c];
+      if (mode == 1) val += v[3 * vtx + c];
+      v[3 * vtx + c] = val;
+      qk[3 * vtx + c] = q[3 * vtx + c] + dt * val;
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sy.queue[0] = 0;
+    sy.queue[1] = 0;
+    *sy.epoch += 1ULL;
+  }
+}
+
+// Clears the solve vectors and rewinds the queues (first use / timing runs).
+template <typename T>
+__global__ void k_solve_prep(int n, T* x, T* y, SweepSync sy) {
+  for (int64_t k = blockIdx.x * blockDim.x + threadIdx.x; k < 3 * (int64_t)n; k += gridDim.x * blockDim.x) {
+    x[k] = 0;
+    y[k] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    sy.queue[0] = 0;
+    sy.queue[1] = 0;
+  }
+}
+
 constexpr int kSweepCtas = 148 * 8;
 
 template <typename T>
-void launch_sweep_forward(cudaStream_t st, const SweepTask* tasks, int ntasks, const SnInfo* sn, const int* rows,
-                          const T* W, T* b, T* y, int n) {
-  const int grid = std::min(kSweepCtas, (ntasks + 7) / 8);
-  k_sweep_forward<T><<<grid, 256, 0, st>>>(tasks, ntasks, sn, rows, W, b, y, n);
+void launch_solve_sweeps(cudaStream_t st, const SweepTask* ftasks, int nf, const SweepTask* btasks, int nb,
+                         const SnInfo* sn, const int* rows, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
+                         SweepSync sy) {
+  k_sweep_forward<T><<<std::min(kSweepCtas, (nf + 7) / 8), 256, 0, st>>>(ftasks, nf, sn, rows, Wf, b, y, n, sy);
+  k_sweep_backward<T><<<std::min(kSweepCtas, (nb + 7) / 8), 256, 0, st>>>(btasks, nb, sn, rows, Wb, y, x, n, sy);
 }
 template <typename T>
-void launch_sweep_backward(cudaStream_t st, const SweepTask* tasks, int ntasks, const SnInfo* sn, const int* rows,
-                           const T* W, const T* y, T* x, const int* perm, double* v, double* qk, const double* q,
-                           double dt, int mode, int n) {
-  const int grid = std::min(kSweepCtas, (ntasks + 7) / 8);
-  k_sweep_backward<T><<<grid, 256, 0, st>>>(tasks, ntasks, sn, rows, W, y, x, perm, v, qk, q, dt, mode, n);
+void launch_solve_post(cudaStream_t st, int n, const int* perm, T* x, T* y, double* v, double* qk, const double* q,
+                       double dt, int mode, SweepSync sy) {
+  k_solve_post<T><<<std::min(148 * 4, (n + 255) / 256), 256, 0, st>>>(n, perm, x, y, v, qk, q, dt, mode, sy);
 }
-template void launch_sweep_forward<double>(cudaStream_t, const SweepTask*, int, const SnInfo*, const int*,
-                                           const double*, double*, double*, int);
-template void launch_sweep_forward<float>(cudaStream_t, const SweepTask*, int, const SnInfo*, const int*, const float*,
-                                          float*, float*, int);
-template void launch_sweep_backward<double>(cudaStream_t, const SweepTask*, int, const SnInfo*, const int*,
-                                            const double*, const double*, double*, const int*, double*, double*,
-                                            const double*, double, int, int);
-template void launch_sweep_backward<float>(cudaStream_t, const SweepTask*, int, const SnInfo*, const int*,
-                                           const float*, const float*, float*, const int*, double*, double*,
-                                           const double*, double, int, int);
+template <typename T>
+void launch_solve_prep(cudaStream_t st, int n, T* x, T* y, SweepSync sy) {
+  k_solve_prep<T><<<std::min(148 * 4, (3 * n + 255) / 256), 256, 0, st>>>(n, x, y, sy);
+}
+
+template void launch_solve_sweeps<double>(cudaStream_t, const SweepTask*, int, const SweepTask*, int, const SnInfo*,
+                                          const int*, const double*, const double*, double*, double*, double*, int,
+                                          SweepSync);
+template void launch_solve_sweeps<float>(cudaStream_t, const SweepTask*, int, const SweepTask*, int, const SnInfo*,
+                                         const int*, const float*, const float*, float*, float*, float*, int,
+                                         SweepSync);
+template void launch_solve_post<double>(cudaStream_t, int, const int*, double*, double*, double*, double*,
+                                        const double*, double, int, SweepSync);
+template void launch_solve_post<float>(cudaStream_t, int, const int*, float*, float*, double*, double*, const double*,
+                                       double, int, SweepSync);
+template void launch_solve_prep<double>(cudaStream_t, int, double*, double*, SweepSync);
+template void launch_solve_prep<float>(cudaStream_t, int, float*, float*, SweepSync);
 
 }  // namespace pdfb

@@ -54,6 +54,7 @@ def lib():
     L.pdf_export_stats.argtypes = [vp, C.c_char_p]
     L.pdf_get_residual_history.argtypes = [vp, vp, i32, C.POINTER(i32)]
     L.pdf_time_phase.argtypes = [vp, i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.pdf_factor_check.argtypes = [C.POINTER(abi.pdf_scene_desc), C.POINTER(abi.pdf_params), vp, vp]
     L.pdf_destroy.argtypes = [vp]
     L.pdf_detect_candidates.argtypes = [vp, i32, vp, i32, C.c_double, vp, i32, C.POINTER(i32), i32]
     L.pdf_detect_self_collisions.argtypes = [vp, i32, vp, i32, C.c_double, vp, i32, C.POINTER(i32), i32]
@@ -210,6 +211,15 @@ def getSimulationParametersFromJSONFileName(path):
 def getSimulation(scene, params):
     """Mirror of getSimulation (src/simulation_building.cpp:80-98)."""
     return Simulation(scene, params)
+
+
+def factor_check(scene, params, b):
+    """Host emulation of the device solve on the tiled factor layout (no GPU)."""
+    d = scene.desc()
+    bb = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.empty_like(bb)
+    _check(lib().pdf_factor_check(C.byref(d), C.byref(params), _ptr(bb), _ptr(x)))
+    return x
 
 
 def detect_candidates(positions, triangles, tolerance, device=0, cap=None):

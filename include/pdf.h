@@ -245,6 +245,14 @@ int pdf_get_residual_history(pdf_handle* h, double* out, int32_t cap,
 int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms,
                    double* bytes);
 
+/* Host-only consistency check of the factorisation and of the device sweep
+ * layout (no GPU needed): builds the global-step matrix of the scene, factors
+ * it, and runs a sequential emulation of the two device sweeps (same work
+ * items, same tiled layout, every index bounds-checked) to solve
+ * (M + dt^2 A^T A) x = b for three right-hand sides (3N, vertex-major). */
+int pdf_factor_check(const pdf_scene_desc* scene, const pdf_params* params,
+                     const double* b, double* x);
+
 /* Last error message of this handle (never NULL). */
 const char* pdf_last_error(const pdf_handle* h);
 /* Last error of calls that have no handle (loading, create failures). */
