@@ -52,7 +52,7 @@ inline int blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kThread
 constexpr int kStrideBlocks = 592;  // 4 x 148 SMs for grid-stride kernels
 
 // Work items of one sweep are at most 32 x kChunk elements.
-constexpr int kChunk = 256;
+constexpr int kChunk = 64;
 
 // Work-item lists of the two sweeps in elimination-tree order (forward:
 // levels bottom-up, backward: top-down), one item per tile and chunk.

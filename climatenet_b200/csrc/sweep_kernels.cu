@@ -29,6 +29,7 @@
 namespace pdfb {
 
 constexpr int kMaxSpins = 1 << 22;
+constexpr int kTicketBatch = 2;
 
 __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long* p) {
   return *reinterpret_cast<const volatile unsigned long long*>(p);
@@ -57,10 +58,16 @@ __global__ void __launch_bounds__(256) k_sweep_forward(const SweepTask* __restri
                                                        const T* __restrict__ W, T* b, T* y, int n, SweepSync sy) {
   const int lane = threadIdx.x & 31;
   const unsigned long long ep = *reinterpret_cast<const volatile unsigned long long*>(sy.epoch);
-  while (true) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(sy.queue + 0, 1);
-    t = __shfl_sync(0xffffffffu, t, 0);
+  // tickets are taken kTicketBatch at a time and processed in order: every
+  // item with a smaller ticket is held by a running warp, so the waits below
+  // always end
+  int t = 0, tend = 0;
+  for (;; ++t) {
+    if (t >= tend) {
+      if (lane == 0) t = atomicAdd(sy.queue + 0, kTicketBatch);
+      t = __shfl_sync(0xffffffffu, t, 0);
+      tend = t + kTicketBatch;
+    }
     if (t >= ntasks) return;
     const SweepTask tk = tasks[t];
     const SnInfo s = sn[tk.sn];
@@ -75,30 +82,23 @@ __global__ void __launch_bounds__(256) k_sweep_forward(const SweepTask* __restri
       const T* bz = by + n;
       for (int j0 = tk.a0; j0 < tk.a1; j0 += 32) {
         const int jl = j0 + lane;
+        const int m = min(32, tk.a1 - j0);
+        const T* wp = W + tk.off + (int64_t)j0 * kTile + lane;
+        // all 32 tile loads in flight before the first use
+        T w[32];
+#pragma unroll
+        for (int u = 0; u < 32; ++u) w[u] = (u < m) ? __ldg(wp + u * kTile) : T(0);
         T vx = 0, vy = 0, vz = 0;
         if (jl < tk.a1) {
           vx = ldcg(bx + jl);
           vy = ldcg(by + jl);
           vz = ldcg(bz + jl);
         }
-        const int m = min(32, tk.a1 - j0);
-        const T* wp = W + tk.off + (int64_t)j0 * kTile + lane;
-        int u = 0;
-        for (; u + 4 <= m; u += 4) {
-          const T w0 = __ldg(wp + u * kTile), w1 = __ldg(wp + (u + 1) * kTile);
-          const T w2 = __ldg(wp + (u + 2) * kTile), w3 = __ldg(wp + (u + 3) * kTile);
-          ax += w0 * __shfl_sync(0xffffffffu, vx, u) + w1 * __shfl_sync(0xffffffffu, vx, u + 1) +
-                w2 * __shfl_sync(0xffffffffu, vx, u + 2) + w3 * __shfl_sync(0xffffffffu, vx, u + 3);
-          ay += w0 * __shfl_sync(0xffffffffu, vy, u) + w1 * __shfl_sync(0xffffffffu, vy, u + 1) +
-                w2 * __shfl_sync(0xffffffffu, vy, u + 2) + w3 * __shfl_sync(0xffffffffu, vy, u + 3);
-          az += w0 * __shfl_sync(0xffffffffu, vz, u) + w1 * __shfl_sync(0xffffffffu, vz, u + 1) +
-                w2 * __shfl_sync(0xffffffffu, vz, u + 2) + w3 * __shfl_sync(0xffffffffu, vz, u + 3);
-        }
-        for (; u < m; ++u) {
-          const T w = __ldg(wp + u * kTile);
-          ax += w * __shfl_sync(0xffffffffu, vx, u);
-          ay += w * __shfl_sync(0xffffffffu, vy, u);
-          az += w * __shfl_sync(0xffffffffu, vz, u);
+#pragma unroll
+        for (int u = 0; u < 32; ++u) {
+          ax += w[u] * __shfl_sync(0xffffffffu, vx, u);
+          ay += w[u] * __shfl_sync(0xffffffffu, vy, u);
+          az += w[u] * __shfl_sync(0xffffffffu, vz, u);
         }
       }
       if (row < s.ns) {
@@ -132,10 +132,13 @@ __global__ void __launch_bounds__(256) k_sweep_backward(const SweepTask* __restr
                                                         SweepSync sy) {
   const int lane = threadIdx.x & 31;
   const unsigned long long ep = *reinterpret_cast<const volatile unsigned long long*>(sy.epoch);
-  while (true) {
-    int t = 0;
-    if (lane == 0) t = atomicAdd(sy.queue + 1, 1);
-    t = __shfl_sync(0xffffffffu, t, 0);
+  int t = 0, tend = 0;
+  for (;; ++t) {
+    if (t >= tend) {
+      if (lane == 0) t = atomicAdd(sy.queue + 1, kTicketBatch);
+      t = __shfl_sync(0xffffffffu, t, 0);
+      tend = t + kTicketBatch;
+    }
     if (t >= ntasks) return;
     const SweepTask tk = tasks[t];
     const SnInfo s = sn[tk.sn];
@@ -150,6 +153,11 @@ __global__ void __launch_bounds__(256) k_sweep_backward(const SweepTask* __restr
     if (ok) {
       for (int i0 = tk.a0; i0 < tk.a1; i0 += 32) {
         const int il = i0 + lane;
+        const int m = min(32, tk.a1 - i0);
+        const T* wp = W + tk.off + (int64_t)i0 * kTile + lane;
+        T w[32];
+#pragma unroll
+        for (int u = 0; u < 32; ++u) w[u] = (u < m) ? __ldg(wp + u * kTile) : T(0);
         T vx = 0, vy = 0, vz = 0;
         if (il < tk.a1) {
           if (il < nd) {
@@ -164,24 +172,11 @@ __global__ void __launch_bounds__(256) k_sweep_backward(const SweepTask* __restr
             vz = -ldcg(x + r + 2 * (int64_t)n);
           }
         }
-        const int m = min(32, tk.a1 - i0);
-        const T* wp = W + tk.off + (int64_t)i0 * kTile + lane;
-        int u = 0;
-        for (; u + 4 <= m; u += 4) {
-          const T w0 = __ldg(wp + u * kTile), w1 = __ldg(wp + (u + 1) * kTile);
-          const T w2 = __ldg(wp + (u + 2) * kTile), w3 = __ldg(wp + (u + 3) * kTile);
-          ax += w0 * __shfl_sync(0xffffffffu, vx, u) + w1 * __shfl_sync(0xffffffffu, vx, u + 1) +
-                w2 * __shfl_sync(0xffffffffu, vx, u + 2) + w3 * __shfl_sync(0xffffffffu, vx, u + 3);
-          ay += w0 * __shfl_sync(0xffffffffu, vy, u) + w1 * __shfl_sync(0xffffffffu, vy, u + 1) +
-                w2 * __shfl_sync(0xffffffffu, vy, u + 2) + w3 * __shfl_sync(0xffffffffu, vy, u + 3);
-          az += w0 * __shfl_sync(0xffffffffu, vz, u) + w1 * __shfl_sync(0xffffffffu, vz, u + 1) +
-                w2 * __shfl_sync(0xffffffffu, vz, u + 2) + w3 * __shfl_sync(0xffffffffu, vz, u + 3);
-        }
-        for (; u < m; ++u) {
-          const T w = __ldg(wp + u * kTile);
-          ax += w * __shfl_sync(0xffffffffu, vx, u);
-          ay += w * __shfl_sync(0xffffffffu, vy, u);
-          az += w * __shfl_sync(0xffffffffu, vz, u);
+#pragma unroll
+        for (int u = 0; u < 32; ++u) {
+          ax += w[u] * __shfl_sync(0xffffffffu, vx, u);
+          ay += w[u] * __shfl_sync(0xffffffffu, vy, u);
+          az += w[u] * __shfl_sync(0xffffffffu, vz, u);
         }
       }
       if (col < s.ns) {
@@ -239,14 +234,24 @@ __global__ void k_solve_prep(int n, T* x, T* y, SweepSync sy) {
   }
 }
 
-constexpr int kSweepCtas = 148 * 8;
+// Persistent grid: as many CTAs as can be resident at once.
+template <typename K>
+int resident_ctas(K kernel) {
+  int dev = 0, sms = 148, per_sm = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, 0);
+  return std::max(1, per_sm) * sms;
+}
 
 template <typename T>
 void launch_solve_sweeps(cudaStream_t st, const SweepTask* ftasks, int nf, const SweepTask* btasks, int nb,
                          const SnInfo* sn, const int* rows, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
                          SweepSync sy) {
-  k_sweep_forward<T><<<std::min(kSweepCtas, (nf + 7) / 8), 256, 0, st>>>(ftasks, nf, sn, rows, Wf, b, y, n, sy);
-  k_sweep_backward<T><<<std::min(kSweepCtas, (nb + 7) / 8), 256, 0, st>>>(btasks, nb, sn, rows, Wb, y, x, n, sy);
+  static const int gf = resident_ctas(k_sweep_forward<T>);
+  static const int gb = resident_ctas(k_sweep_backward<T>);
+  k_sweep_forward<T><<<std::min(gf, (nf + 7) / 8), 256, 0, st>>>(ftasks, nf, sn, rows, Wf, b, y, n, sy);
+  k_sweep_backward<T><<<std::min(gb, (nb + 7) / 8), 256, 0, st>>>(btasks, nb, sn, rows, Wb, y, x, n, sy);
 }
 template <typename T>
 void launch_solve_post(cudaStream_t st, int n, const int* perm, T* x, T* y, double* v, double* qk, const double* q,
