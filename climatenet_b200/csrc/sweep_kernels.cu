@@ -38,6 +38,10 @@ __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned lon
 __device__ __forceinline__ float ldcg(const float* p) { return __ldcg(p); }
 __device__ __forceinline__ double ldcg(const double* p) { return __ldcg(p); }
 
+// Release / acquire fence at device scope (lighter than the sequentially
+// consistent __threadfence()).
+__device__ __forceinline__ void fence_acq_rel_gpu() { asm volatile("fence.acq_rel.gpu;" ::: "memory"); }
+
 // lane 0 waits until *ctr >= target; false (and error flag set) on timeout
 __device__ __forceinline__ bool wait_counter(const unsigned long long* ctr, unsigned long long target, int* err) {
   int spins = 0;
@@ -46,10 +50,18 @@ __device__ __forceinline__ bool wait_counter(const unsigned long long* ctr, unsi
       atomicExch(err, 1);
       return false;
     }
-    __nanosleep(64);
+    __nanosleep(32);
   }
-  __threadfence();
+  fence_acq_rel_gpu();
   return true;
+}
+
+// Issues the (up to) 32 loads of one 32-column slab of a tile: lane l reads
+// element (l, u) at p[32 u]; absent columns read as zero.
+template <typename T>
+__device__ __forceinline__ void load_tile(T (&w)[32], const T* p, int m) {
+#pragma unroll
+  for (int u = 0; u < 32; ++u) w[u] = (u < m) ? __ldg(p + u * kTile) : T(0);
 }
 
 template <typename T>
@@ -71,6 +83,11 @@ __global__ void __launch_bounds__(256) k_sweep_forward(const SweepTask* __restri
     if (t >= ntasks) return;
     const SweepTask tk = tasks[t];
     const SnInfo s = sn[tk.sn];
+    // the factor does not depend on the wait: its first 32 tile columns are
+    // already in flight while lane 0 checks the children
+    const T* wbase = W + tk.off + lane;
+    T w[32];
+    load_tile(w, wbase + (int64_t)tk.a0 * kTile, min(32, tk.a1 - tk.a0));
     int ok = 1;
     if (lane == 0 && s.nchild > 0) ok = wait_counter(sy.fchild + tk.sn, ep * (unsigned long long)s.nchild, sy.err);
     ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -82,12 +99,7 @@ __global__ void __launch_bounds__(256) k_sweep_forward(const SweepTask* __restri
       const T* bz = by + n;
       for (int j0 = tk.a0; j0 < tk.a1; j0 += 32) {
         const int jl = j0 + lane;
-        const int m = min(32, tk.a1 - j0);
-        const T* wp = W + tk.off + (int64_t)j0 * kTile + lane;
-        // all 32 tile loads in flight before the first use
-        T w[32];
-#pragma unroll
-        for (int u = 0; u < 32; ++u) w[u] = (u < m) ? __ldg(wp + u * kTile) : T(0);
+        if (j0 != tk.a0) load_tile(w, wbase + (int64_t)j0 * kTile, min(32, tk.a1 - j0));
         T vx = 0, vy = 0, vz = 0;
         if (jl < tk.a1) {
           vx = ldcg(bx + jl);
@@ -113,12 +125,12 @@ __global__ void __launch_bounds__(256) k_sweep_forward(const SweepTask* __restri
         atomicAdd(b + r + 2 * (int64_t)n, -az);
       }
     }
-    __threadfence();
+    fence_acq_rel_gpu();
     __syncwarp();
     if (lane == 0) {
       const unsigned long long done = atomicAdd(sy.fdone + tk.sn, 1ULL) + 1ULL;
       if (done == ep * (unsigned long long)s.ntf && s.parent >= 0) {
-        __threadfence();
+        fence_acq_rel_gpu();
         atomicAdd(sy.fchild + s.parent, 1ULL);
       }
     }
@@ -142,6 +154,9 @@ __global__ void __launch_bounds__(256) k_sweep_backward(const SweepTask* __restr
     if (t >= ntasks) return;
     const SweepTask tk = tasks[t];
     const SnInfo s = sn[tk.sn];
+    const T* wbase = W + tk.off + lane;
+    T w[32];
+    load_tile(w, wbase + (int64_t)tk.a0 * kTile, min(32, tk.a1 - tk.a0));
     int ok = 1;
     if (lane == 0 && s.parent >= 0)
       ok = wait_counter(sy.bdone + s.parent, ep * (unsigned long long)sn[s.parent].ntb, sy.err);
@@ -153,11 +168,7 @@ __global__ void __launch_bounds__(256) k_sweep_backward(const SweepTask* __restr
     if (ok) {
       for (int i0 = tk.a0; i0 < tk.a1; i0 += 32) {
         const int il = i0 + lane;
-        const int m = min(32, tk.a1 - i0);
-        const T* wp = W + tk.off + (int64_t)i0 * kTile + lane;
-        T w[32];
-#pragma unroll
-        for (int u = 0; u < 32; ++u) w[u] = (u < m) ? __ldg(wp + u * kTile) : T(0);
+        if (i0 != tk.a0) load_tile(w, wbase + (int64_t)i0 * kTile, min(32, tk.a1 - i0));
         T vx = 0, vy = 0, vz = 0;
         if (il < tk.a1) {
           if (il < nd) {
@@ -186,7 +197,7 @@ __global__ void __launch_bounds__(256) k_sweep_backward(const SweepTask* __restr
         atomicAdd(x + o + 2 * (int64_t)n, az);
       }
     }
-    __threadfence();
+    fence_acq_rel_gpu();
     __syncwarp();
     if (lane == 0) atomicAdd(sy.bdone + tk.sn, 1ULL);
   }
