@@ -74,6 +74,8 @@ struct pdf_handle {
 };
 
 namespace pdfb {
+// api.cu: message returned by pdf_global_error()
+void set_global_error(const std::string& msg);
 // selfdetect.cu
 int self_detect_init(pdf_handle* h);
 int self_detect_step(pdf_handle* h);  // self contacts of the step (detection + pairing)

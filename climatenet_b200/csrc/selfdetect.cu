@@ -796,4 +796,141 @@ int standalone_self(const double* pos, int nv, const int* tris, int nt, double t
   return status;
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free candidate detection (pdf_detect_candidates_noalloc).
+//
+// Some callers cannot allocate device memory at the point where they need
+// the candidate pairs: code running inside another framework's memory pool
+// that must not grow the process footprint, real-time loops with a fixed
+// memory budget that forbid cudaMalloc/cudaFree after start-up, and hosts whose
+// allocator is not the CUDA runtime's.  For them the whole workspace of the
+// detection (LBVH boxes and nodes, Morton keys, candidate keys, radix-sort
+// temporary storage) lives in one file-scope device array of fixed size.
+// Every GPU that loads this library holds that array until the process exits.
+constexpr int kNoAllocMaxTriangles = 65536;
+constexpr int kNoAllocMaxPairs = 262144;
+constexpr size_t kNoAllocSortBytes = size_t(8) << 20;
+constexpr size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+// byte layout of the array (each block 256-byte aligned)
+constexpr size_t kTriBytes = align256(sizeof(double) * 3 * kNoAllocMaxTriangles);      // tlo, thi, nlo, nhi
+constexpr size_t kTriKeyBytes = align256(sizeof(unsigned long long) * kNoAllocMaxTriangles);  // mkey, mkey2
+constexpr size_t kTriIntBytes = align256(sizeof(int) * kNoAllocMaxTriangles);  // mval, mval2, left, right, parent, leaf_parent, visits
+constexpr size_t kPairKeyBytes = align256(sizeof(unsigned long long) * kNoAllocMaxPairs);  // hkey, hkey2
+constexpr size_t kPairIntBytes = align256(sizeof(int) * kNoAllocMaxPairs);                  // hval, hval2
+constexpr size_t kPairBaryBytes = align256(sizeof(double) * 3 * kNoAllocMaxPairs);          // hbary (unused in mode 0)
+constexpr size_t kSmallBytes = 256 * 3;                                                     // bbox, n_hits, err
+constexpr size_t kNoAllocScratchBytes = 4 * kTriBytes + 2 * kTriKeyBytes + 7 * kTriIntBytes + 2 * kPairKeyBytes +
+                                        2 * kPairIntBytes + kPairBaryBytes + kSmallBytes + kNoAllocSortBytes;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+// Device address of g_noalloc_scratch per device, looked up once per device
+// with that device current (the array's name is only a host-side stand-in).
+static unsigned char* g_noalloc_ptr[64] = {};
+
+__global__ void k_keys_to_pairs(int n, const unsigned long long* __restrict__ keys, int* __restrict__ pairs) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  pairs[2 * k] = (int)(keys[k] >> 32);
+  pairs[2 * k + 1] = (int)(keys[k] & 0xffffffffu);
+}
+
+int noalloc_candidates(const double* positions, int nv, const int* triangles, int nt, double tol, int* pairs,
+                       int cap, int* n_out, cudaStream_t st, std::string& err) {
+  if (!positions || !triangles || nv <= 0 || nt <= 0 || cap < 0 || !n_out) {
+    err = "invalid arguments";
+    return PDF_INVALID_ARG;
+  }
+  if (nt > kNoAllocMaxTriangles) {
+    err = "pdf_detect_candidates_noalloc handles at most " + std::to_string(kNoAllocMaxTriangles) +
+          " triangles (got " + std::to_string(nt) + ")";
+    return PDF_CAPACITY_EXCEEDED;
+  }
+  int dev = 0;
+  CKS(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    err = "device ordinal out of range";
+    return PDF_INVALID_ARG;
+  }
+  if (!g_noalloc_ptr[dev]) {
+    // first call on this device: set-up (must not happen during stream capture)
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      err = std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e);
+      return PDF_CUDA_ERROR;
+    }
+    size_t b1 = 0, b2 = 0;
+    CKS(cub::DeviceRadixSort::SortPairs(nullptr, b1, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                        (int*)nullptr, (int*)nullptr, kNoAllocMaxTriangles));
+    CKS(cub::DeviceRadixSort::SortPairs(nullptr, b2, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                        (int*)nullptr, (int*)nullptr, kNoAllocMaxPairs));
+    if (std::max(b1, b2) > kNoAllocSortBytes) {
+      err = "radix-sort workspace larger than the reserved scratch";
+      return PDF_CAPACITY_EXCEEDED;
+    }
+    g_noalloc_ptr[dev] = (unsigned char*)p;
+  }
+  unsigned char* base = g_noalloc_ptr[dev];
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    unsigned char* q = base + off;
+    off += bytes;
+    return q;
+  };
+  SelfWS w;
+  w.max_nt = nt;
+  w.max_nv = nv;
+  w.hit_cap = kNoAllocMaxPairs;
+  w.tlo = (double*)take(kTriBytes);
+  w.thi = (double*)take(kTriBytes);
+  w.nlo = (double*)take(kTriBytes);
+  w.nhi = (double*)take(kTriBytes);
+  w.mkey = (unsigned long long*)take(kTriKeyBytes);
+  w.mkey2 = (unsigned long long*)take(kTriKeyBytes);
+  w.mval = (int*)take(kTriIntBytes);
+  w.mval2 = (int*)take(kTriIntBytes);
+  w.left = (int*)take(kTriIntBytes);
+  w.right = (int*)take(kTriIntBytes);
+  w.parent = (int*)take(kTriIntBytes);
+  w.leaf_parent = (int*)take(kTriIntBytes);
+  w.visits = (int*)take(kTriIntBytes);
+  w.hkey = (unsigned long long*)take(kPairKeyBytes);
+  w.hkey2 = (unsigned long long*)take(kPairKeyBytes);
+  w.hval = (int*)take(kPairIntBytes);
+  w.hval2 = (int*)take(kPairIntBytes);
+  w.hbary = (double*)take(kPairBaryBytes);
+  w.bbox = (unsigned long long*)take(256);
+  w.n_hits = (int*)take(256);
+  w.err = (int*)take(256);
+  w.cub_tmp = take(kNoAllocSortBytes);
+  w.cub_bytes = kNoAllocSortBytes;
+  const int nh = detect_mesh(w, positions, triangles, 0, nv, nt, tol, 0, st);
+  *n_out = nh;
+  if (nh > kNoAllocMaxPairs || nh > cap) {
+    err = "candidate pairs exceed the output capacity or the scratch limit (" + std::to_string(kNoAllocMaxPairs) + ")";
+    return PDF_CAPACITY_EXCEEDED;
+  }
+  if (nh > 0) k_keys_to_pairs<<<(nh + 255) / 256, 256, 0, st>>>(nh, w.hkey2, pairs);
+  CKS(cudaGetLastError());
+  CKS(cudaStreamSynchronize(st));
+  return PDF_OK;
+}
+
 }  // namespace pdfb
+
+extern "C" int pdf_detect_candidates_noalloc(const double* positions, int32_t n_vertices, const int32_t* triangles,
+                                             int32_t n_triangles, double tolerance, int32_t* pairs, int32_t cap,
+                                             int32_t* n, void* cuda_stream) {
+  std::string err;
+  int st;
+  try {
+    st = pdfb::noalloc_candidates(positions, n_vertices, triangles, n_triangles, tolerance, pairs, cap, n,
+                                  (cudaStream_t)cuda_stream, err);
+  } catch (const std::exception& e) {
+    err = e.what();
+    st = PDF_CUDA_ERROR;
+  }
+  if (st != PDF_OK) pdfb::set_global_error(err);
+  return st;
+}

@@ -282,6 +282,28 @@ int pdf_detect_self_collisions(const double* positions, int32_t n_vertices,
                                double tolerance, pdf_contact* out, int32_t cap,
                                int32_t* n, int32_t device);
 
+/* Allocation-free variant of pdf_detect_candidates.  It has no counterpart in
+ * the reference.  For callers that must not allocate device memory when they
+ * detect (code inside another framework's memory pool, real-time loops with a
+ * fixed memory budget, hosts whose allocator is not the CUDA runtime's): the
+ * whole workspace is one fixed, file-scope device array (about 30 MB, held by
+ * every GPU that loads this library until the process exits); the call makes
+ * no cudaMalloc / cudaFree and no allocating library call.
+ *   positions (3*n_vertices doubles), triangles (3*n_triangles) and pairs
+ *   (2*cap int32) are DEVICE pointers on the current device; *n (host)
+ *   receives the number of candidate pairs, written sorted by (vertex,
+ *   triangle) exactly as pdf_detect_candidates returns them.
+ *   Limits: n_triangles <= 65536 and at most 262144 candidate pairs; larger
+ *   inputs return PDF_CAPACITY_EXCEEDED without touching pairs.
+ *   The first call on a device looks up the array's device address; make that
+ *   first call before any stream capture.  All calls share the one array:
+ *   calls that overlap on the GPU (other streams, other host threads) race.
+ *   The call synchronises cuda_stream (NULL = the legacy default stream). */
+int pdf_detect_candidates_noalloc(const double* positions, int32_t n_vertices,
+                                  const int32_t* triangles, int32_t n_triangles,
+                                  double tolerance, int32_t* pairs, int32_t cap,
+                                  int32_t* n, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
