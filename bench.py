@@ -88,7 +88,10 @@ class ClockSampler:
 
 def build_workload(args):
     from climatenet_b200 import abi, scenes
-    s, pk, _ = scenes.workload(3, n_override=args.n)
+    if args.workload == "batch":
+        s, _, pk = scenes.batch_scene(n_instances=64, seed=4)
+    else:
+        s, pk, _ = scenes.workload(3, n_override=args.n)
     pk = dict(pk)
     if args.precision == "fp32":
         pk["precision"] = abi.PDF_FP32_REFINE
@@ -96,6 +99,9 @@ def build_workload(args):
 
 
 def workload_name(args):
+    if args.workload == "batch":
+        return ("64 independent cloths, n ~ U{20..150} (seed 4), each over its own sphere R ~ U[0.2, 0.5], "
+                "mu ~ U[0.1, 0.8], dt=2.5e-3, 20 PD iterations/step, stepped as one block-diagonal scene")
     return ("%dx%d cloth (%d vertices) on a sphere R=0.5 m rotating about z at 1 rad/s, mu=0.5, "
             "self-collision tol 2 mm, dt=2e-3, 20 PD iterations/step" % (args.n, args.n, args.n * args.n))
 
@@ -141,6 +147,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--n", type=int, default=500)
+    ap.add_argument("--workload", default="cloth", choices=["cloth", "batch"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     args = ap.parse_args()

@@ -44,6 +44,7 @@ class pdf_obstacle(C.Structure):
         ("point", C.c_double * 3), ("normal", C.c_double * 3),
         ("n_vertices", C.c_int32), ("n_triangles", C.c_int32),
         ("vertices", _dp), ("triangles", _ip), ("threshold", C.c_double),
+        ("mesh", C.c_int32),
     ]
 
 
@@ -103,7 +104,8 @@ class pdf_stats(C.Structure):
         ("factor_nnz", C.c_int64), ("n_supernodes", C.c_int32),
         ("n_levels", C.c_int32), ("lhs_nnz", C.c_int64),
         ("n_constraint_rows", C.c_int32), ("kernel_launches", C.c_int64),
-        ("factor_nnz_true", C.c_int64),
+        ("factor_nnz_true", C.c_int64), ("sweep_chunk", C.c_int32),
+        ("sweep_chunk_ms", C.c_double * 3),
     ]
 
 

@@ -51,31 +51,39 @@ constexpr int kThreads = 256;
 inline int blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kThreads - 1) / kThreads); }
 constexpr int kStrideBlocks = 592;  // 4 x 148 SMs for grid-stride kernels
 
-// Work items of one sweep are at most 32 x kChunk elements.
-constexpr int kChunk = 64;
+// Work items of one sweep are at most 32 x chunk elements; the chunk is
+// chosen per scene by the autotuner in create_impl among these.
+constexpr int kChunk = 64;  // host emulation check (pdf_factor_check)
+constexpr int kChunkCandidates[3] = {32, 64, 128};
 
 // Work-item lists of the two sweeps in elimination-tree order (forward:
-// levels bottom-up, backward: top-down), one item per tile and chunk.
-void build_schedule(pdf_handle* h) {
+// levels bottom-up, backward: top-down), one item per tile and chunk.  The
+// completion counters are cumulative per schedule, so they restart here.
+void build_schedule(pdf_handle* h, int chunk) {
   const Factor& f = h->fac;
   std::vector<SweepTask> fa, ba;
   std::vector<SnInfo> sn;
-  build_sweep_tasks(f, kChunk, fa, ba, sn);
+  build_sweep_tasks(f, chunk, fa, ba, sn);
+  if (h->d.ftasks) cudaFree(h->d.ftasks);
+  if (h->d.btasks) cudaFree(h->d.btasks);
+  if (h->d.sn) cudaFree(h->d.sn);
   h->d.ftasks = upload(fa);
   h->d.btasks = upload(ba);
   h->d.nf = (int)fa.size();
   h->d.nb = (int)ba.size();
   h->d.sn = upload(sn);
-  h->d.rows = upload(f.rows);
+  if (!h->d.rows) h->d.rows = upload(f.rows);
   h->n_levels = f.n_levels;
   // dependency counters start at zero, the solve counter at one
   SweepSync& sy = h->d.sync;
-  sy.queue = dalloc<int>(2);
-  sy.epoch = dalloc<unsigned long long>(1);
-  sy.fdone = dalloc<unsigned long long>(f.n_sn);
-  sy.fchild = dalloc<unsigned long long>(f.n_sn);
-  sy.bdone = dalloc<unsigned long long>(f.n_sn);
-  sy.err = dalloc<int>(1);
+  if (!sy.queue) {
+    sy.queue = dalloc<int>(2);
+    sy.epoch = dalloc<unsigned long long>(1);
+    sy.fdone = dalloc<unsigned long long>(f.n_sn);
+    sy.fchild = dalloc<unsigned long long>(f.n_sn);
+    sy.bdone = dalloc<unsigned long long>(f.n_sn);
+    sy.err = dalloc<int>(1);
+  }
   CK(cudaMemset(sy.queue, 0, 2 * sizeof(int)));
   const unsigned long long one = 1ULL;
   CK(cudaMemcpy(sy.epoch, &one, sizeof(one), cudaMemcpyHostToDevice));
@@ -84,6 +92,8 @@ void build_schedule(pdf_handle* h) {
   CK(cudaMemset(sy.bdone, 0, f.n_sn * sizeof(unsigned long long)));
   CK(cudaMemset(sy.err, 0, sizeof(int)));
 }
+
+void autotune_schedule(pdf_handle* h);
 
 void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   auto t0 = std::chrono::steady_clock::now();
@@ -94,7 +104,6 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   h->prm = *p;
   h->fp32 = p->precision == PDF_FP32_REFINE;
   if (p->precision != PDF_FP64 && p->precision != PDF_FP32_REFINE) throw std::invalid_argument("unknown precision mode");
-  if (sc->n_obstacles > kMaxObstacles) throw std::invalid_argument("at most 8 obstacles are supported");
   build_model(*sc, *p, h->model);
   const Model& m = h->model;
   std::string ferr;
@@ -150,12 +159,14 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   dm.iperm = d.iperm;
   // obstacles
   h->obs.n = (int)m.obstacles.size();
+  h->host_obs.assign(h->obs.n, DObstacle{});
   for (int k = 0; k < h->obs.n; ++k) {
     const pdf_obstacle& o = m.obstacles[k];
-    DObstacle& ob = h->obs.o[k];
-    ob = DObstacle{};
+    DObstacle& ob = h->host_obs[k];
     ob.type = o.type;
     ob.material = o.material;
+    ob.mesh = o.mesh;
+    if (o.mesh >= (int)m.meshes.size()) throw std::invalid_argument("obstacle mesh out of range");
     for (int c = 0; c < 3; ++c) {
       ob.c[c] = o.center[c];
       ob.p[c] = o.point[c];
@@ -196,6 +207,10 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
     }
     h->host_time_before_start.push_back(o.rotation_start_time);
   }
+  d.obstacles = dalloc<DObstacle>(std::max(1, h->obs.n));
+  d.vmesh = upload(m.vmesh);
+  h->obs.o = d.obstacles;
+  h->obs.vmesh = d.vmesh;
   // state
   d.q = upload(m.q0);
   d.v = upload(m.v0);
@@ -204,7 +219,7 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   d.cstep = dalloc<double>(3 * (size_t)N);
   d.bp = dalloc<double>(3 * (size_t)std::max(1, dm.B));
   // solve
-  build_schedule(h);
+  build_schedule(h, kChunk);
   if (h->fp32) {
     d.Wf32 = upload(std::vector<float>(f.Wf.begin(), f.Wf.end()));
     d.Wb32 = upload(std::vector<float>(f.Wb.begin(), f.Wb.end()));
@@ -286,6 +301,10 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
     if (st != PDF_OK) throw CudaFail("self-collision workspace: " + h->err);
   }
   CK(cudaDeviceSynchronize());
+  autotune_schedule(h);
+  // the timing solves overwrote v and q^k: restore the initial state
+  CK(cudaMemcpy(d.v, m.v0.data(), m.v0.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d.qk, m.q0.data(), m.q0.size() * sizeof(double), cudaMemcpyHostToDevice));
   h->stats.factor_ms = f.factor_ms;
   h->stats.factor_nnz = f.nnz_w;
   h->stats.factor_nnz_true = f.nnz_l_true;
@@ -314,6 +333,57 @@ void launch_solve(pdf_handle* h, T* b, T* y, T* x, const T* Wf, const T* Wb, int
   DeviceBuffers& d = h->d;
   launch_solve_sweeps<T>(h->stream, d.ftasks, d.nf, d.btasks, d.nb, d.sn, d.rows, Wf, Wb, b, y, x, h->dm.N, d.sync);
   launch_solve_post<T>(h->stream, h->dm.N, d.perm, x, y, d.v, d.qk, d.q, h->prm.time_step, mode, d.sync);
+}
+
+// Schedule autotuner: times the global solve with each candidate work-item
+// width on this scene's factor (zero right-hand side: the sweeps read the
+// same data and wait on the same dependencies whatever the values) and keeps
+// the fastest.
+void autotune_schedule(pdf_handle* h) {
+  DeviceBuffers& d = h->d;
+  const int N = h->dm.N;
+  cudaStream_t st = h->stream;
+  double best = 1e300;
+  int best_chunk = kChunk;
+  for (int ci = 0; ci < 3; ++ci) {
+    const int chunk = kChunkCandidates[ci];
+    build_schedule(h, chunk);
+    double total = 0.;
+    for (int r = 0; r < 4; ++r) {
+      if (h->fp32) {
+        CK(cudaMemsetAsync(d.b32, 0, 3 * (size_t)N * sizeof(float), st));
+        launch_solve_prep<float>(st, N, d.x32, d.y32, d.sync);
+      } else {
+        CK(cudaMemsetAsync(d.b64, 0, 3 * (size_t)N * sizeof(double), st));
+        launch_solve_prep<double>(st, N, d.x64, d.y64, d.sync);
+      }
+      CK(cudaEventRecord(h->ev[5], st));
+      if (h->fp32)
+        launch_solve<float>(h, d.b32, d.y32, d.x32, d.Wf32, d.Wb32, 1);
+      else
+        launch_solve<double>(h, d.b64, d.y64, d.x64, d.Wf64, d.Wb64, 0);
+      CK(cudaEventRecord(h->ev[6], st));
+      CK(cudaEventSynchronize(h->ev[6]));
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]));
+      if (r > 0) total += ms;  // first run warms up
+    }
+    h->stats.sweep_chunk_ms[ci] = total / 3.;
+    if (total / 3. < best) {
+      best = total / 3.;
+      best_chunk = chunk;
+    }
+  }
+  build_schedule(h, best_chunk);
+  h->stats.sweep_chunk = best_chunk;
+  if (h->fp32)
+    launch_solve_prep<float>(st, N, d.x32, d.y32, d.sync);
+  else
+    launch_solve_prep<double>(st, N, d.x64, d.y64, d.sync);
+  int derr = 0;
+  CK(cudaMemcpy(&derr, d.sync.err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (derr) throw CudaFail("a supernodal sweep gave up waiting for a dependency while tuning");
+  CK(cudaStreamSynchronize(st));
 }
 
 // One PD iteration (SimulationBase.cpp:119-157): local step + friction
@@ -369,7 +439,8 @@ void step_once(pdf_handle* h, bool want_report) {
                                                   h->prm.gravity[1], h->prm.gravity[2], dt);
   // obstacle detection on the start-of-step positions (SimulationBase.cpp:333-366)
   if (h->obs.n > 0) {
-    for (int k = 0; k < h->obs.n; ++k) h->obs.o[k].time_before_start = h->host_time_before_start[k];
+    for (int k = 0; k < h->obs.n; ++k) h->host_obs[k].time_before_start = h->host_time_before_start[k];
+    CK(cudaMemcpyAsync(d.obstacles, h->host_obs.data(), h->obs.n * sizeof(DObstacle), cudaMemcpyHostToDevice, st));
     k_obstacle_flags<<<blocks_for(N), kThreads, 0, st>>>(N, d.q, h->obs, d.flags);
     thrust::counting_iterator<int> it(0);
     CK(cub::DeviceSelect::Flagged(d.cub_tmp, d.cub_tmp_bytes, it, d.flags, d.sel_idx, d.c.n_contacts,
@@ -394,7 +465,26 @@ void step_once(pdf_handle* h, bool want_report) {
   CK(cudaEventRecord(h->ev[2], st));
   CK(cudaMemsetAsync(d.ac_hist, 0, 4 * (size_t)K * sizeof(double), st));
   // iterations
-  if (h->prm.use_graph) {
+  int iters = K;
+  if (h->prm.residual_tolerance > 0.) {
+    // iterate to tolerance: stop after the first iteration whose mean
+    // Alart-Curnier residual is at or below the tolerance (LocalGlobal caps it)
+    int counts[2];
+    CK(cudaMemcpyAsync(&counts[0], d.c.n_contacts, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&counts[1], d.c.n_self, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const int nc = counts[0] + counts[1];
+    iters = 0;
+    while (iters < K) {
+      launch_iterations(h, iters, iters + 1);
+      ++iters;
+      if (nc == 0) continue;
+      double sum = 0.;
+      CK(cudaMemcpyAsync(&sum, d.ac_hist + 4 * (size_t)(iters - 1), sizeof(double), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      if (sum / nc <= h->prm.residual_tolerance) break;
+    }
+  } else if (h->prm.use_graph) {
     if (!h->graph) {
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
@@ -417,8 +507,9 @@ void step_once(pdf_handle* h, bool want_report) {
   for (auto& t : h->host_time_before_start) t -= dt;
   h->time += dt;
   h->stats.steps += 1;
-  h->stats.iterations += K;
-  h->stats.kernel_launches += launches_per_step_extra(h) + K * launches_per_iteration(h);
+  h->stats.iterations += iters;
+  h->stats.kernel_launches += launches_per_step_extra(h) + iters * launches_per_iteration(h);
+  h->last_iters = iters;
   if (want_report) {
     CK(cudaStreamSynchronize(st));
     float a, b, cc, dd;
@@ -437,17 +528,18 @@ void step_once(pdf_handle* h, bool want_report) {
     std::vector<double> hist(4 * (size_t)K);
     CK(cudaMemcpy(hist.data(), d.ac_hist, hist.size() * sizeof(double), cudaMemcpyDeviceToHost));
     const int nc = counts[0] + counts[1];
-    h->residual_hist.resize(K);
-    for (int k = 0; k < K; ++k) h->residual_hist[k] = nc ? hist[4 * k] / nc : 0.;
+    h->residual_hist.resize(iters);
+    for (int k = 0; k < iters; ++k) h->residual_hist[k] = nc ? hist[4 * k] / nc : 0.;
     pdf_step_report& r = h->last;
     r.n_contacts = counts[0];
     r.n_self_contacts = counts[1];
     r.n_levels = counts[2];
-    r.iterations = K;
-    r.residual = nc ? hist[4 * (K - 1)] / nc : 0.;
-    r.residual_max = hist[4 * (K - 1) + 1];
-    r.normal_residual = nc ? hist[4 * (K - 1) + 2] / nc : 0.;
-    r.tangential_residual = nc ? hist[4 * (K - 1) + 3] / nc : 0.;
+    r.iterations = iters;
+    const int kl = std::max(iters, 1) - 1;
+    r.residual = nc ? hist[4 * kl] / nc : 0.;
+    r.residual_max = hist[4 * kl + 1];
+    r.normal_residual = nc ? hist[4 * kl + 2] / nc : 0.;
+    r.tangential_residual = nc ? hist[4 * kl + 3] / nc : 0.;
     r.time = h->time;
   }
 }
@@ -488,7 +580,8 @@ void free_handle(pdf_handle* h) {
   DeviceBuffers& d = h->d;
   void* ptrs[] = {d.mass, d.ring_kappa, d.ring_bend, d.self_bend, d.ring_ptr, d.ring_idx, d.bend_of, d.bend_ptr,
                   d.bend_idx, d.bend_coef, d.bend_w, d.bend_rest, d.pin_term, d.ata_ptr, d.ata_col, d.ata_val,
-                  d.perm, d.iperm, d.vmat, d.friction, d.tris, d.q, d.v, d.tn, d.qk, d.cstep, d.bp, d.ftasks,
+                  d.perm, d.iperm, d.vmat, d.friction, d.tris, d.obstacles, d.vmesh, d.q, d.v, d.tn, d.qk,
+                  d.cstep, d.bp, d.ftasks,
                   d.btasks, d.sn, d.rows, d.Wf64, d.Wb64, d.Wf32, d.Wb32, d.sync.queue, d.sync.epoch,
                   d.sync.fdone, d.sync.fchild, d.sync.bdone, d.sync.err, d.b64, d.y64, d.x64, d.b32, d.y32,
                   d.x32, d.flags, d.sel_idx, d.cub_tmp, d.newf, d.ac_hist, d.c.n_contacts, d.c.c_vertex,

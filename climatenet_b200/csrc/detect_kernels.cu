@@ -18,10 +18,13 @@ __global__ void k_obstacle_flags(int N, const double* __restrict__ q, DObstacles
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= N) return;
   const double3 x = ld3(q, i);
+  const int mi = obs.vmesh[i];
   for (int o = 0; o < obs.n; ++o) {
     const DObstacle& ob = obs.o[o];
     bool hit = false;
-    if (ob.type == 0 || ob.type == 1) {
+    if (ob.mesh >= 0 && ob.mesh != mi) {
+      hit = false;  // obstacle restricted to another mesh
+    } else if (ob.type == 0 || ob.type == 1) {
       // Sphere::isInside Sphere.cpp:93-98 (hard-coded 1 cm margin)
       const double3 r = x - make_double3(ob.c[0], ob.c[1], ob.c[2]);
       hit = sqrt(dot3(r, r)) < ob.R + 1e-2;

@@ -25,6 +25,8 @@ struct DeviceBuffers {
   int* tris = nullptr;  // 3T scene-global
   std::vector<double*> obstacle_v;
   std::vector<int*> obstacle_t;
+  DObstacle* obstacles = nullptr;
+  int* vmesh = nullptr;
   // state
   double *q = nullptr, *v = nullptr, *tn = nullptr, *qk = nullptr, *cstep = nullptr, *bp = nullptr;
   // solve
@@ -58,6 +60,7 @@ struct pdf_handle {
   pdfb::DeviceBuffers d;
   pdfb::DModel dm{};
   pdfb::DObstacles obs{};
+  std::vector<pdfb::DObstacle> host_obs;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[8] = {};
   cudaGraphExec_t graph = nullptr;
@@ -69,6 +72,7 @@ struct pdf_handle {
   pdf_step_report last{};
   pdf_stats stats{};
   std::vector<double> residual_hist;
+  int last_iters = 0;
   std::vector<double> host_time_before_start;
   bool fp32 = false;
 };

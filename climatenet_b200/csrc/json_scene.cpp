@@ -396,6 +396,7 @@ int pdf_scene_load_json(const char* json_path, pdf_scene** out) {
     for (const JVal& oo : obs.a) {
       const std::string& type = req_string(oo, "Type");
       pdf_obstacle ob{};
+      ob.mesh = -1;  // the reference's obstacles act on every dynamic mesh
       std::vector<double> ov;
       std::vector<int> ot;
       if (type == "Sphere") {

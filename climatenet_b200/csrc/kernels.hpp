@@ -18,10 +18,10 @@ struct SweepSync {
   int* err;                    // set when a dependency wait gives up
 };
 
-// Analytic and mesh obstacles, passed by value.
-constexpr int kMaxObstacles = 8;
+// Analytic and mesh obstacles (device array, refreshed every step for the
+// rotating spheres' clocks).
 struct DObstacle {
-  int type, material, n_tri, pad;
+  int type, material, n_tri, mesh;  // mesh: -1 = every dynamic mesh
   double c[3], R;
   double rot[3], time_before_start;
   double p[3], n[3];
@@ -31,7 +31,8 @@ struct DObstacle {
 };
 struct DObstacles {
   int n;
-  DObstacle o[kMaxObstacles];
+  const DObstacle* o;
+  const int* vmesh;  // containing mesh of every vertex
 };
 
 __global__ void k_step_init(DModel m, const double* q, double* v, double* tn, double* qk, double* cstep, double gx,

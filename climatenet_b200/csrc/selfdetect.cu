@@ -83,17 +83,34 @@ __device__ __forceinline__ double from_ord(unsigned long long u) {
   return __longlong_as_double((long long)u);
 }
 
+// Bounding box of the vertices (order-preserving integer images of the
+// coordinates): warp and block reductions, then one atomic per block and bound.
 __global__ void k_bbox(int nv, const double* __restrict__ q, unsigned long long* bbox) {
-  unsigned long long lo[3] = {~0ULL, ~0ULL, ~0ULL}, hi[3] = {0ULL, 0ULL, 0ULL};
+  __shared__ unsigned long long red[6][32];
+  unsigned long long v[6] = {~0ULL, ~0ULL, ~0ULL, 0ULL, 0ULL, 0ULL};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nv; i += gridDim.x * blockDim.x)
     for (int c = 0; c < 3; ++c) {
       unsigned long long u = ord_bits(q[3 * (int64_t)i + c]);
-      lo[c] = min(lo[c], u);
-      hi[c] = max(hi[c], u);
+      v[c] = min(v[c], u);
+      v[3 + c] = max(v[3 + c], u);
     }
-  for (int c = 0; c < 3; ++c) {
-    atomicMin(bbox + c, lo[c]);
-    atomicMax(bbox + 3 + c, hi[c]);
+  for (int o = 16; o > 0; o >>= 1)
+    for (int c = 0; c < 3; ++c) {
+      v[c] = min(v[c], __shfl_xor_sync(0xffffffffu, v[c], o));
+      v[3 + c] = max(v[3 + c], __shfl_xor_sync(0xffffffffu, v[3 + c], o));
+    }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  if (lane == 0)
+    for (int c = 0; c < 6; ++c) red[c][warp] = v[c];
+  __syncthreads();
+  if (threadIdx.x < 6) {
+    const int c = threadIdx.x;
+    unsigned long long r = red[c][0];
+    for (int k = 1; k < nw; ++k) r = c < 3 ? min(r, red[c][k]) : max(r, red[c][k]);
+    if (c < 3)
+      atomicMin(bbox + c, r);
+    else
+      atomicMax(bbox + c, r);
   }
 }
 

@@ -333,7 +333,23 @@ __global__ void k_alart_curnier(DContacts c, const double* __restrict__ v, doubl
     st += __shfl_xor_sync(0xffffffffu, st, o);
     mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   }
-  if ((threadIdx.x & 31) == 0 && (C + S) > 0) {
+  // block reduction, then one set of atomics per block that had work
+  __shared__ double red[4][32];
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][warp] = s;
+    red[1][warp] = mx;
+    red[2][warp] = sn;
+    red[3][warp] = st;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && (int64_t)blockIdx.x * blockDim.x < (int64_t)(C + S)) {
+    for (int k = 1; k < nw; ++k) {
+      s += red[0][k];
+      mx = fmax(mx, red[1][k]);
+      sn += red[2][k];
+      st += red[3][k];
+    }
     atomicAdd(acc, s);
     atomic_max_pos(acc + 1, mx);
     atomicAdd(acc + 2, sn);

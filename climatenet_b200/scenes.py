@@ -139,6 +139,7 @@ class Scene:
             ob = obs[k]
             ob.type = o["type"]
             ob.material = o.get("material", 0)
+            ob.mesh = o.get("mesh", -1)
             for key in ("center", "axis", "point", "normal"):
                 if key in o:
                     for c in range(3):
@@ -211,18 +212,42 @@ def workload(cfg, n_override=None):
     raise ValueError("unknown workload %r" % (cfg,))
 
 
-def batch_workload(n_instances=64, seed=4):
+def batch_instances(n_instances=64, seed=4):
     """Batching shape: instances with n ~ U{20..150}, R ~ U[0.2, 0.5],
     mu ~ U[0.1, 0.8], height above the sphere top ~ U[0.1, 0.5] (numpy PCG64,
-    seed 4).  Returns a list of (Scene, params kwargs)."""
+    seed 4).  Returns a list of dicts (n, R, mu, h)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     out = []
     for _ in range(n_instances):
-        n = int(rng.integers(20, 151))
-        R = float(rng.uniform(0.2, 0.5))
-        mu = float(rng.uniform(0.1, 0.8))
-        h = float(rng.uniform(0.1, 0.5))
-        s = cloth_on_sphere(n=n, side=1.0, z=h, mu=mu, sphere_center=(0, 0, -R),
-                            sphere_radius=R)
-        out.append((s, dict(time_step=2.5e-3, iterations=20)))
+        out.append(dict(n=int(rng.integers(20, 151)), R=float(rng.uniform(0.2, 0.5)),
+                        mu=float(rng.uniform(0.1, 0.8)), h=float(rng.uniform(0.1, 0.5))))
     return out
+
+
+def instance_scene(inst):
+    """One instance of the batch as a scene of its own (for parity checks)."""
+    s = cloth_on_sphere(n=inst["n"], side=1.0, z=inst["h"], mu=inst["mu"],
+                        sphere_center=(0, 0, -inst["R"]), sphere_radius=inst["R"])
+    return s
+
+
+def batch_scene(n_instances=64, seed=4, spacing=3.0):
+    """All instances of the batch as ONE scene: instance k is mesh k (material
+    k) translated by a grid offset, with its own sphere restricted to mesh k
+    (material n_instances + k, friction table entry [k][n_instances + k] =
+    mu_k).  The global matrix is block diagonal, so one factorisation and one
+    set of launches per PD iteration step every instance together."""
+    insts = batch_instances(n_instances, seed)
+    m = len(insts)
+    fr = np.zeros((2 * m, 2 * m))
+    for k, it in enumerate(insts):
+        fr[k, m + k] = it["mu"]
+    s = Scene(friction=fr)
+    side = int(np.ceil(np.sqrt(m)))
+    for k, it in enumerate(insts):
+        ox, oy = spacing * (k % side), spacing * (k // side)
+        p, t = grid_mesh(it["n"], 1.0, z=it["h"], center=(ox, oy))
+        s.add_mesh(p, t, area_density=0.1, bending=1e-2, stretching=1e3, material=k)
+        s.obstacles.append(dict(type=abi.PDF_OBSTACLE_SPHERE, center=(ox, oy, -it["R"]), radius=it["R"],
+                                material=m + k, mesh=k))
+    return s, insts, dict(time_step=2.5e-3, iterations=20)

@@ -59,6 +59,9 @@ typedef struct pdf_obstacle {
   const double* vertices;       /* mesh obstacle: 3*n_vertices doubles        */
   const int32_t* triangles;     /* mesh obstacle: 3*n_triangles indices       */
   double threshold;             /* mesh obstacle: "Threshold"                 */
+  int32_t mesh;                 /* -1: acts on every dynamic mesh (the
+                                   reference's behaviour); >= 0: only on that
+                                   mesh (batches of independent cloths)       */
 } pdf_obstacle;
 
 /* ---- dynamic meshes (include/physics/PhysicMesh.hpp, PhysicParameters) -- */
@@ -157,6 +160,8 @@ typedef struct pdf_stats {
   int32_t n_constraint_rows;        /* rows(A)                                  */
   int64_t kernel_launches;          /* this library's kernels launched so far   */
   int64_t factor_nnz_true;          /* structural nnz(L) without padding        */
+  int32_t sweep_chunk;              /* work-item width chosen by the autotuner  */
+  double sweep_chunk_ms[3];         /* solve time measured for 32, 64, 128      */
 } pdf_stats;
 
 /* One contact, as the reference's CollisionInfo / SelfCollisionInfo plus

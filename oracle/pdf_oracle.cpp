@@ -583,6 +583,7 @@ struct Obstacle {
   std::vector<V3> mverts;
   std::vector<std::array<int, 3>> mtris;
   double threshold;
+  int mesh; /* -1: every dynamic mesh; else only vertices of that mesh */
 };
 
 struct CInfo {
@@ -856,6 +857,7 @@ static void detect_obstacles(Sim& s) {
       }
     }
     for (auto& c : found) {
+      if (ob.mesh >= 0 && s.vmesh[c.vertex] != ob.mesh) continue;
       int mm = s.meshes[s.vmesh[c.vertex]].material;
       c.mu = s.friction[(size_t)mm * s.n_mat + ob.material];
       s.contacts.push_back(c);
@@ -1277,6 +1279,8 @@ static void build(Sim& s, const pdf_scene_desc* sc, const pdf_params* p) {
     ob.point = {o.point[0], o.point[1], o.point[2]};
     ob.normal = normalized(V3{o.normal[0], o.normal[1], o.normal[2]});
     ob.threshold = o.threshold;
+    ob.mesh = o.mesh;
+    if (ob.mesh >= sc->n_meshes) throw std::invalid_argument("obstacle mesh out of range");
     if (o.type == PDF_OBSTACLE_MESH) {
       for (int i = 0; i < o.n_vertices; ++i) ob.mverts.push_back(ld(o.vertices, i));
       for (int t = 0; t < o.n_triangles; ++t)
