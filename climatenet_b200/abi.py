@@ -31,6 +31,9 @@ PDF_FP32_REFINE = 1
 PDF_WARM_NONE = 0
 PDF_WARM_MLP = 1
 
+MLP_IN, MLP_HIDDEN, MLP_OUT = 10, 64, 3
+MLP_PARAMS = MLP_HIDDEN * MLP_IN + MLP_HIDDEN + MLP_HIDDEN * MLP_HIDDEN + MLP_HIDDEN + MLP_OUT * MLP_HIDDEN + MLP_OUT
+
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int32)
 
@@ -79,6 +82,7 @@ class pdf_params(C.Structure):
         ("warm_start", C.c_int32), ("refine_max", C.c_int32),
         ("refine_tolerance", C.c_double), ("device", C.c_int32),
         ("contact_capacity", C.c_int32), ("use_graph", C.c_int32),
+        ("mlp_weights", C.c_char * 256),
     ]
 
 
@@ -120,7 +124,7 @@ class pdf_contact(C.Structure):
 def params(time_step=5e-3, iterations=20, self_collision=False, self_tol=0.0,
            gravity=(0.0, 0.0, -9.81), air_damping=0.0, precision=PDF_FP64,
            residual_tolerance=0.0, warm_start=PDF_WARM_NONE, refine_max=4,
-           refine_tolerance=1e-10, device=0, contact_capacity=0, use_graph=1):
+           refine_tolerance=1e-10, device=0, contact_capacity=0, use_graph=1, mlp_weights=""):
     """Build a pdf_params with the reference's meaning for each field."""
     p = pdf_params()
     p.time_step = time_step
@@ -138,6 +142,7 @@ def params(time_step=5e-3, iterations=20, self_collision=False, self_tol=0.0,
     p.device = device
     p.contact_capacity = contact_capacity
     p.use_graph = use_graph
+    p.mlp_weights = mlp_weights.encode() if isinstance(mlp_weights, str) else bytes(mlp_weights)
     return p
 
 

@@ -10,6 +10,8 @@
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
 #include <fstream>
+#include <ios>
+#include <random>
 #include <stdexcept>
 #include <string>
 
@@ -94,6 +96,58 @@ void build_schedule(pdf_handle* h, int chunk) {
 }
 
 void autotune_schedule(pdf_handle* h);
+
+// Warm-start feature / prediction buffers and the impulse memory.
+void ensure_mlp_buffers(pdf_handle* h) {
+  if (h->mlp_X) return;
+  const size_t cc = h->cap_contacts;
+  h->mlp_X = dalloc<float>(kMlpIn * cc);
+  h->mlp_Y = dalloc<float>(kMlpOut * cc);
+  h->rprev = dalloc<double>(3 * (size_t)h->dm.N);
+  h->rprev_tag = dalloc<int>(h->dm.N);
+  CK(cudaMemset(h->rprev, 0, 3 * (size_t)h->dm.N * sizeof(double)));
+  CK(cudaMemset(h->rprev_tag, 0x80, h->dm.N * sizeof(int)));  // large negative tags: no memory yet
+}
+
+// Weights file: "PDFMLP01", int32 {in, hidden, out, count}, count floats.
+constexpr char kMlpMagic[8] = {'P', 'D', 'F', 'M', 'L', 'P', '0', '1'};
+void load_weights_file(const std::string& path, float* w) {
+  std::ifstream in(path, std::ios::binary);
+  if (!in) throw std::ios_base::failure("cannot open MLP weights file " + path);
+  char magic[8];
+  int32_t hdr[4];
+  in.read(magic, 8);
+  in.read(reinterpret_cast<char*>(hdr), sizeof(hdr));
+  if (!in || std::memcmp(magic, kMlpMagic, 8) != 0) throw std::ios_base::failure("not an MLP weights file: " + path);
+  if (hdr[0] != kMlpIn || hdr[1] != kMlpHidden || hdr[2] != kMlpOut || hdr[3] != kMlpParams)
+    throw std::invalid_argument("MLP weights file has another network shape: " + path);
+  in.read(reinterpret_cast<char*>(w), kMlpParams * sizeof(float));
+  if (!in) throw std::ios_base::failure("truncated MLP weights file " + path);
+  for (int i = 0; i < kMlpParams; ++i)
+    if (!std::isfinite(w[i])) throw std::invalid_argument("non-finite value in MLP weights file " + path);
+}
+
+// Seeded He initialisation: W ~ N(0, 2 / fan_in) (output layer scaled by 0.1), b = 0.
+void mlp_init_host(float* w, uint64_t seed) {
+  std::mt19937_64 rng(seed);
+  std::normal_distribution<double> nd(0., 1.);
+  int o = 0;
+  auto layer = [&](int nout, int nin, double scale) {
+    const double sd = scale * std::sqrt(2. / nin);
+    for (int i = 0; i < nout * nin; ++i) w[o++] = (float)(sd * nd(rng));
+    for (int i = 0; i < nout; ++i) w[o++] = 0.f;
+  };
+  layer(kMlpHidden, kMlpIn, 1.);
+  layer(kMlpHidden, kMlpHidden, 1.);
+  layer(kMlpOut, kMlpHidden, 0.1);
+}
+
+double gravity_dt(const pdf_handle* h) {
+  const double* g = h->prm.gravity;
+  double gn = std::sqrt((g[0] * g[0] + g[1] * g[1]) + g[2] * g[2]);
+  if (!(gn > 1e-12)) gn = 1e-12;
+  return gn * h->prm.time_step;
+}
 
 void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   auto t0 = std::chrono::steady_clock::now();
@@ -236,8 +290,12 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
     launch_solve_prep<double>(h->stream, N, d.x64, d.y64, d.sync);
   }
   // contacts
-  const int nobs = std::max(1, h->obs.n);
-  h->cap_contacts = p->contact_capacity > 0 ? p->contact_capacity : nobs * N;
+  // at most one contact per (obstacle, vertex of the meshes it acts on)
+  int64_t cap_auto = 0;
+  for (const DObstacle& ob : h->host_obs) cap_auto += ob.mesh >= 0 ? m.meshes[ob.mesh].n_vertices : N;
+  cap_auto = std::max<int64_t>(1, cap_auto);
+  if (cap_auto > (int64_t)INT32_MAX) throw std::overflow_error("contact capacity above 2^31");
+  h->cap_contacts = p->contact_capacity > 0 ? p->contact_capacity : (int)cap_auto;
   h->cap_self = p->contact_capacity > 0 ? p->contact_capacity : 2 * N;
   DContacts& c = d.c;
   c.cap = h->cap_contacts;
@@ -261,6 +319,9 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   CK(cudaMemset(c.c_force, 0, 3 * cc * sizeof(double)));
   c.c_ac = dalloc<double>(cc);
   c.c_slot = dalloc<int>(cc);
+  c.c_gap = dalloc<double>(cc);
+  c.c_active = dalloc<int>(cc);
+  CK(cudaMemset(c.c_active, 0, cc * sizeof(int)));
   c.s_vertex = dalloc<int>(cs);
   c.s_partner = dalloc<int>(cs);
   c.s_face = dalloc<int>(3 * cs);
@@ -286,7 +347,13 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
     CK(cudaMemset(c.sf[k], 0, 3 * (size_t)N * sizeof(double)));
   }
   d.newf = dalloc<double>(3 * cs);
-  d.ac_hist = dalloc<double>(4 * (size_t)p->local_global_iterations);
+  d.ac_hist = dalloc<double>(4 * (size_t)std::max(1, p->local_global_iterations));
+  d.iter = dalloc<int>(1);
+  d.iter_total = dalloc<long long>(1);
+  d.blocks_done = dalloc<unsigned int>(1);
+  CK(cudaMemset(d.iter, 0, sizeof(int)));
+  CK(cudaMemset(d.iter_total, 0, sizeof(long long)));
+  CK(cudaMemset(d.blocks_done, 0, sizeof(unsigned int)));
   if (h->obs.n > 0) {
     const int nitems = h->obs.n * N;
     d.flags = dalloc<unsigned char>(nitems);
@@ -299,6 +366,20 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   if (p->self_collision) {
     int st = self_detect_init(h);
     if (st != PDF_OK) throw CudaFail("self-collision workspace: " + h->err);
+  }
+  // learned warm start
+  if (p->warm_start != PDF_WARM_NONE && p->warm_start != PDF_WARM_MLP) throw std::invalid_argument("unknown warm start");
+  h->mlp_w = dalloc<float>(kMlpParams);
+  if (p->warm_start == PDF_WARM_MLP) {
+    ensure_mlp_buffers(h);
+    const size_t len = strnlen(p->mlp_weights, sizeof(p->mlp_weights));
+    if (len == sizeof(p->mlp_weights)) throw std::invalid_argument("mlp_weights path is not terminated");
+    if (len > 0) {
+      std::vector<float> w(kMlpParams);
+      load_weights_file(std::string(p->mlp_weights, len), w.data());
+      CK(cudaMemcpy(h->mlp_w, w.data(), kMlpParams * sizeof(float), cudaMemcpyHostToDevice));
+      h->mlp_ready = true;
+    }
   }
   CK(cudaDeviceSynchronize());
   autotune_schedule(h);
@@ -388,18 +469,24 @@ void autotune_schedule(pdf_handle* h) {
 
 // One PD iteration (SimulationBase.cpp:119-157): local step + friction
 // (SFE::computeRhs), global solve (SimulationSpeed::solve), AC residual.
+// The iteration index comes from the device counter d.iter (advanced by the
+// AC kernel), so the same launches serve fixed and iterate-to-tolerance runs.
 template <typename T>
-void launch_iteration(pdf_handle* h, int k, T* b, T* y, T* x, const T* Wf, const T* Wb, int mode) {
+void launch_iteration(pdf_handle* h, T* b, T* y, T* x, const T* Wf, const T* Wb, int mode) {
   DeviceBuffers& d = h->d;
   const DModel& dm = h->dm;
   cudaStream_t st = h->stream;
   const int self_mode = h->prm.self_collision ? 1 : 0;
-  const int cur = k & 1, nxt = 1 - cur;
   launch_local<T>(h, b, mode);
-  launch_friction_obstacle<T>(kStrideBlocks, kThreads, st, dm, d.c, b, self_mode, cur, nxt);
-  if (self_mode) launch_friction_self<T>(1, 1024, st, dm, d.c, b, d.newf, cur, nxt);
+  // learned warm start: the first iteration of the step takes the predicted forces
+  const bool warm = h->prm.warm_start == PDF_WARM_MLP;
+  launch_friction_obstacle<T>(kStrideBlocks, kThreads, st, dm, d.c, b, self_mode, d.iter, warm ? h->mlp_Y : nullptr,
+                              warm ? gravity_dt(h) : 0.);
+  if (self_mode) launch_friction_self<T>(1, 1024, st, dm, d.c, b, d.newf, d.iter);
   launch_solve<T>(h, b, y, x, Wf, Wb, mode);
-  k_alart_curnier<<<kStrideBlocks, kThreads, 0, st>>>(d.c, d.v, d.ac_hist + 4 * (size_t)k);
+  IterCtl ctl{d.iter, d.iter_total, d.blocks_done, h->prm.residual_tolerance, h->prm.local_global_iterations,
+              h->capturing_cond ? 1 : 0, h->cond};
+  k_alart_curnier<<<kStrideBlocks, kThreads, 0, st>>>(d.c, d.v, d.ac_hist, ctl);
 }
 
 // Kernels of this library launched by one PD iteration (CUB's not counted):
@@ -408,23 +495,51 @@ int64_t launches_per_iteration(const pdf_handle* h) {
   return 6 + (h->dm.B > 0 ? 1 : 0) + (h->prm.self_collision ? 1 : 0);
 }
 
-// Per step outside the iterations: predictor, obstacle flags + materialise,
+// Per step outside the iterations: predictor, obstacle flags + clamp + materialise,
 // slots (2), slot reset, finalize; self-collision: register reset, per mesh
 // bbox/keys/build/refit/traverse/pair, bases, levels.
 int64_t launches_per_step_extra(const pdf_handle* h) {
-  int64_t n = 1 + (h->obs.n > 0 ? 2 : 0) + 2 + 1 + 1;
+  int64_t n = 1 + (h->obs.n > 0 ? 3 : 0) + 2 + 1 + 1;
   if (h->prm.self_collision) n += 1 + 6 * (int64_t)h->model.meshes.size() + 1 + 1;
+  // warm start: features, forward; record (clear + accumulate [+ count])
+  const bool warm = h->prm.warm_start == PDF_WARM_MLP;
+  if (warm || h->log_cap > 0) n += 1 + 2 + (h->log_cap > 0 ? 1 : 0) + (warm ? 1 : 0);
   return n;
 }
 
-void launch_iterations(pdf_handle* h, int k0, int k1) {
+void launch_iterations(pdf_handle* h, int count) {
   DeviceBuffers& d = h->d;
-  for (int k = k0; k < k1; ++k) {
+  for (int k = 0; k < count; ++k) {
     if (h->fp32)
-      launch_iteration<float>(h, k, d.b32, d.y32, d.x32, d.Wf32, d.Wb32, 1);
+      launch_iteration<float>(h, d.b32, d.y32, d.x32, d.Wf32, d.Wb32, 1);
     else
-      launch_iteration<double>(h, k, d.b64, d.y64, d.x64, d.Wf64, d.Wb64, 0);
+      launch_iteration<double>(h, d.b64, d.y64, d.x64, d.Wf64, d.Wb64, 0);
   }
+}
+
+// Iterate-to-tolerance graph: one conditional WHILE node whose body is one PD
+// iteration; the AC kernel's last block decides whether the body runs again.
+void build_tolerance_graph(pdf_handle* h) {
+  cudaGraph_t g;
+  CK(cudaGraphCreate(&g, 0));
+  CK(cudaGraphConditionalHandleCreate(&h->cond, g, 1, cudaGraphCondAssignDefault));
+  cudaGraphNodeParams np = {};
+  np.type = cudaGraphNodeTypeConditional;
+  np.conditional.handle = h->cond;
+  np.conditional.type = cudaGraphCondTypeWhile;
+  np.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, g, nullptr, 0, &np));
+  cudaGraph_t body = np.conditional.phGraph_out[0];
+  h->capturing_cond = true;
+  CK(cudaStreamBeginCaptureToGraph(h->stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  launch_iterations(h, 1);
+  cudaGraph_t captured;
+  const cudaError_t e = cudaStreamEndCapture(h->stream, &captured);
+  h->capturing_cond = false;
+  CK(e);
+  CK(cudaGraphInstantiate(&h->graph, g, 0));
+  CK(cudaGraphDestroy(g));
 }
 
 void step_once(pdf_handle* h, bool want_report) {
@@ -445,6 +560,7 @@ void step_once(pdf_handle* h, bool want_report) {
     thrust::counting_iterator<int> it(0);
     CK(cub::DeviceSelect::Flagged(d.cub_tmp, d.cub_tmp_bytes, it, d.flags, d.sel_idx, d.c.n_contacts,
                                   h->obs.n * N, st));
+    k_clamp_contacts<<<1, 1, 0, st>>>(d.c.n_contacts, d.c.cap, d.sync.err);
     k_obstacle_materialize<<<kStrideBlocks, kThreads, 0, st>>>(N, d.q, h->obs, d.sel_idx, d.vmat, d.friction,
                                                                h->model.n_materials, d.c);
   } else {
@@ -462,42 +578,63 @@ void step_once(pdf_handle* h, bool want_report) {
   k_contact_slots<<<kStrideBlocks, kThreads, 0, st>>>(d.c);
   k_contact_slots_fill<<<kStrideBlocks, kThreads, 0, st>>>(d.c);
   if (h->prm.self_collision) self_levels_step(h);
+  // learned warm start: features of every obstacle contact, predicted forces
+  const bool warm = h->prm.warm_start == PDF_WARM_MLP;
+  const bool mlp_features = warm || h->log_cap > 0;
+  if (mlp_features) {
+    launch_mlp_features(st, d.c, d.tn, d.mass, h->rprev, h->rprev_tag, h->mlp_tag - 1, h->prm.gravity, dt, h->mlp_X);
+    if (warm) mlp_forward_counted(h->mlp_w, h->mlp_X, d.c.n_contacts, h->cap_contacts, h->mlp_Y, st);
+  }
   CK(cudaEventRecord(h->ev[2], st));
   CK(cudaMemsetAsync(d.ac_hist, 0, 4 * (size_t)K * sizeof(double), st));
+  CK(cudaMemsetAsync(d.iter, 0, sizeof(int), st));
   // iterations
-  int iters = K;
+  int iters = -1;  // -1: known on the device only
   if (h->prm.residual_tolerance > 0.) {
     // iterate to tolerance: stop after the first iteration whose mean
     // Alart-Curnier residual is at or below the tolerance (LocalGlobal caps it)
-    int counts[2];
-    CK(cudaMemcpyAsync(&counts[0], d.c.n_contacts, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&counts[1], d.c.n_self, sizeof(int), cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    const int nc = counts[0] + counts[1];
-    iters = 0;
-    while (iters < K) {
-      launch_iterations(h, iters, iters + 1);
-      ++iters;
-      if (nc == 0) continue;
-      double sum = 0.;
-      CK(cudaMemcpyAsync(&sum, d.ac_hist + 4 * (size_t)(iters - 1), sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (h->prm.use_graph) {
+      if (!h->graph) build_tolerance_graph(h);
+      CK(cudaGraphLaunch(h->graph, st));
+    } else {
+      int counts[2];
+      CK(cudaMemcpyAsync(&counts[0], d.c.n_contacts, sizeof(int), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(&counts[1], d.c.n_self, sizeof(int), cudaMemcpyDeviceToHost, st));
       CK(cudaStreamSynchronize(st));
-      if (sum / nc <= h->prm.residual_tolerance) break;
+      const int nc = counts[0] + counts[1];
+      iters = 0;
+      while (iters < K) {
+        launch_iterations(h, 1);
+        ++iters;
+        if (nc == 0) continue;
+        double sum = 0.;
+        CK(cudaMemcpyAsync(&sum, d.ac_hist + 4 * (size_t)(iters - 1), sizeof(double), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (sum / nc <= h->prm.residual_tolerance) break;
+      }
     }
   } else if (h->prm.use_graph) {
     if (!h->graph) {
       cudaGraph_t g;
       CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      launch_iterations(h, 0, K);
+      launch_iterations(h, K);
       CK(cudaStreamEndCapture(st, &g));
       CK(cudaGraphInstantiate(&h->graph, g, 0));
       CK(cudaGraphDestroy(g));
     }
     CK(cudaGraphLaunch(h->graph, st));
+    iters = K;
   } else {
-    launch_iterations(h, 0, K);
+    launch_iterations(h, K);
+    iters = K;
   }
   CK(cudaEventRecord(h->ev[3], st));
+  if (mlp_features) {
+    const bool log = h->log_cap > 0;
+    launch_mlp_record(st, d.c, d.mass, h->rprev, h->rprev_tag, h->mlp_tag, h->prm.gravity, dt, h->mlp_X,
+                      log ? h->log_X : nullptr, h->log_T, h->log_n, h->log_cap);
+  }
+  h->mlp_tag += 1;
   k_contact_slots_reset<<<kStrideBlocks, kThreads, 0, st>>>(d.c);
   CK(cudaMemsetAsync(d.c.n_slots, 0, sizeof(int), st));
   k_finalize<<<blocks_for(3 * (int64_t)N), kThreads, 0, st>>>(3 * N, d.qk, d.q);
@@ -507,9 +644,7 @@ void step_once(pdf_handle* h, bool want_report) {
   for (auto& t : h->host_time_before_start) t -= dt;
   h->time += dt;
   h->stats.steps += 1;
-  h->stats.iterations += iters;
-  h->stats.kernel_launches += launches_per_step_extra(h) + iters * launches_per_iteration(h);
-  h->last_iters = iters;
+  h->launches_outside += launches_per_step_extra(h);
   if (want_report) {
     CK(cudaStreamSynchronize(st));
     float a, b, cc, dd;
@@ -525,6 +660,7 @@ void step_once(pdf_handle* h, bool want_report) {
     CK(cudaMemcpy(&counts[0], d.c.n_contacts, sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(&counts[1], d.c.n_self, sizeof(int), cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(&counts[2], d.c.n_levels, sizeof(int), cudaMemcpyDeviceToHost));
+    if (iters < 0) CK(cudaMemcpy(&iters, d.iter, sizeof(int), cudaMemcpyDeviceToHost));
     std::vector<double> hist(4 * (size_t)K);
     CK(cudaMemcpy(hist.data(), d.ac_hist, hist.size() * sizeof(double), cudaMemcpyDeviceToHost));
     const int nc = counts[0] + counts[1];
@@ -556,6 +692,8 @@ int guarded(pdf_handle* h, F&& fn) {
     return fn();
   } catch (const CudaFail& e) {
     return fail(h, PDF_CUDA_ERROR, e.what());
+  } catch (const std::ios_base::failure& e) {
+    return fail(h, PDF_IO_ERROR, e.what());
   } catch (const std::overflow_error& e) {
     return fail(h, PDF_CAPACITY_EXCEEDED, e.what());
   } catch (const std::range_error& e) {
@@ -589,7 +727,8 @@ void free_handle(pdf_handle* h) {
                   d.c.s_vertex, d.c.s_partner, d.c.s_face, d.c.s_normal, d.c.s_mu, d.c.s_basis, d.c.s_force,
                   d.c.s_ac, d.c.s_slota, d.c.s_slotb, d.c.s_remember, d.c.n_levels, d.c.level_ptr,
                   d.c.level_order, d.c.slot_of, d.c.n_slots, d.c.slot_vertex, d.c.f, d.c.cf[0], d.c.cf[1],
-                  d.c.sf[0], d.c.sf[1]};
+                  d.c.sf[0], d.c.sf[1], d.c.c_gap, d.c.c_active, h->mlp_w, h->mlp_X, h->mlp_Y, h->rprev,
+                  h->rprev_tag, h->log_X, h->log_T, h->log_n, d.iter, d.iter_total, d.blocks_done};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto p : d.obstacle_v) cudaFree(p);
@@ -657,6 +796,8 @@ int pdf_create(const pdf_scene_desc* scene, const pdf_params* params, pdf_handle
 
 int pdf_step(pdf_handle* h, int32_t nsteps, pdf_step_report* report) {
   if (!h || nsteps < 0) return fail(h, PDF_INVALID_ARG, "invalid handle or step count");
+  if (h->prm.warm_start == PDF_WARM_MLP && !h->mlp_ready)
+    return fail(h, PDF_INVALID_ARG, "PDF_WARM_MLP needs weights (mlp_weights, pdf_mlp_set_weights or pdf_mlp_train)");
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->prm.device));
     CK(cudaEventRecord(h->ev[5], h->stream));
@@ -669,6 +810,7 @@ int pdf_step(pdf_handle* h, int32_t nsteps, pdf_step_report* report) {
     if (report) *report = h->last;
     int derr = 0;
     CK(cudaMemcpy(&derr, h->d.sync.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (derr & 2) return fail(h, PDF_CAPACITY_EXCEEDED, "more obstacle contacts than contact_capacity");
     if (derr) return fail(h, PDF_DEVICE_TIMEOUT, "a supernodal sweep gave up waiting for a dependency");
     return PDF_OK;
   });
@@ -735,9 +877,9 @@ int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms_out, d
           launch_local<double>(h, d.b64, 0);
       } else if (phase == 2) {
         if (h->fp32)
-          launch_friction_obstacle<float>(kStrideBlocks, kThreads, st, dm, d.c, d.b32, 0, 0, 1);
+          launch_friction_obstacle<float>(kStrideBlocks, kThreads, st, dm, d.c, d.b32, 0, d.iter);
         else
-          launch_friction_obstacle<double>(kStrideBlocks, kThreads, st, dm, d.c, d.b64, 0, 0, 1);
+          launch_friction_obstacle<double>(kStrideBlocks, kThreads, st, dm, d.c, d.b64, 0, d.iter);
       } else {
         if (h->obs.n > 0) {
           k_obstacle_flags<<<blocks_for(dm.N), kThreads, 0, st>>>(dm.N, d.q, h->obs, d.flags);
@@ -788,6 +930,7 @@ int pdf_set_state(pdf_handle* h, const double* q, const double* v) {
     CK(cudaStreamSynchronize(h->stream));
     if (q) CK(cudaMemcpy(h->d.q, q, n3 * sizeof(double), cudaMemcpyHostToDevice));
     if (v) CK(cudaMemcpy(h->d.v, v, n3 * sizeof(double), cudaMemcpyHostToDevice));
+    h->mlp_tag += 2;  // the previous step's contact impulses no longer apply
     return PDF_OK;
   });
 }
@@ -872,8 +1015,16 @@ int pdf_get_self_levels(pdf_handle* h, int32_t* level_ptr, int32_t level_cap, in
 
 int pdf_get_stats(pdf_handle* h, pdf_stats* out) {
   if (!h || !out) return fail(h, PDF_INVALID_ARG, "null argument");
-  *out = h->stats;
-  return PDF_OK;
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    CK(cudaStreamSynchronize(h->stream));
+    long long total = 0;
+    CK(cudaMemcpy(&total, h->d.iter_total, sizeof(long long), cudaMemcpyDeviceToHost));
+    h->stats.iterations = total;
+    h->stats.kernel_launches = h->launches_outside + total * launches_per_iteration(h);
+    *out = h->stats;
+    return PDF_OK;
+  });
 }
 
 int pdf_export_stats(pdf_handle* h, const char* path) {
@@ -952,6 +1103,196 @@ int pdf_detect_self_collisions(const double* positions, int32_t n_vertices, cons
   }
   if (st != PDF_OK) g_error = err;
   return st;
+}
+
+// ---- learned warm start ----------------------------------------------------
+
+int32_t pdf_mlp_param_count(void) { return kMlpParams; }
+
+int pdf_mlp_init(float* weights, uint64_t seed) {
+  if (!weights) return fail(nullptr, PDF_INVALID_ARG, "null weights");
+  mlp_init_host(weights, seed);
+  return PDF_OK;
+}
+
+int pdf_mlp_save(const char* path, const float* weights) {
+  if (!path || !weights) return fail(nullptr, PDF_INVALID_ARG, "null path or weights");
+  std::ofstream out(path, std::ios::binary);
+  if (!out) return fail(nullptr, PDF_IO_ERROR, std::string("cannot write ") + path);
+  const int32_t hdr[4] = {kMlpIn, kMlpHidden, kMlpOut, kMlpParams};
+  out.write(kMlpMagic, 8);
+  out.write(reinterpret_cast<const char*>(hdr), sizeof(hdr));
+  out.write(reinterpret_cast<const char*>(weights), kMlpParams * sizeof(float));
+  if (!out) return fail(nullptr, PDF_IO_ERROR, std::string("write failed: ") + path);
+  return PDF_OK;
+}
+
+int pdf_mlp_load(const char* path, float* weights) {
+  if (!path || !weights) return fail(nullptr, PDF_INVALID_ARG, "null path or weights");
+  return guarded(nullptr, [&]() -> int {
+    load_weights_file(path, weights);
+    return PDF_OK;
+  });
+}
+
+}  // extern "C"
+
+namespace {
+void select_device(int32_t device) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) throw std::domain_error("no CUDA device");
+  if (device < 0 || device >= ndev) throw std::invalid_argument("device ordinal out of range");
+  CK(cudaSetDevice(device));
+}
+template <typename T>
+struct HostToDevice {  // device copy of a host array, freed on scope exit
+  T* p = nullptr;
+  HostToDevice(const T* src, size_t n) {
+    p = dalloc<T>(n);
+    if (src && n) CK(cudaMemcpy(p, src, n * sizeof(T), cudaMemcpyHostToDevice));
+  }
+  ~HostToDevice() { cudaFree(p); }
+};
+}  // namespace
+
+extern "C" {
+
+int pdf_mlp_forward(const float* weights, const float* X, int32_t n, float* Y, int32_t device) {
+  if (!weights || n < 0 || (n > 0 && (!X || !Y))) return fail(nullptr, PDF_INVALID_ARG, "invalid MLP forward arguments");
+  return guarded(nullptr, [&]() -> int {
+    select_device(device);
+    if (n == 0) return PDF_OK;
+    HostToDevice<float> w(weights, kMlpParams), x(X, (size_t)n * kMlpIn), y(nullptr, (size_t)n * kMlpOut);
+    mlp_forward_device(w.p, x.p, n, y.p, 0);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(Y, y.p, (size_t)n * kMlpOut * sizeof(float), cudaMemcpyDeviceToHost));
+    return PDF_OK;
+  });
+}
+
+int pdf_mlp_gradient(const float* weights, const float* X, const float* T, int32_t n, float* grad, double* loss,
+                     int32_t device) {
+  if (!weights || !X || !T || !grad || n <= 0) return fail(nullptr, PDF_INVALID_ARG, "invalid MLP gradient arguments");
+  return guarded(nullptr, [&]() -> int {
+    select_device(device);
+    HostToDevice<float> w(weights, kMlpParams), x(X, (size_t)n * kMlpIn), t(T, (size_t)n * kMlpOut),
+        g(nullptr, kMlpParams);
+    HostToDevice<double> l(nullptr, 1);
+    CK(cudaMemset(g.p, 0, kMlpParams * sizeof(float)));
+    CK(cudaMemset(l.p, 0, sizeof(double)));
+    mlp_grad_device(w.p, x.p, t.p, nullptr, n, g.p, l.p, 0);
+    CK(cudaGetLastError());
+    CK(cudaMemcpy(grad, g.p, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost));
+    double lv = 0.;
+    CK(cudaMemcpy(&lv, l.p, sizeof(double), cudaMemcpyDeviceToHost));
+    if (loss) *loss = lv;
+    return PDF_OK;
+  });
+}
+
+int pdf_mlp_fit(float* weights, const float* X, const float* T, int32_t n, int32_t epochs, int32_t batch,
+                double learning_rate, uint64_t seed, int32_t device, double* train_loss, double* val_loss) {
+  if (!weights || !X || !T || n < 2 || epochs <= 0 || batch <= 0 || !(learning_rate > 0.))
+    return fail(nullptr, PDF_INVALID_ARG, "invalid MLP training arguments");
+  return guarded(nullptr, [&]() -> int {
+    select_device(device);
+    HostToDevice<float> w(weights, kMlpParams), x(X, (size_t)n * kMlpIn), t(T, (size_t)n * kMlpOut);
+    double vl = 0.;
+    const double tl = mlp_train_device(w.p, x.p, t.p, n, epochs, batch, learning_rate, seed, &vl, 0);
+    CK(cudaMemcpy(weights, w.p, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost));
+    if (train_loss) *train_loss = tl;
+    if (val_loss) *val_loss = vl;
+    return PDF_OK;
+  });
+}
+
+int pdf_mlp_set_weights(pdf_handle* h, const float* weights, int32_t count) {
+  if (!h || !weights || count != kMlpParams) return fail(h, PDF_INVALID_ARG, "invalid MLP weights");
+  for (int i = 0; i < kMlpParams; ++i)
+    if (!std::isfinite(weights[i])) return fail(h, PDF_NAN_DETECTED, "non-finite MLP weight");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(h->mlp_w, weights, kMlpParams * sizeof(float), cudaMemcpyHostToDevice));
+    h->mlp_ready = true;
+    return PDF_OK;
+  });
+}
+
+int pdf_mlp_get_weights(pdf_handle* h, float* weights, int32_t count) {
+  if (!h || !weights || count != kMlpParams) return fail(h, PDF_INVALID_ARG, "invalid MLP weights buffer");
+  if (!h->mlp_ready) return fail(h, PDF_INVALID_ARG, "no MLP weights set");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaMemcpy(weights, h->mlp_w, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost));
+    return PDF_OK;
+  });
+}
+
+int pdf_mlp_log(pdf_handle* h, int32_t capacity) {
+  if (!h || capacity < 0) return fail(h, PDF_INVALID_ARG, "invalid sample log capacity");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    CK(cudaStreamSynchronize(h->stream));
+    if (h->log_cap > 0) {  // a running log is freed and restarted empty
+      cudaFree(h->log_X);
+      cudaFree(h->log_T);
+      cudaFree(h->log_n);
+      h->log_X = h->log_T = nullptr;
+      h->log_n = nullptr;
+      h->log_cap = 0;
+    }
+    if (capacity == 0) return PDF_OK;
+    ensure_mlp_buffers(h);
+    h->log_X = dalloc<float>((size_t)capacity * kMlpIn);
+    h->log_T = dalloc<float>((size_t)capacity * kMlpOut);
+    h->log_n = dalloc<int>(1);
+    CK(cudaMemset(h->log_n, 0, sizeof(int)));
+    h->log_cap = capacity;
+    return PDF_OK;
+  });
+}
+
+int pdf_mlp_samples(pdf_handle* h, float* X, float* T, int32_t cap, int32_t* n) {
+  if (!h || !n || cap < 0) return fail(h, PDF_INVALID_ARG, "invalid sample read-back arguments");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    CK(cudaStreamSynchronize(h->stream));
+    int cnt = 0;
+    if (h->log_cap > 0) CK(cudaMemcpy(&cnt, h->log_n, sizeof(int), cudaMemcpyDeviceToHost));
+    *n = cnt;
+    const size_t m = std::min(cnt, cap);
+    if (X && m) CK(cudaMemcpy(X, h->log_X, m * kMlpIn * sizeof(float), cudaMemcpyDeviceToHost));
+    if (T && m) CK(cudaMemcpy(T, h->log_T, m * kMlpOut * sizeof(float), cudaMemcpyDeviceToHost));
+    if ((X || T) && cnt > cap) return fail(h, PDF_CAPACITY_EXCEEDED, "sample buffer too small");
+    return PDF_OK;
+  });
+}
+
+int pdf_mlp_train(pdf_handle* h, int32_t epochs, int32_t batch, double learning_rate, uint64_t seed,
+                  double* train_loss, double* val_loss) {
+  if (!h || epochs <= 0 || batch <= 0 || !(learning_rate > 0.))
+    return fail(h, PDF_INVALID_ARG, "invalid MLP training arguments");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    CK(cudaStreamSynchronize(h->stream));
+    int cnt = 0;
+    if (h->log_cap > 0) CK(cudaMemcpy(&cnt, h->log_n, sizeof(int), cudaMemcpyDeviceToHost));
+    if (cnt < 2) return fail(h, PDF_INVALID_ARG, "fewer than 2 logged samples (pdf_mlp_log, then step)");
+    if (!h->mlp_ready) {
+      std::vector<float> w(kMlpParams);
+      mlp_init_host(w.data(), seed);
+      CK(cudaMemcpy(h->mlp_w, w.data(), kMlpParams * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    double vl = 0.;
+    const double tl = mlp_train_device(h->mlp_w, h->log_X, h->log_T, cnt, epochs, batch, learning_rate, seed, &vl,
+                                       h->stream);
+    h->mlp_ready = true;
+    if (train_loss) *train_loss = tl;
+    if (val_loss) *val_loss = vl;
+    return PDF_OK;
+  });
 }
 
 }  // extern "C"

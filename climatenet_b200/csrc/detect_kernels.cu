@@ -41,6 +41,16 @@ __global__ void k_obstacle_flags(int N, const double* __restrict__ q, DObstacles
   }
 }
 
+// Obstacle contacts beyond the capacity are dropped: the count is clamped and
+// bit 1 of the handle's error word is set (the step then reports
+// PDF_CAPACITY_EXCEEDED).
+__global__ void k_clamp_contacts(int* n, int cap, int* err) {
+  if (*n > cap) {
+    *n = cap;
+    atomicOr(err, 2);
+  }
+}
+
 // contact basis, computeBasis SFE:91-105
 __device__ void write_basis(double* B, double3 n) {
   double3 t = cross3(n, make_double3(1., 0., 0.));
@@ -67,10 +77,13 @@ __global__ void k_obstacle_materialize(int N, const double* __restrict__ q, DObs
     const DObstacle& ob = obs.o[o];
     const double3 x = ld3(q, i);
     double3 nrm, sp = make_double3(0., 0., 0.);
+    double gap;  // signed distance to the surface (warm-start feature)
     if (ob.type == 0 || ob.type == 1) {
       // Sphere::project Sphere.cpp:104-113
       const double3 ctr = make_double3(ob.c[0], ob.c[1], ob.c[2]);
-      nrm = normalized3(x - ctr);
+      const double3 rel = x - ctr;
+      gap = sqrt(dot3(rel, rel)) - ob.R;
+      nrm = normalized3(rel);
       const double3 cp = ctr + ob.R * nrm;
       if (ob.type == 1 && ob.time_before_start < 0) {
         // RotatingSphere::checkCollision RotatingSphere.cpp:71-93: omega x (p - c)
@@ -78,13 +91,16 @@ __global__ void k_obstacle_materialize(int N, const double* __restrict__ q, DObs
       }
     } else if (ob.type == 2) {
       nrm = make_double3(ob.n[0], ob.n[1], ob.n[2]);
+      gap = dot3(x - make_double3(ob.p[0], ob.p[1], ob.p[2]), nrm);
     } else {
       int tri;
       double3 cp;
       mesh_obstacle_closest(x, ob.mv, ob.mt, ob.n_tri, ob.tol, &tri, &cp);
       const double3 a = ld3(ob.mv, ob.mt[3 * tri]), b = ld3(ob.mv, ob.mt[3 * tri + 1]), cc = ld3(ob.mv, ob.mt[3 * tri + 2]);
       nrm = normalized3(cross3(b - a, cc - a));  // Mesh::getTriangleNormal Mesh.cpp:120-126
+      gap = dot3(x - cp, nrm);
     }
+    c.c_gap[k] = gap;
     c.c_vertex[k] = i;
     st3(c.c_normal, k, nrm);
     st3(c.c_speed, k, sp);

@@ -39,6 +39,8 @@ struct DContacts {
   double* c_force;          // 3 cap persistent local forces
   double* c_ac;             // cap
   int* c_slot;              // cap: slot of the contact vertex
+  double* c_gap;            // cap: signed distance to the obstacle surface
+  int* c_active;            // cap: 1 if the last projection was not a take-off
   int* n_self;              // [1]
   int* s_vertex;            // cap
   int* s_partner;           // cap

@@ -9,6 +9,7 @@
 #include "../../include/pdf.h"
 #include "factor.hpp"
 #include "kernels.hpp"
+#include "mlp.hpp"
 #include "model.hpp"
 
 namespace pdfb {
@@ -47,6 +48,11 @@ struct DeviceBuffers {
   size_t cub_tmp_bytes = 0;
   double* newf = nullptr;
   double* ac_hist = nullptr;  // 4 per iteration
+  // device iteration control (IterCtl): iterations of the current step, of
+  // the handle's lifetime, and the AC kernel's block-completion counter
+  int* iter = nullptr;
+  long long* iter_total = nullptr;
+  unsigned int* blocks_done = nullptr;
   // self-collision detection scratch (selfdetect.cu)
   void* self_ws = nullptr;
 };
@@ -72,9 +78,24 @@ struct pdf_handle {
   pdf_step_report last{};
   pdf_stats stats{};
   std::vector<double> residual_hist;
-  int last_iters = 0;
+  int64_t launches_outside = 0;  // kernels launched outside PD iterations so far
+  // iterate-to-tolerance graph: the iterations are one conditional WHILE node
+  cudaGraphConditionalHandle cond{};
+  bool capturing_cond = false;
   std::vector<double> host_time_before_start;
   bool fp32 = false;
+  // learned warm start (mlp.cu): device weights, per-contact features and
+  // predictions, the per-vertex impulse memory of the previous step (valid
+  // where rprev_tag == mlp_tag - 1) and the optional sample log
+  float* mlp_w = nullptr;
+  bool mlp_ready = false;
+  float *mlp_X = nullptr, *mlp_Y = nullptr;
+  double* rprev = nullptr;
+  int* rprev_tag = nullptr;
+  int mlp_tag = 0;
+  float *log_X = nullptr, *log_T = nullptr;
+  int* log_n = nullptr;
+  int log_cap = 0;
 };
 
 namespace pdfb {

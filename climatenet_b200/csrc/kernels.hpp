@@ -38,7 +38,22 @@ struct DObstacles {
 __global__ void k_step_init(DModel m, const double* q, double* v, double* tn, double* qk, double* cstep, double gx,
                             double gy, double gz, double dt);
 __global__ void k_bend_proj(DModel m, const double* qk, double* bp);
-__global__ void k_alart_curnier(DContacts c, const double* v, double* acc);
+// Iteration control of one step, on the device.  iter = PD iterations
+// completed in this step (kernels of iteration k read k from it); the last
+// block of the Alart-Curnier kernel closes the iteration: it advances iter and
+// iter_total and, inside a conditional WHILE graph body, sets the loop
+// condition (continue while iter < kmax and not (tol > 0, contacts > 0 and
+// mean |AC| <= tol)).
+struct IterCtl {
+  int* iter;
+  long long* iter_total;
+  unsigned int* blocks_done;
+  double tol;
+  int kmax;
+  int set_cond;
+  cudaGraphConditionalHandle cond;
+};
+__global__ void k_alart_curnier(DContacts c, const double* v, double* hist, IterCtl ctl);
 __global__ void k_finalize(int n3, const double* qk, double* q);
 
 // Templated kernels are launched through host wrappers defined (and
@@ -48,12 +63,15 @@ template <typename T>
 void launch_vertex_rhs(dim3 grid, dim3 block, cudaStream_t st, DModel m, const double* qk, const double* v,
                        const double* cstep, const double* bp, double air_damping, const int* slot_of, double* fslot,
                        T* b, double dt, int residual_mode);
+// The contact kernels take the iteration index from *iter: the parity selects
+// the current / next self-contact force buffers, and iteration 0 uses the
+// learned prediction when pred is given.
 template <typename T>
 void launch_friction_obstacle(dim3 grid, dim3 block, cudaStream_t st, DModel m, DContacts c, T* b, int self_mode,
-                              int cur, int nxt);
+                              const int* iter, const float* pred = nullptr, double pred_sv = 0.);
 template <typename T>
-void launch_friction_self(dim3 grid, dim3 block, cudaStream_t st, DModel m, DContacts c, T* b, double* newf, int cur,
-                          int nxt);
+void launch_friction_self(dim3 grid, dim3 block, cudaStream_t st, DModel m, DContacts c, T* b, double* newf,
+                          const int* iter);
 // Solve vectors b, y, x are three planes of n values (x, y, z components) in
 // pivot order.  y and x must be zero before a solve (k_solve_post / prep).
 template <typename T>
@@ -70,6 +88,7 @@ void launch_solve_prep(cudaStream_t st, int n, T* x, T* y, SweepSync sy);
 __global__ void k_obstacle_flags(int N, const double* q, DObstacles obs, unsigned char* flags);
 __global__ void k_obstacle_materialize(int N, const double* q, DObstacles obs, const int* idx, const int* vmat,
                                        const double* friction, int n_mat, DContacts c);
+__global__ void k_clamp_contacts(int* n, int cap, int* err);
 __global__ void k_contact_slots(DContacts c);
 __global__ void k_contact_slots_fill(DContacts c);
 __global__ void k_contact_slots_reset(DContacts c);

@@ -169,21 +169,56 @@ __device__ __forceinline__ double3 cone_project(double3 fl, double mu) {
 }
 
 // Obstacle contacts (SFE:350-423).  One thread per contact.
+// pred (learned warm start, first iteration of a step only): the predicted
+// local force y_k, in units of s_r = m |g| dt (pred_sv = |g| dt), replaces the
+// projection; it is projected on the friction cone, and a non-finite
+// prediction falls back to the projection for that contact.
 template <typename T>
-__global__ void k_friction_obstacle(DModel m, DContacts c, T* __restrict__ b, int self_mode, int cur, int nxt) {
+__global__ void k_friction_obstacle(DModel m, DContacts c, T* __restrict__ b, int self_mode, const int* __restrict__ iter,
+                                    const float* __restrict__ pred, double pred_sv) {
   const int C = *c.n_contacts;
   const int S = self_mode ? *c.n_self : 0;
+  const int it = *iter;
+  const int cur = it & 1, nxt = 1 - cur;
+  if (it != 0) pred = nullptr;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C; k += gridDim.x * blockDim.x) {
     const int vid = c.c_vertex[k];
     const int slot = c.c_slot[k];
     const double* B = c.c_basis + 9 * (int64_t)k;
-    double3 f = ld3(c.f, slot);
-    if (self_mode) f = f + ld3(c.sf[cur], slot);
     const double mv = m.mass[vid];
-    const double3 sp = ld3(c.c_speed, k);
-    const double3 fl = basis_t(B, make_double3(f.x - mv * sp.x, f.y - mv * sp.y, f.z - mv * sp.z));
-    if (fl.x > 0.) continue;  // take-off: the stored local force keeps its old value
-    const double3 r = cone_project(fl, c.c_mu[k]);
+    double3 r;
+    bool predicted = false;
+    if (pred) {
+      const double sr = mv * pred_sv;
+      r = make_double3(sr * (double)pred[3 * (int64_t)k], sr * (double)pred[3 * (int64_t)k + 1],
+                       sr * (double)pred[3 * (int64_t)k + 2]);
+      if (isfinite(r.x) && isfinite(r.y) && isfinite(r.z)) {
+        predicted = true;
+        if (!(r.x > 0.)) {  // predicted separation
+          st3(c.c_force, k, make_double3(0., 0., 0.));
+          c.c_active[k] = 0;
+          continue;
+        }
+        const double mu = c.c_mu[k];
+        const double rtn = sqrt(r.y * r.y + r.z * r.z);
+        if (rtn > mu * r.x) {
+          r.y *= mu * r.x / rtn;
+          r.z *= mu * r.x / rtn;
+        }
+      }
+    }
+    if (!predicted) {
+      double3 f = ld3(c.f, slot);
+      if (self_mode) f = f + ld3(c.sf[cur], slot);
+      const double3 sp = ld3(c.c_speed, k);
+      const double3 fl = basis_t(B, make_double3(f.x - mv * sp.x, f.y - mv * sp.y, f.z - mv * sp.z));
+      if (fl.x > 0.) {  // take-off: the stored local force keeps its old value
+        c.c_active[k] = 0;
+        continue;
+      }
+      r = cone_project(fl, c.c_mu[k]);
+    }
+    c.c_active[k] = 1;
     st3(c.c_force, k, r);
     const double3 g = basis_v(B, r);
     if (!self_mode || S == 0) atomic_add3(b, m.iperm[vid], m.N, g);
@@ -192,11 +227,13 @@ __global__ void k_friction_obstacle(DModel m, DContacts c, T* __restrict__ b, in
 }
 template <typename T>
 void launch_friction_obstacle(dim3 grid, dim3 block, cudaStream_t st, DModel m, DContacts c, T* b, int self_mode,
-                              int cur, int nxt) {
-  k_friction_obstacle<T><<<grid, block, 0, st>>>(m, c, b, self_mode, cur, nxt);
+                              const int* iter, const float* pred, double pred_sv) {
+  k_friction_obstacle<T><<<grid, block, 0, st>>>(m, c, b, self_mode, iter, pred, pred_sv);
 }
-template void launch_friction_obstacle<double>(dim3, dim3, cudaStream_t, DModel, DContacts, double*, int, int, int);
-template void launch_friction_obstacle<float>(dim3, dim3, cudaStream_t, DModel, DContacts, float*, int, int, int);
+template void launch_friction_obstacle<double>(dim3, dim3, cudaStream_t, DModel, DContacts, double*, int, const int*,
+                                               const float*, double);
+template void launch_friction_obstacle<float>(dim3, dim3, cudaStream_t, DModel, DContacts, float*, int, const int*,
+                                              const float*, double);
 
 // Self contacts (SFE:431-587).  One CTA walks the breadth-first levels in
 // order; inside a level every contact is estimated from the buffers as they
@@ -205,8 +242,9 @@ template void launch_friction_obstacle<float>(dim3, dim3, cudaStream_t, DModel, 
 // self-contact forces are added to the right-hand side and the buffer that
 // becomes "next" is cleared.
 template <typename T>
-__global__ void k_friction_self(DModel m, DContacts c, T* __restrict__ b, double* __restrict__ newf, int cur,
-                                int nxt) {
+__global__ void k_friction_self(DModel m, DContacts c, T* __restrict__ b, double* __restrict__ newf,
+                                const int* __restrict__ iter) {
+  const int cur = (*iter) & 1, nxt = 1 - cur;
   const int S = *c.n_self;
   const int C = *c.n_contacts;
   const int nl = *c.n_levels;
@@ -275,12 +313,12 @@ __global__ void k_friction_self(DModel m, DContacts c, T* __restrict__ b, double
   }
 }
 template <typename T>
-void launch_friction_self(dim3 grid, dim3 block, cudaStream_t st, DModel m, DContacts c, T* b, double* newf, int cur,
-                          int nxt) {
-  k_friction_self<T><<<grid, block, 0, st>>>(m, c, b, newf, cur, nxt);
+void launch_friction_self(dim3 grid, dim3 block, cudaStream_t st, DModel m, DContacts c, T* b, double* newf,
+                          const int* iter) {
+  k_friction_self<T><<<grid, block, 0, st>>>(m, c, b, newf, iter);
 }
-template void launch_friction_self<double>(dim3, dim3, cudaStream_t, DModel, DContacts, double*, double*, int, int);
-template void launch_friction_self<float>(dim3, dim3, cudaStream_t, DModel, DContacts, float*, double*, int, int);
+template void launch_friction_self<double>(dim3, dim3, cudaStream_t, DModel, DContacts, double*, double*, const int*);
+template void launch_friction_self<float>(dim3, dim3, cudaStream_t, DModel, DContacts, float*, double*, const int*);
 
 // Alart-Curnier residual with rho = 1 (coulomb_util.cpp:92-152) for every
 // contact after the solve (SFE:590-652).  acc[4] += {sum |AC|, max |AC|,
@@ -305,8 +343,10 @@ __device__ __forceinline__ void atomic_max_pos(double* addr, double val) {
   atomicMax(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)__double_as_longlong(val));
 }
 
-__global__ void k_alart_curnier(DContacts c, const double* __restrict__ v, double* __restrict__ acc) {
+__global__ void k_alart_curnier(DContacts c, const double* __restrict__ v, double* __restrict__ hist, IterCtl ctl) {
   const int C = *c.n_contacts, S = *c.n_self;
+  const int it = *ctl.iter;
+  double* acc = hist + 4 * (int64_t)it;
   double s = 0, mx = 0, sn = 0, st = 0;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C + S; k += gridDim.x * blockDim.x) {
     double an, at, n;
@@ -354,6 +394,23 @@ __global__ void k_alart_curnier(DContacts c, const double* __restrict__ v, doubl
     atomic_max_pos(acc + 1, mx);
     atomicAdd(acc + 2, sn);
     atomicAdd(acc + 3, st);
+  }
+  // the last block to finish closes the iteration
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned int prev = atomicAdd(ctl.blocks_done, 1u);
+    if (prev == gridDim.x - 1) {
+      *ctl.blocks_done = 0u;
+      const int k1 = it + 1;
+      *ctl.iter = k1;
+      *ctl.iter_total += 1;
+      if (ctl.set_cond) {
+        const int nc = C + S;
+        const double mean = nc > 0 ? __ldcg(acc) / nc : 0.;
+        const bool stop = k1 >= ctl.kmax || (ctl.tol > 0. && nc > 0 && mean <= ctl.tol);
+        cudaGraphSetConditional(ctl.cond, stop ? 0u : 1u);
+      }
+    }
   }
 }
 

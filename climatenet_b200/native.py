@@ -59,6 +59,20 @@ def lib():
     L.pdf_destroy.argtypes = [vp]
     L.pdf_detect_candidates.argtypes = [vp, i32, vp, i32, C.c_double, vp, i32, C.POINTER(i32), i32]
     L.pdf_detect_self_collisions.argtypes = [vp, i32, vp, i32, C.c_double, vp, i32, C.POINTER(i32), i32]
+    L.pdf_mlp_param_count.restype = i32
+    L.pdf_mlp_init.argtypes = [vp, C.c_uint64]
+    L.pdf_mlp_save.argtypes = [C.c_char_p, vp]
+    L.pdf_mlp_load.argtypes = [C.c_char_p, vp]
+    L.pdf_mlp_forward.argtypes = [vp, vp, i32, vp, i32]
+    L.pdf_mlp_gradient.argtypes = [vp, vp, vp, i32, vp, C.POINTER(C.c_double), i32]
+    L.pdf_mlp_fit.argtypes = [vp, vp, vp, i32, i32, i32, C.c_double, C.c_uint64, i32, C.POINTER(C.c_double),
+                              C.POINTER(C.c_double)]
+    L.pdf_mlp_set_weights.argtypes = [vp, vp, i32]
+    L.pdf_mlp_get_weights.argtypes = [vp, vp, i32]
+    L.pdf_mlp_log.argtypes = [vp, i32]
+    L.pdf_mlp_samples.argtypes = [vp, vp, vp, i32, C.POINTER(i32)]
+    L.pdf_mlp_train.argtypes = [vp, i32, i32, C.c_double, C.c_uint64, C.POINTER(C.c_double),
+                                C.POINTER(C.c_double)]
     _lib = L
     return L
 
@@ -197,6 +211,83 @@ class Simulation:
         out = np.zeros(max(1, n.value))
         lib().pdf_get_residual_history(self.h, _ptr(out), n.value, C.byref(n))
         return out[:n.value]
+
+
+    # ---- learned warm start ------------------------------------------------
+    def mlp_set_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        _check(lib().pdf_mlp_set_weights(self.h, _ptr(w), w.size), self.h)
+
+    def mlp_get_weights(self):
+        w = np.zeros(abi.MLP_PARAMS, dtype=np.float32)
+        _check(lib().pdf_mlp_get_weights(self.h, _ptr(w), w.size), self.h)
+        return w
+
+    def mlp_log(self, capacity):
+        """Start (or restart, empty) the per-contact sample log; 0 stops it."""
+        _check(lib().pdf_mlp_log(self.h, capacity), self.h)
+
+    def mlp_samples(self):
+        n = C.c_int32()
+        _check(lib().pdf_mlp_samples(self.h, None, None, 0, C.byref(n)), self.h)
+        X = np.zeros((max(1, n.value), abi.MLP_IN), dtype=np.float32)
+        T = np.zeros((max(1, n.value), abi.MLP_OUT), dtype=np.float32)
+        _check(lib().pdf_mlp_samples(self.h, _ptr(X), _ptr(T), n.value, C.byref(n)), self.h)
+        return X[:n.value], T[:n.value]
+
+    def mlp_train(self, epochs=20, batch=4096, lr=1e-3, seed=0):
+        """Train the handle's weights on its logged samples on the GPU; (train, held-out) loss."""
+        tl, vl = C.c_double(), C.c_double()
+        _check(lib().pdf_mlp_train(self.h, epochs, batch, lr, seed, C.byref(tl), C.byref(vl)), self.h)
+        return tl.value, vl.value
+
+
+def mlp_init(seed=0):
+    w = np.zeros(abi.MLP_PARAMS, dtype=np.float32)
+    _check(lib().pdf_mlp_init(_ptr(w), seed))
+    return w
+
+
+def mlp_save(path, w):
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    _check(lib().pdf_mlp_save(str(path).encode(), _ptr(w)))
+
+
+def mlp_load(path):
+    w = np.zeros(abi.MLP_PARAMS, dtype=np.float32)
+    _check(lib().pdf_mlp_load(str(path).encode(), _ptr(w)))
+    return w
+
+
+def mlp_forward(w, X, device=0):
+    """BF16 tensor-core forward of the warm-start MLP on the GPU."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    Y = np.zeros((X.shape[0], abi.MLP_OUT), dtype=np.float32)
+    _check(lib().pdf_mlp_forward(_ptr(w), _ptr(X), X.shape[0], _ptr(Y), device))
+    return Y
+
+
+def mlp_gradient(w, X, T, device=0):
+    """(loss, gradient) of the mean squared error, GPU backward kernels."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    g = np.zeros(abi.MLP_PARAMS, dtype=np.float32)
+    loss = C.c_double()
+    _check(lib().pdf_mlp_gradient(_ptr(w), _ptr(X), _ptr(T), X.shape[0], _ptr(g), C.byref(loss), device))
+    return loss.value, g
+
+
+def mlp_fit(w, X, T, epochs=20, batch=4096, lr=1e-3, seed=0, device=0):
+    """Adam training on the GPU; returns (weights, train loss, held-out loss)."""
+    w = np.array(w, dtype=np.float32, copy=True)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    T = np.ascontiguousarray(T, dtype=np.float32)
+    tl, vl = C.c_double(), C.c_double()
+    _check(lib().pdf_mlp_fit(_ptr(w), _ptr(X), _ptr(T), X.shape[0], epochs, batch, lr, seed, device,
+                             C.byref(tl), C.byref(vl)))
+    return w, tl.value, vl.value
 
 
 def getSceneFromJSONFileName(path):

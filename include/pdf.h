@@ -125,6 +125,9 @@ typedef struct pdf_params {
   int32_t device;                   /* CUDA device ordinal                       */
   int32_t contact_capacity;         /* 0 = automatic                             */
   int32_t use_graph;                /* capture the iteration loop in a CUDA graph */
+  char mlp_weights[256];            /* PDF_WARM_MLP: weights file loaded at create
+                                       ("" = set later with pdf_mlp_set_weights
+                                       or pdf_mlp_train)                        */
 } pdf_params;
 
 /* Fills p with the reference defaults (air damping 0, FP64, fixed iterations). */
@@ -308,6 +311,50 @@ int pdf_detect_candidates_noalloc(const double* positions, int32_t n_vertices,
                                   const int32_t* triangles, int32_t n_triangles,
                                   double tolerance, int32_t* pairs, int32_t cap,
                                   int32_t* n, void* cuda_stream);
+
+/* ---- learned warm start (no counterpart in the reference) --------------- */
+/* A per-contact MLP 10 -> 64 -> 64 -> 3 (ReLU) predicts the converged local
+ * force of every obstacle contact from the predictor velocity relative to the
+ * obstacle, the gap, the vertex's contact impulse of the previous step and
+ * mu; under PDF_WARM_MLP the first PD iteration of a step uses the prediction
+ * (projected on the friction cone) instead of the cone projection.  BF16
+ * tensor-core forward and backward kernels, FP32 master weights, Adam.
+ * Weights: pdf_mlp_param_count() floats, W1[64][10] b1 W2[64][64] b2 W3[3][64] b3. */
+int32_t pdf_mlp_param_count(void);
+/* Seeded He initialisation (host only). */
+int pdf_mlp_init(float* weights, uint64_t seed);
+/* Weights file: "PDFMLP01", int32 {10, 64, 3, count}, count little-endian floats. */
+int pdf_mlp_save(const char* path, const float* weights);
+int pdf_mlp_load(const char* path, float* weights);
+/* Stand-alone kernels on host buffers (device = CUDA ordinal):
+ * Y[n][3] = MLP(X[n][10]); grad = d(mean_s |MLP(x_s) - t_s|^2)/d(weights)
+ * and *loss = that mean; fit = seeded shuffle, 90/10 split, Adam over
+ * mini-batches, weights updated in place, losses of the last epoch and of the
+ * held-out part. */
+int pdf_mlp_forward(const float* weights, const float* X, int32_t n, float* Y,
+                    int32_t device);
+int pdf_mlp_gradient(const float* weights, const float* X, const float* T,
+                     int32_t n, float* grad, double* loss, int32_t device);
+int pdf_mlp_fit(float* weights, const float* X, const float* T, int32_t n,
+                int32_t epochs, int32_t batch, double learning_rate,
+                uint64_t seed, int32_t device, double* train_loss,
+                double* val_loss);
+/* Per-handle: weights used by PDF_WARM_MLP steps. */
+int pdf_mlp_set_weights(pdf_handle* h, const float* weights, int32_t count);
+int pdf_mlp_get_weights(pdf_handle* h, float* weights, int32_t count);
+/* Sample log on the device: after every step, one (features, converged local
+ * force / (m |g| dt)) sample per obstacle contact (0 for a contact that took
+ * off in the last iteration), up to capacity samples.  capacity 0 stops
+ * logging and frees the log; a new call restarts it empty. */
+int pdf_mlp_log(pdf_handle* h, int32_t capacity);
+/* Copies the logged samples out (X: n*10, T: n*3 floats; either NULL to query *n). */
+int pdf_mlp_samples(pdf_handle* h, float* X, float* T, int32_t cap, int32_t* n);
+/* Trains the handle's weights on its logged samples without leaving the
+ * device (starting from the current weights, or a seeded He initialisation
+ * when none were set). */
+int pdf_mlp_train(pdf_handle* h, int32_t epochs, int32_t batch,
+                  double learning_rate, uint64_t seed, double* train_loss,
+                  double* val_loss);
 
 #ifdef __cplusplus
 }

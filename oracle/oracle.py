@@ -53,6 +53,10 @@ def lib():
         L.orc_self_collisions.argtypes = [C.c_void_p, C.c_int32, C.c_void_p, C.c_int32, C.c_double,
                                           C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]
         L.orc_closest_point.argtypes = [C.c_void_p] * 4 + [C.c_double, C.c_void_p, C.c_void_p]
+        L.orc_mlp_set_weights.argtypes = [vp, C.c_void_p, C.c_int32]
+        L.orc_mlp_log.argtypes = [vp, C.c_int32]
+        L.orc_mlp_samples.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]
+        L.orc_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p]
         _lib = L
     return _lib
 
@@ -127,6 +131,23 @@ class Oracle:
         order = np.zeros(max(1, ns), dtype=np.int32)
         lib().orc_get_self_levels(self.h, _ptr(ptr), nl.value + 1, _ptr(order), ns, C.byref(nl))
         return ptr, order[:ns]
+
+    def mlp_set_weights(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        st = lib().orc_mlp_set_weights(self.h, _ptr(w), w.size)
+        if st != 0:
+            raise OracleError(st, "weights")
+
+    def mlp_log(self, capacity):
+        lib().orc_mlp_log(self.h, capacity)
+
+    def mlp_samples(self):
+        n = C.c_int32()
+        lib().orc_mlp_samples(self.h, None, None, 0, C.byref(n))
+        X = np.zeros((max(1, n.value), abi.MLP_IN), dtype=np.float32)
+        T = np.zeros((max(1, n.value), abi.MLP_OUT), dtype=np.float32)
+        lib().orc_mlp_samples(self.h, _ptr(X), _ptr(T), n.value, C.byref(n))
+        return X[:n.value], T[:n.value]
 
     def residual_history(self):
         n = C.c_int32()
@@ -211,3 +232,12 @@ def closest_point(p, a, b, c, tol2):
     bary = np.zeros(3)
     lib().orc_closest_point(*[_ptr(x) for x in arrs], tol2, _ptr(cp), _ptr(bary))
     return cp, bary
+
+
+def mlp_forward_bf16(w, X):
+    """The warm-start MLP with the tensor cores' bfloat16 rounding emulated."""
+    w = np.ascontiguousarray(w, dtype=np.float32)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    Y = np.zeros((X.shape[0], abi.MLP_OUT), dtype=np.float32)
+    lib().orc_mlp_forward(_ptr(w), _ptr(X), X.shape[0], _ptr(Y))
+    return Y

@@ -590,6 +590,7 @@ struct CInfo {
   int vertex;
   V3 cp, normal, speed;
   double mu;
+  double gap; /* signed distance to the obstacle surface (warm-start feature) */
 };
 
 /* -------------------------------------------------------------- sim */
@@ -647,6 +648,17 @@ struct Sim {
   std::vector<double> residual_hist;
   pdf_step_report last{};
   std::vector<double> tmpx;
+
+  /* learned warm start (restates climatenet_b200/csrc/mlp.cu for checking) */
+  std::vector<float> mlp_w;
+  bool mlp_ready = false;
+  std::vector<char> c_active;   /* last projection of the contact was not a take-off */
+  std::vector<double> rprev;    /* world impulse per vertex, end of the tagged step */
+  std::vector<int> rprev_tag;
+  int mlp_tag = 0;
+  std::vector<float> feat, pred; /* C x 10, C x 3 */
+  std::vector<float> log_X, log_T;
+  int log_cap = 0, log_n = 0;
 
   int partner(const SelfInfo& s) const {
     const V3& a = s.bary;
@@ -803,6 +815,7 @@ static void detect_obstacles(Sim& s) {
         V3 rn = normalized(verts[i] - ob.center);
         CInfo c;
         c.vertex = i;
+        c.gap = nrm(r) - ob.radius;
         c.cp = ob.center + ob.radius * rn;
         c.normal = rn;
         c.speed = {0, 0, 0};
@@ -819,6 +832,7 @@ static void detect_obstacles(Sim& s) {
         if (!(d < 1.5e-2)) continue;
         CInfo c;
         c.vertex = i;
+        c.gap = d;
         c.cp = verts[i] - ob.normal * d;
         c.normal = ob.normal;
         c.speed = {0, 0, 0};
@@ -851,6 +865,7 @@ static void detect_obstacles(Sim& s) {
           c.vertex = i;
           c.cp = bp;
           c.normal = normalized(cross(ob.mverts[t[1]] - ob.mverts[t[0]], ob.mverts[t[2]] - ob.mverts[t[0]]));
+          c.gap = dot(verts[i] - bp, c.normal);
           c.speed = {0, 0, 0};
           found.push_back(c);
         }
@@ -863,6 +878,118 @@ static void detect_obstacles(Sim& s) {
       s.contacts.push_back(c);
     }
   }
+}
+
+/* ------------------------------------------------- learned warm start
+ * No counterpart in the reference: restates the product's warm start
+ * (climatenet_b200/csrc/mlp.cu) so that its steps can be checked.  The MLP
+ * forward emulates the tensor-core arithmetic: inputs, weights and hidden
+ * activations rounded to bfloat16 (round to nearest even), products summed per
+ * 16-wide k block in double and accumulated in float, biases added in float. */
+static const int kMIn = 10, kMH = 64, kMOut = 3;
+static const int kMParams = kMH * kMIn + kMH + kMH * kMH + kMH + kMOut * kMH + kMOut;
+
+static float to_bf16(float f) {
+  uint32_t u;
+  std::memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return f;
+  u += 0x7fffu + ((u >> 16) & 1u);
+  u &= 0xffff0000u;
+  std::memcpy(&f, &u, 4);
+  return f;
+}
+
+static void mlp_layer(const float* W, const float* b, int nout, int nin, const float* in, float* out, bool relu) {
+  for (int o = 0; o < nout; ++o) {
+    float acc = 0.f;
+    for (int k0 = 0; k0 < nin; k0 += 16) {
+      double blk = 0.;
+      for (int k = k0; k < std::min(nin, k0 + 16); ++k)
+        blk += (double)to_bf16(in[k]) * (double)to_bf16(W[(size_t)o * nin + k]);
+      acc = (float)((double)acc + blk);
+    }
+    const float z = acc + b[o];
+    out[o] = relu ? (z > 0.f ? z : 0.f) : z;
+  }
+}
+
+static void mlp_forward_one(const float* w, const float* x, float* y) {
+  const float* W1 = w;
+  const float* b1 = W1 + kMH * kMIn;
+  const float* W2 = b1 + kMH;
+  const float* b2 = W2 + kMH * kMH;
+  const float* W3 = b2 + kMH;
+  const float* b3 = W3 + kMOut * kMH;
+  float h1[kMH], h2[kMH];
+  mlp_layer(W1, b1, kMH, kMIn, x, h1, true);
+  mlp_layer(W2, b2, kMH, kMH, h1, h2, true);
+  mlp_layer(W3, b3, kMOut, kMH, h2, y, false);
+}
+
+static double gravity_norm(const Sim& s) {
+  const double* g = s.prm.gravity;
+  const double gn = std::sqrt((g[0] * g[0] + g[1] * g[1]) + g[2] * g[2]);
+  return gn > 1e-12 ? gn : 1e-12;
+}
+
+/* Features of every obstacle contact (definitions in mlp.cu's header). */
+static void mlp_features(Sim& s) {
+  const int C = (int)s.contacts.size();
+  const double g = gravity_norm(s);
+  const double sv = g * s.prm.time_step;
+  const V3 gv{s.prm.gravity[0], s.prm.gravity[1], s.prm.gravity[2]};
+  s.feat.assign((size_t)C * kMIn, 0.f);
+  for (int k = 0; k < C; ++k) {
+    const CInfo& ci = s.contacts[k];
+    const Basis& B = s.cbasis[k];
+    const int v = ci.vertex;
+    const V3 d = ld(s.tn.data(), v) - ci.speed;
+    float* x = &s.feat[(size_t)k * kMIn];
+    x[0] = (float)(dot(B.c0, d) / sv);
+    x[1] = (float)(dot(B.c1, d) / sv);
+    x[2] = (float)(dot(B.c2, d) / sv);
+    x[3] = (float)(ci.gap / 1e-2);
+    const double sr = s.mass[v] * sv;
+    if (s.rprev_tag[v] == s.mlp_tag - 1) {
+      const V3 R = ld(s.rprev.data(), v);
+      x[4] = (float)(dot(B.c0, R) / sr);
+      x[5] = (float)(dot(B.c1, R) / sr);
+      x[6] = (float)(dot(B.c2, R) / sr);
+    }
+    x[7] = (float)ci.mu;
+    x[8] = (float)(dot(B.c0, gv) / g);
+    x[9] = 1.f;
+  }
+}
+
+/* End of step: impulse memory and optional sample log (contact order). */
+static void mlp_record(Sim& s) {
+  const int C = (int)s.contacts.size();
+  const double sv = gravity_norm(s) * s.prm.time_step;
+  for (int k = 0; k < C; ++k) {
+    const int v = s.contacts[k].vertex;
+    st(s.rprev.data(), v, {0, 0, 0});
+    s.rprev_tag[v] = s.mlp_tag;
+  }
+  const int base = s.log_n;
+  for (int k = 0; k < C; ++k) {
+    const int v = s.contacts[k].vertex;
+    const bool active = s.c_active[k] != 0;
+    const V3 r = active ? s.c_local_forces[k] : V3{0, 0, 0};
+    if (active) {
+      const V3 g = bv(s.cbasis[k], r);
+      for (int c = 0; c < 3; ++c) s.rprev[3 * (size_t)v + c] += comp(g, c);
+    }
+    if (s.log_cap > 0 && (int64_t)base + k < s.log_cap) {
+      const size_t o = (size_t)base + k;
+      for (int d = 0; d < kMIn; ++d) s.log_X[o * kMIn + d] = s.feat[(size_t)k * kMIn + d];
+      const double sr = s.mass[v] * sv;
+      s.log_T[o * kMOut] = (float)(r.x / sr);
+      s.log_T[o * kMOut + 1] = (float)(r.y / sr);
+      s.log_T[o * kMOut + 2] = (float)(r.z / sr);
+    }
+  }
+  if (s.log_cap > 0) s.log_n = (int)std::min<int64_t>((int64_t)s.log_n + C, s.log_cap);
 }
 
 /* One SimulationBase::step(), SimulationBase.cpp:103-173, with the
@@ -927,6 +1054,18 @@ static void step(Sim& s) {
   if (self && !s.selfc.empty()) compute_order(s);
 
   const int C = (int)s.contacts.size(), S = (int)s.selfc.size();
+  const bool warm = s.prm.warm_start == PDF_WARM_MLP;
+  const bool mlp_on = warm || s.log_cap > 0;
+  if (warm && !s.mlp_ready) throw std::invalid_argument("PDF_WARM_MLP needs weights");
+  if (mlp_on) {
+    mlp_features(s);
+    if (warm) {
+      s.pred.assign((size_t)C * kMOut, 0.f);
+      for (int k = 0; k < C; ++k) mlp_forward_one(s.mlp_w.data(), &s.feat[(size_t)k * kMIn], &s.pred[(size_t)k * kMOut]);
+    }
+  }
+  if ((int)s.c_active.size() < C) s.c_active.resize(C, 0);
+  const double pred_sv = gravity_norm(s) * dt;
   s.residual_hist.clear();
   int it = 0;
   double res_mean = 0, res_max = 0, res_n = 0, res_t = 0;
@@ -949,16 +1088,44 @@ static void step(Sim& s) {
         const int vid = ci.vertex;
         const Basis& B = s.cbasis[c];
         const double mu = ci.mu;
-        V3 f = ld(s.forces.data(), vid);
-        if (self) f = f + ld(s.self_forces[s.cur].data(), vid);
-        V3 fl = btv(B, f - s.mass[vid] * ci.speed);
-        if (fl.x > 0.) continue;
-        V3 r{-fl.x, -fl.y, -fl.z};
-        const double rtn = std::sqrt(r.y * r.y + r.z * r.z);
-        if (rtn > mu * r.x) {
-          r.y *= mu * r.x / rtn;
-          r.z *= mu * r.x / rtn;
+        V3 r;
+        bool predicted = false;
+        if (warm && it == 0) {
+          /* first iteration under the learned warm start: the predicted force,
+           * projected on the cone; non-finite -> the projection below */
+          const double sr = s.mass[vid] * pred_sv;
+          r = {sr * (double)s.pred[3 * (size_t)c], sr * (double)s.pred[3 * (size_t)c + 1],
+               sr * (double)s.pred[3 * (size_t)c + 2]};
+          if (std::isfinite(r.x) && std::isfinite(r.y) && std::isfinite(r.z)) {
+            predicted = true;
+            if (!(r.x > 0.)) {
+              s.c_local_forces[c] = {0, 0, 0};
+              s.c_active[c] = 0;
+              continue;
+            }
+            const double rtn = std::sqrt(r.y * r.y + r.z * r.z);
+            if (rtn > mu * r.x) {
+              r.y *= mu * r.x / rtn;
+              r.z *= mu * r.x / rtn;
+            }
+          }
         }
+        if (!predicted) {
+          V3 f = ld(s.forces.data(), vid);
+          if (self) f = f + ld(s.self_forces[s.cur].data(), vid);
+          V3 fl = btv(B, f - s.mass[vid] * ci.speed);
+          if (fl.x > 0.) {
+            s.c_active[c] = 0;
+            continue;
+          }
+          r = {-fl.x, -fl.y, -fl.z};
+          const double rtn = std::sqrt(r.y * r.y + r.z * r.z);
+          if (rtn > mu * r.x) {
+            r.y *= mu * r.x / rtn;
+            r.z *= mu * r.x / rtn;
+          }
+        }
+        s.c_active[c] = 1;
         s.c_local_forces[c] = r;
         V3 g = bv(B, r);
         if (!self || S == 0) {
@@ -1081,6 +1248,8 @@ static void step(Sim& s) {
       break;
     }
   }
+  if (mlp_on) mlp_record(s);
+  s.mlp_tag += 1;
   /* SFE::updateScene SFE:64-87 */
   s.q = s.qnext;
   s.v = s.vnext;
@@ -1118,6 +1287,8 @@ static void build(Sim& s, const pdf_scene_desc* sc, const pdf_params* p) {
   s.q.assign(sc->rest_positions, sc->rest_positions + 3 * (size_t)N);
   if (sc->positions) s.q.assign(sc->positions, sc->positions + 3 * (size_t)N);
   s.v.assign(3 * (size_t)N, 0.);
+  s.rprev.assign(3 * (size_t)N, 0.);
+  s.rprev_tag.assign(N, -0x40000000);
   if (sc->velocities) s.v.assign(sc->velocities, sc->velocities + 3 * (size_t)N);
   for (double x : s.q)
     if (!std::isfinite(x)) throw std::invalid_argument("non-finite position");
@@ -1354,8 +1525,44 @@ int orc_create(const pdf_scene_desc* scene, const pdf_params* params, orc_sim** 
 
 int orc_step(orc_sim* h, int32_t nsteps, pdf_step_report* report) {
   if (!h || nsteps < 0) return PDF_INVALID_ARG;
-  for (int i = 0; i < nsteps; ++i) step(h->s);
+  try {
+    for (int i = 0; i < nsteps; ++i) step(h->s);
+  } catch (const std::exception& e) {
+    g_error = e.what();
+    return PDF_INVALID_ARG;
+  }
   if (report) *report = h->s.last;
+  return PDF_OK;
+}
+
+int orc_mlp_set_weights(orc_sim* h, const float* w, int32_t count) {
+  if (!h || !w || count != kMParams) return PDF_INVALID_ARG;
+  h->s.mlp_w.assign(w, w + kMParams);
+  h->s.mlp_ready = true;
+  return PDF_OK;
+}
+
+int orc_mlp_log(orc_sim* h, int32_t capacity) {
+  if (!h || capacity < 0) return PDF_INVALID_ARG;
+  h->s.log_cap = capacity;
+  h->s.log_n = 0;
+  h->s.log_X.assign((size_t)capacity * kMIn, 0.f);
+  h->s.log_T.assign((size_t)capacity * kMOut, 0.f);
+  return PDF_OK;
+}
+
+int orc_mlp_samples(orc_sim* h, float* X, float* T, int32_t cap, int32_t* n) {
+  if (!h || !n) return PDF_INVALID_ARG;
+  *n = h->s.log_n;
+  const int m = std::min(h->s.log_n, cap);
+  if (X) std::memcpy(X, h->s.log_X.data(), sizeof(float) * (size_t)m * kMIn);
+  if (T) std::memcpy(T, h->s.log_T.data(), sizeof(float) * (size_t)m * kMOut);
+  return PDF_OK;
+}
+
+int orc_mlp_forward(const float* w, const float* X, int32_t n, float* Y) {
+  if (!w || n < 0 || (n > 0 && (!X || !Y))) return PDF_INVALID_ARG;
+  for (int i = 0; i < n; ++i) mlp_forward_one(w, X + (size_t)i * kMIn, Y + (size_t)i * kMOut);
   return PDF_OK;
 }
 
@@ -1370,6 +1577,7 @@ int orc_set_state(orc_sim* h, const double* q, const double* v) {
   if (!h) return PDF_INVALID_ARG;
   if (q) std::memcpy(h->s.q.data(), q, sizeof(double) * h->s.q.size());
   if (v) std::memcpy(h->s.v.data(), v, sizeof(double) * h->s.v.size());
+  h->s.mlp_tag += 2; /* the previous step's contact impulses no longer apply */
   return PDF_OK;
 }
 

@@ -30,6 +30,13 @@ int orc_get_self_contacts(orc_sim* s, pdf_contact* out, int32_t cap, int32_t* n)
 int orc_get_self_levels(orc_sim* s, int32_t* level_ptr, int32_t level_cap,
                         int32_t* order, int32_t order_cap, int32_t* n_levels);
 int orc_get_residual_history(orc_sim* s, double* out, int32_t cap, int32_t* n);
+/* Learned warm start, restated from the product (climatenet_b200/csrc/mlp.cu):
+ * weights (5,059 floats), the per-contact sample log, and the MLP forward with
+ * the tensor cores' bfloat16 rounding emulated. */
+int orc_mlp_set_weights(orc_sim* s, const float* w, int32_t count);
+int orc_mlp_log(orc_sim* s, int32_t capacity);
+int orc_mlp_samples(orc_sim* s, float* X, float* T, int32_t cap, int32_t* n);
+int orc_mlp_forward(const float* w, const float* X, int32_t n, float* Y);
 /* rows(A), nnz(A), nnz(LHS) (full symmetric), nnz(L) */
 int orc_get_sizes(orc_sim* s, int64_t* sizes4);
 /* Projections p (rows x 3) for positions q (3N). */

@@ -50,17 +50,21 @@ def test_gpu_batch_matches_oracle():
 
 
 @pytest.mark.gpu
-def test_tolerance_mode_matches_oracle():
+@pytest.mark.parametrize("use_graph", [1, 0])  # conditional WHILE graph / host-driven loop
+def test_tolerance_mode_matches_oracle(use_graph):
     s = scenes.cloth_on_sphere(n=30, side=1.0, z=-0.2455, mu=0.3, sphere_center=(0, 0, -0.5),
                                sphere_radius=0.25, pins=True)
-    p = abi.params(time_step=5e-3, iterations=60, residual_tolerance=0.05)
+    p = abi.params(time_step=5e-3, iterations=60, residual_tolerance=0.05, use_graph=use_graph)
     g = native.Simulation(s, p)
     o = Oracle(s, p)
+    total = 0
     for _ in range(5):
         rg = g.step(1)
         ro = o.step(1)
         assert rg.iterations == ro.iterations
         assert 1 <= rg.iterations <= 60
+        total += rg.iterations
+    assert g.stats().iterations == total  # counted on the device
     qg, _ = g.state()
     qo, _ = o.state()
     assert np.abs(qg - qo).max() / np.abs(qo).max() < 1e-6

@@ -1,0 +1,144 @@
+"""Learned warm start on the GPU: the BF16 tensor-core forward and backward
+kernels against the CPU oracles, training, and the warm-started step against
+the CPU oracle's restatement of it.
+"""
+import numpy as np
+import pytest
+
+from climatenet_b200 import abi, native, scenes
+from oracle import mlp_oracle as M
+from oracle.oracle import Oracle, mlp_forward_bf16
+
+from test_mlp_oracle import constant_weights, plane_scene, G
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand_inputs(n, seed):
+    rng = np.random.default_rng(seed)
+    X = rng.normal(0, 1, (n, M.IN)).astype(np.float32)
+    X[:, 9] = 1.0
+    return X
+
+
+def test_forward_matches_bf16_emulation():
+    w = native.mlp_init(seed=11)
+    X = _rand_inputs(3000, 1)
+    Y = native.mlp_forward(w, X)
+    Ye = mlp_forward_bf16(w, X)
+    Y64 = M.forward(w, X)
+    scale = np.abs(Y64).max()
+    # same roundings as the emulation; only the FP32 accumulation order differs
+    assert np.abs(Y - Ye).max() <= 2e-3 * scale
+    assert np.abs(Y - Y64).max() <= 2e-2 * scale
+
+
+def test_forward_edge_sizes():
+    w = native.mlp_init(seed=2)
+    for n in (1, 15, 16, 17, 63, 64, 65):
+        X = _rand_inputs(n, n)
+        np.testing.assert_allclose(native.mlp_forward(w, X), mlp_forward_bf16(w, X), atol=2e-3, rtol=2e-3)
+    assert native.mlp_forward(w, np.zeros((0, 10), np.float32)).shape == (0, 3)
+
+
+def test_gradient_matches_fp64_oracle():
+    """GPU backward (bfloat16 operands, FP32 accumulation) against the FP64
+    backpropagation of the same network on the same samples."""
+    w = native.mlp_init(seed=5)
+    X = _rand_inputs(2048, 3)
+    T = np.random.default_rng(4).normal(0, 1, (2048, 3)).astype(np.float32)
+    loss, g = native.mlp_gradient(w, X, T)
+    loss64, g64 = M.loss_and_grad(w, X, T)
+    assert abs(loss - loss64) <= 2e-2 * loss64
+    cos = float(g @ g64 / (np.linalg.norm(g) * np.linalg.norm(g64)))
+    assert cos > 0.999
+    assert np.linalg.norm(g - g64) <= 3e-2 * np.linalg.norm(g64)
+    # every parameter block gets its gradient
+    o = 0
+    for name, shp in M.SHAPES:
+        k = int(np.prod(shp))
+        gb, gb64 = g[o:o + k], g64[o:o + k]
+        assert np.linalg.norm(gb - gb64) <= 5e-2 * np.linalg.norm(gb64) + 1e-9, name
+        o += k
+
+
+def test_fit_learns_a_teacher_network():
+    teacher = native.mlp_init(seed=21)
+    X = _rand_inputs(40000, 7)
+    T = M.forward(teacher, X).astype(np.float32)
+    w0 = native.mlp_init(seed=22)
+    loss0, _ = M.loss_and_grad(w0, X, T)
+    w, tl, vl = native.mlp_fit(w0, X, T, epochs=15, batch=1024, lr=2e-3, seed=3)
+    loss1, _ = M.loss_and_grad(w, X, T)
+    assert loss1 < 0.05 * loss0
+    assert vl < 0.05 * loss0 and tl < 0.05 * loss0
+
+
+def test_warm_start_known_answer_on_gpu():
+    dt = 2e-3
+    s = plane_scene(mu=0.2)
+    for y, v_over in [((0.5, 0.3, 0.0), (0.0, 0.1, -0.5)), ((-1.0, 0.0, 0.0), (0.0, 0.0, -1.0))]:
+        g = native.Simulation(s, abi.params(time_step=dt, iterations=1, warm_start=abi.PDF_WARM_MLP))
+        g.mlp_set_weights(constant_weights(y))
+        g.step(1)
+        _, v = g.state()
+        np.testing.assert_allclose(v, np.broadcast_to(np.array(v_over) * G * dt, v.shape), atol=1e-12)
+        g.close()
+
+
+def test_warm_start_needs_weights():
+    g = native.Simulation(plane_scene(), abi.params(time_step=2e-3, iterations=2, warm_start=abi.PDF_WARM_MLP))
+    with pytest.raises(native.PdfError) as e:
+        g.step(1)
+    assert e.value.status == abi.PDF_INVALID_ARG
+
+
+def _sphere_scene():
+    """A 24 x 24 cloth 5 mm above the top of a wide rotating sphere (about 50
+    vertices inside its 1 cm contact margin from the first step)."""
+    return scenes.cloth_on_sphere(n=24, side=1.0, z=-0.245, mu=0.4, sphere_center=(0, 0, -1.25),
+                                  sphere_radius=1.0, rotating=1.0)
+
+
+def test_logged_samples_match_oracle():
+    s = _sphere_scene()
+    p = abi.params(time_step=2e-3, iterations=10)
+    g, o = native.Simulation(s, p), Oracle(s, p)
+    g.mlp_log(100000)
+    o.mlp_log(100000)
+    for _ in range(8):
+        g.step(1)
+        o.step(1)
+    Xg, Tg = g.mlp_samples()
+    Xo, To = o.mlp_samples()
+    assert Xg.shape == Xo.shape and Xg.shape[0] > 100
+    np.testing.assert_allclose(Xg, Xo, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(Tg, To, rtol=1e-4, atol=1e-5 * np.abs(To).max())
+
+
+def test_warm_started_steps_match_oracle():
+    """The whole warm-started step (features, BF16 forward, predicted first
+    iteration, impulse memory) against the oracle with the same weights."""
+    s = _sphere_scene()
+    p = abi.params(time_step=2e-3, iterations=10, warm_start=abi.PDF_WARM_MLP)
+    w = native.mlp_init(seed=9)
+    w[-3] = 1.0  # a network that predicts mostly-normal forces of the right size
+    g, o = native.Simulation(s, p), Oracle(s, p)
+    g.mlp_set_weights(w)
+    o.mlp_set_weights(w)
+    for _ in range(6):
+        rg = g.step(1)
+        ro = o.step(1)
+        assert rg.n_contacts == ro.n_contacts
+    qg, _ = g.state()
+    qo, _ = o.state()
+    assert rg.n_contacts > 0
+    assert np.abs(qg - qo).max() / np.abs(qo).max() < 1e-6
+
+
+def test_contact_capacity_overflow_is_reported():
+    s = _sphere_scene()
+    g = native.Simulation(s, abi.params(time_step=2e-3, iterations=2, contact_capacity=4))
+    with pytest.raises(native.PdfError) as e:
+        g.step(1)
+    assert e.value.status == abi.PDF_CAPACITY_EXCEEDED
