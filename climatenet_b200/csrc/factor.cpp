@@ -282,11 +282,13 @@ bool factorize(const Model& m, double dt, int leaf_size, Factor& f, std::string&
       const int64_t ns = f.sn_ns[s], nr = f.sn_nr[s];
       for (int64_t t = 0; t < ft0[s + 1] - ft0[s]; ++t) {
         const int64_t w = std::min(ns, kTile * t + kTile);
-        f.ftile_off[ft0[s] + t + 1] = f.ftile_off[ft0[s] + t] + kTile * w;
+        const int64_t m = std::min<int64_t>(kTile, ns + nr - kTile * t);
+        f.ftile_off[ft0[s] + t + 1] = f.ftile_off[ft0[s] + t] + m * w;
       }
       for (int64_t t = 0; t < f.sn_btile0[s + 1] - f.sn_btile0[s]; ++t) {
         const int64_t hgt = ns - kTile * t + nr;
-        f.btile_off[f.sn_btile0[s] + t + 1] = f.btile_off[f.sn_btile0[s] + t] + kTile * hgt;
+        const int64_t mc = std::min<int64_t>(kTile, ns - kTile * t);
+        f.btile_off[f.sn_btile0[s] + t + 1] = f.btile_off[f.sn_btile0[s] + t] + mc * hgt;
       }
     }
     f.sn_ftile0 = ft0;
@@ -304,15 +306,17 @@ bool factorize(const Model& m, double dt, int leaf_size, Factor& f, std::string&
       for (int64_t t = 0; t < ft0[s + 1] - ft0[s]; ++t) {
         double* T = &f.Wf[f.ftile_off[ft0[s] + t]];
         const int64_t w = std::min(ns, kTile * t + kTile);
+        const int64_t m = std::min<int64_t>(kTile, ns + nr - kTile * t);
         for (int64_t j = 0; j < w; ++j)
-          for (int64_t l = 0; l < kTile; ++l) T[kTile * j + l] = wval(kTile * t + l, j);
+          for (int64_t l = 0; l < m; ++l) T[m * j + l] = wval(kTile * t + l, j);
       }
       for (int64_t t = 0; t < f.sn_btile0[s + 1] - f.sn_btile0[s]; ++t) {
         double* T = &f.Wb[f.btile_off[f.sn_btile0[s] + t]];
         const int64_t j0 = kTile * t, hgt = ns - j0 + nr;
         for (int64_t i = 0; i < hgt; ++i) {
           const int64_t row = i < ns - j0 ? j0 + i : ns + (i - (ns - j0));
-          for (int64_t l = 0; l < kTile; ++l) T[kTile * i + l] = (j0 + l < ns) ? wval(row, j0 + l) : 0.;
+          const int64_t mc = std::min<int64_t>(kTile, ns - j0);
+          for (int64_t l = 0; l < mc; ++l) T[mc * i + l] = wval(row, j0 + l);
         }
       }
     }
@@ -410,11 +414,12 @@ bool emulate_sweeps(const Factor& f, int chunk, const std::vector<double>& bin, 
   const int64_t nWf = (int64_t)f.Wf.size(), nWb = (int64_t)f.Wb.size(), nrows = (int64_t)f.rows.size();
   for (const SweepTask& tk : fa) {
     const SnInfo& s = sn[tk.sn];
-    for (int l = 0; l < kTile; ++l) {
+    const int mrows = std::min(kTile, s.ns + s.nr - tk.tile * kTile);
+    for (int l = 0; l < mrows; ++l) {
       const int row = tk.tile * kTile + l;
       double acc[3] = {0, 0, 0};
       for (int j = tk.a0; j < tk.a1; ++j) {
-        const int64_t wi = tk.off + (int64_t)j * kTile + l;
+        const int64_t wi = tk.off + (int64_t)j * mrows + l;
         if (!chk(wi, nWf, "forward tile") || !chk(s.c0 + j, n, "forward vector")) return false;
         for (int c = 0; c < 3; ++c) acc[c] += f.Wf[wi] * b[s.c0 + j + c * n];
       }
@@ -431,11 +436,12 @@ bool emulate_sweeps(const Factor& f, int chunk, const std::vector<double>& bin, 
   for (const SweepTask& tk : ba) {
     const SnInfo& s = sn[tk.sn];
     const int j0t = tk.tile * kTile, nd = s.ns - j0t;
-    for (int l = 0; l < kTile; ++l) {
+    const int mc = std::min(kTile, nd);
+    for (int l = 0; l < mc; ++l) {
       const int col = j0t + l;
       double acc[3] = {0, 0, 0};
       for (int i = tk.a0; i < tk.a1; ++i) {
-        const int64_t wi = tk.off + (int64_t)i * kTile + l;
+        const int64_t wi = tk.off + (int64_t)i * mc + l;
         if (!chk(wi, nWb, "backward tile")) return false;
         double v[3];
         if (i < nd) {

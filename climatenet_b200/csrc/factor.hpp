@@ -18,14 +18,18 @@
 //    both are plain matrix-vector products with no dependency inside a
 //    supernode, so a supernode can be split across any number of warps.
 //  * W_s is stored twice in 32-lane tiles, one copy per sweep, so that a warp
-//    streams a tile with one coalesced 32-element load per step:
-//      forward tile t  = rows [32t, 32t+32) of W_s, columns 0..w_t-1
-//                        (w_t = min(ns, 32t+32): the zero upper part of D^-1
-//                        is not stored beyond the tile's diagonal block);
-//                        element (row 32t+l, col j) at off + 32 j + l;
-//      backward tile t = columns [32t, 32t+32) of W_s, rows 32t..ns-1 of D^-1
-//                        then the nr rows of L_R D^-1 (h_t = ns - 32t + nr);
-//                        element (local row i, col 32t+l) at off + 32 i + l.
+//    streams a tile with one coalesced load per step:
+//      forward tile t  = rows [32t, 32t+m) of W_s, m = min(32, ns+nr-32t),
+//                        columns 0..w_t-1 (w_t = min(ns, 32t+32): the zero
+//                        upper part of D^-1 is not stored beyond the tile's
+//                        diagonal block); element (row 32t+l, col j) at
+//                        off + m j + l;
+//      backward tile t = columns [32t, 32t+mc) of W_s, mc = min(32, ns-32t),
+//                        rows 32t..ns-1 of D^-1 then the nr rows of L_R D^-1
+//                        (h_t = ns - 32t + nr); element (local row i, col
+//                        32t+l) at off + mc i + l.
+//    Only the last tile of a supernode is narrower than 32; no rows or lanes
+//    of zeros are stored.
 #pragma once
 #include <cstdint>
 #include <string>
@@ -53,7 +57,7 @@ struct Factor {
   int n_levels = 0;
   int64_t nnz_w = 0;             // sum ns(ns+1)/2 + nr ns
   int64_t nnz_l_true = 0;        // structural nnz of L (diagonal included)
-  int64_t tiled_w = 0;           // stored elements per tiled copy (with padding)
+  int64_t tiled_w = 0;           // stored elements per tiled copy (upper triangles of the diagonal blocks included)
   double factor_ms = 0;
 };
 

@@ -56,12 +56,13 @@ __device__ __forceinline__ bool wait_counter(const unsigned long long* ctr, unsi
   return true;
 }
 
-// Issues the (up to) 32 loads of one 32-column slab of a tile: lane l reads
-// element (l, u) at p[32 u]; absent columns read as zero.
+// Issues the (up to) 32 loads of one 32-wide slab of a tile: lane l reads
+// element (l, u) at p[stride u]; absent columns (u >= m) and lanes outside the
+// tile (act false) read as zero.
 template <typename T>
-__device__ __forceinline__ void load_tile(T (&w)[32], const T* p, int m) {
+__device__ __forceinline__ void load_tile(T (&w)[32], const T* p, int m, int stride = kTile, bool act = true) {
 #pragma unroll
-  for (int u = 0; u < 32; ++u) w[u] = (u < m) ? __ldg(p + u * kTile) : T(0);
+  for (int u = 0; u < 32; ++u) w[u] = (act && u < m) ? __ldg(p + u * stride) : T(0);
 }
 
 template <typename T>
@@ -85,9 +86,10 @@ __global__ void __launch_bounds__(256) k_sweep_forward(const SweepTask* __restri
     const SnInfo s = sn[tk.sn];
     // the factor does not depend on the wait: its first 32 tile columns are
     // already in flight while lane 0 checks the children
+    const int mrows = min(kTile, s.ns + s.nr - tk.tile * kTile);
     const T* wbase = W + tk.off + lane;
     T w[32];
-    load_tile(w, wbase + (int64_t)tk.a0 * kTile, min(32, tk.a1 - tk.a0));
+    load_tile(w, wbase + (int64_t)tk.a0 * mrows, min(32, tk.a1 - tk.a0), mrows, lane < mrows);
     int ok = 1;
     if (lane == 0 && s.nchild > 0) ok = wait_counter(sy.fchild + tk.sn, ep * (unsigned long long)s.nchild, sy.err);
     ok = __shfl_sync(0xffffffffu, ok, 0);
@@ -99,7 +101,7 @@ __global__ void __launch_bounds__(256) k_sweep_forward(const SweepTask* __restri
       const T* bz = by + n;
       for (int j0 = tk.a0; j0 < tk.a1; j0 += 32) {
         const int jl = j0 + lane;
-        if (j0 != tk.a0) load_tile(w, wbase + (int64_t)j0 * kTile, min(32, tk.a1 - j0));
+        if (j0 != tk.a0) load_tile(w, wbase + (int64_t)j0 * mrows, min(32, tk.a1 - j0), mrows, lane < mrows);
         T vx = 0, vy = 0, vz = 0;
         if (jl < tk.a1) {
           vx = ldcg(bx + jl);
@@ -154,9 +156,10 @@ __global__ void __launch_bounds__(256) k_sweep_backward(const SweepTask* __restr
     if (t >= ntasks) return;
     const SweepTask tk = tasks[t];
     const SnInfo s = sn[tk.sn];
+    const int mcols = min(kTile, s.ns - tk.tile * kTile);
     const T* wbase = W + tk.off + lane;
     T w[32];
-    load_tile(w, wbase + (int64_t)tk.a0 * kTile, min(32, tk.a1 - tk.a0));
+    load_tile(w, wbase + (int64_t)tk.a0 * mcols, min(32, tk.a1 - tk.a0), mcols, lane < mcols);
     int ok = 1;
     if (lane == 0 && s.parent >= 0)
       ok = wait_counter(sy.bdone + s.parent, ep * (unsigned long long)sn[s.parent].ntb, sy.err);
@@ -168,7 +171,7 @@ __global__ void __launch_bounds__(256) k_sweep_backward(const SweepTask* __restr
     if (ok) {
       for (int i0 = tk.a0; i0 < tk.a1; i0 += 32) {
         const int il = i0 + lane;
-        if (i0 != tk.a0) load_tile(w, wbase + (int64_t)i0 * kTile, min(32, tk.a1 - i0));
+        if (i0 != tk.a0) load_tile(w, wbase + (int64_t)i0 * mcols, min(32, tk.a1 - i0), mcols, lane < mcols);
         T vx = 0, vy = 0, vz = 0;
         if (il < tk.a1) {
           if (il < nd) {
