@@ -1,0 +1,85 @@
+"""Training pipeline of the learned contact warm start.
+
+The step loop logs one (features, converged local force) sample per obstacle
+contact (``Simulation.mlp_log``); this module turns such samples into network
+weights with the library's GPU training kernels:
+
+* inputs and targets are standardised (per feature mean / standard deviation,
+  the constant bias feature left alone) so that Adam sees unit-scale data;
+* the network is trained on the standardised data (``native.mlp_fit``: BF16
+  tensor-core forward / backward, Adam, seeded shuffle, 90/10 split);
+* the standardisation is folded back into the first and last layers, so the
+  step loop evaluates the network on the raw features it computes.
+
+It has no counterpart in the reference, whose contact solver has no learned
+component.
+"""
+import numpy as np
+
+from . import abi, native
+
+_SHAPES = [("W1", (abi.MLP_HIDDEN, abi.MLP_IN)), ("b1", (abi.MLP_HIDDEN,)),
+           ("W2", (abi.MLP_HIDDEN, abi.MLP_HIDDEN)), ("b2", (abi.MLP_HIDDEN,)),
+           ("W3", (abi.MLP_OUT, abi.MLP_HIDDEN)), ("b3", (abi.MLP_OUT,))]
+
+
+def unpack(w):
+    out, o = {}, 0
+    for name, shp in _SHAPES:
+        k = int(np.prod(shp))
+        out[name] = np.asarray(w[o:o + k], dtype=np.float64).reshape(shp)
+        o += k
+    return out
+
+
+def pack(d):
+    return np.concatenate([np.asarray(d[name], dtype=np.float64).ravel() for name, _ in _SHAPES]).astype(np.float32)
+
+
+def normalisation(X, T):
+    """Per-feature (mu, sigma) of the inputs and (nu, tau) of the targets."""
+    X = np.asarray(X, dtype=np.float64)
+    T = np.asarray(T, dtype=np.float64)
+    mu, sigma = X.mean(0), X.std(0)
+    const = sigma < 1e-12          # constant features (the bias input)
+    mu[const] = 0.0
+    sigma[const] = 1.0
+    nu, tau = T.mean(0), T.std(0)
+    tau[tau < 1e-12] = 1.0
+    return mu, sigma, nu, tau
+
+
+def fold(w, mu, sigma, nu, tau):
+    """Weights for raw inputs / outputs from weights trained on
+    (x - mu) / sigma -> (t - nu) / tau."""
+    p = unpack(w)
+    W1 = p["W1"] / sigma[None, :]
+    b1 = p["b1"] - (p["W1"] * (mu / sigma)[None, :]).sum(1)
+    W3 = tau[:, None] * p["W3"]
+    b3 = tau * p["b3"] + nu
+    return pack({"W1": W1, "b1": b1, "W2": p["W2"], "b2": p["b2"], "W3": W3, "b3": b3})
+
+
+def collect(scene, params, steps, capacity=None):
+    """Cold-start run of `steps` steps logging every obstacle contact."""
+    sim = native.Simulation(scene, params)
+    sim.mlp_log(capacity or 4_000_000)
+    for _ in range(steps):
+        sim.step(1)
+    X, T = sim.mlp_samples()
+    sim.close()
+    return X, T
+
+
+def train(X, T, epochs=30, batch=4096, lr=2e-3, seed=0, device=0):
+    """Weights (raw features in, raw forces out) and the losses, trained on the GPU.
+
+    Returns (weights, info) with info = dict(train_loss, val_loss, variance):
+    the losses are those of the standardised problem (1.0 = predicting the
+    mean)."""
+    mu, sigma, nu, tau = normalisation(X, T)
+    Xn = ((np.asarray(X, dtype=np.float64) - mu) / sigma).astype(np.float32)
+    Tn = ((np.asarray(T, dtype=np.float64) - nu) / tau).astype(np.float32)
+    w0 = native.mlp_init(seed)
+    w, tl, vl = native.mlp_fit(w0, Xn, Tn, epochs=epochs, batch=batch, lr=lr, seed=seed, device=device)
+    return fold(w, mu, sigma, nu, tau), dict(train_loss=tl, val_loss=vl, samples=len(X))

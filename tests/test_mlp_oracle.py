@@ -123,3 +123,20 @@ def test_warm_start_requires_weights():
     o = Oracle(plane_scene(), abi.params(time_step=2e-3, iterations=2, warm_start=abi.PDF_WARM_MLP))
     with pytest.raises(OracleError):
         o.step(1)
+
+
+def test_standardisation_folds_into_the_weights():
+    """Weights trained on standardised data, folded back, give the same
+    network on raw features (FP64 oracle forward)."""
+    from climatenet_b200 import warmstart
+    rng = np.random.default_rng(3)
+    X = rng.normal(0, 1, (400, 10)) * np.array([20, 5, 3, 0.1, 300, 80, 80, 0.2, 0.2, 0]) + \
+        np.array([-3, 0, 0, 0.9, 100, 0, 0, 0.5, -0.9, 1])
+    T = rng.normal(0, 1, (400, 3)) * np.array([300, 100, 90]) + np.array([120, 0, 0])
+    mu, sigma, nu, tau = warmstart.normalisation(X, T)
+    assert sigma[9] == 1.0 and mu[9] == 0.0  # the bias feature is left alone
+    w = native.mlp_init(4).astype(np.float64)
+    wf = warmstart.fold(w, mu, sigma, nu, tau)
+    y_std = M.forward(w, (X - mu) / sigma) * tau + nu
+    y_raw = M.forward(wf.astype(np.float64), X)
+    np.testing.assert_allclose(y_raw, y_std, rtol=1e-4, atol=1e-4 * np.abs(y_std).max())
