@@ -128,6 +128,12 @@ void load_weights_file(const std::string& path, float* w) {
 }
 
 // Seeded He initialisation: W ~ N(0, 2 / fan_in) (output layer scaled by 0.1), b = 0.
+void mlp_init_host(float* w, uint64_t seed);
+}  // namespace
+namespace pdfb {
+void mlp_init_params(float* w, uint64_t seed) { mlp_init_host(w, seed); }
+}  // namespace pdfb
+namespace {
 void mlp_init_host(float* w, uint64_t seed) {
   std::mt19937_64 rng(seed);
   std::normal_distribution<double> nd(0., 1.);
@@ -1280,14 +1286,9 @@ int pdf_mlp_train(pdf_handle* h, int32_t epochs, int32_t batch, double learning_
     int cnt = 0;
     if (h->log_cap > 0) CK(cudaMemcpy(&cnt, h->log_n, sizeof(int), cudaMemcpyDeviceToHost));
     if (cnt < 2) return fail(h, PDF_INVALID_ARG, "fewer than 2 logged samples (pdf_mlp_log, then step)");
-    if (!h->mlp_ready) {
-      std::vector<float> w(kMlpParams);
-      mlp_init_host(w.data(), seed);
-      CK(cudaMemcpy(h->mlp_w, w.data(), kMlpParams * sizeof(float), cudaMemcpyHostToDevice));
-    }
     double vl = 0.;
-    const double tl = mlp_train_device(h->mlp_w, h->log_X, h->log_T, cnt, epochs, batch, learning_rate, seed, &vl,
-                                       h->stream);
+    const double tl = mlp_train_standardized(h->mlp_w, h->log_X, h->log_T, cnt, epochs, batch, learning_rate, seed,
+                                             &vl, h->stream);
     h->mlp_ready = true;
     if (train_loss) *train_loss = tl;
     if (val_loss) *val_loss = vl;

@@ -481,6 +481,91 @@ double mlp_train_device(float* prm, const float* X, const float* T, int n, int e
 }
 
 // ---------------------------------------------------------------------------
+// Standardised training: per-column mean / standard deviation of the samples
+// (double accumulation), standardised copies, training, and the
+// standardisation folded back into the first and last layers so that the
+// network takes the raw features and returns raw forces.
+
+__global__ void k_col_stats(const float* __restrict__ A, int64_t n, int ncol, double* __restrict__ acc) {
+  // acc[2c] += sum of column c, acc[2c+1] += sum of squares (ncol <= 16)
+  __shared__ double red[2 * 16];
+  for (int i = threadIdx.x; i < 2 * 16; i += blockDim.x) red[i] = 0.;
+  __syncthreads();
+  double loc[2 * 16];
+  for (int c = 0; c < 2 * ncol; ++c) loc[c] = 0.;
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x)
+    for (int c = 0; c < ncol; ++c) {
+      const double v = A[r * ncol + c];
+      loc[2 * c] += v;
+      loc[2 * c + 1] += v * v;
+    }
+  for (int c = 0; c < 2 * ncol; ++c) atomicAdd(&red[c], loc[c]);
+  __syncthreads();
+  for (int c = threadIdx.x; c < 2 * ncol; c += blockDim.x) atomicAdd(&acc[c], red[c]);
+}
+
+__global__ void k_standardize(const float* __restrict__ A, int64_t n, int ncol, const float* __restrict__ shift,
+                              const float* __restrict__ scale, float* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n * ncol;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = (int)(i % ncol);
+    out[i] = (A[i] - shift[c]) / scale[c];
+  }
+}
+
+double mlp_train_standardized(float* prm, const float* X, const float* T, int n, int epochs, int batch, double lr,
+                              uint64_t seed, double* val_loss, cudaStream_t st) {
+  if (n < 2) throw std::invalid_argument("fewer than 2 samples");
+  DBuf<double> acc(2 * (kIn + kOut));
+  CKM(cudaMemsetAsync(acc.p, 0, 2 * (kIn + kOut) * sizeof(double), st));
+  k_col_stats<<<2 * 148, 256, 0, st>>>(X, n, kIn, acc.p);
+  k_col_stats<<<2 * 148, 256, 0, st>>>(T, n, kOut, acc.p + 2 * kIn);
+  std::vector<double> a(2 * (kIn + kOut));
+  CKM(cudaMemcpyAsync(a.data(), acc.p, a.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+  CKM(cudaStreamSynchronize(st));
+  std::vector<float> shift(kIn + kOut), scale(kIn + kOut);
+  for (int c = 0; c < kIn + kOut; ++c) {
+    const double mean = a[2 * c] / n, var = std::max(0., a[2 * c + 1] / n - mean * mean);
+    double sd = std::sqrt(var), sh = mean;
+    if (sd < 1e-12) {  // constant column (the bias feature): left alone
+      sd = 1.;
+      if (c < kIn) sh = 0.;
+    }
+    shift[c] = (float)sh;
+    scale[c] = (float)sd;
+  }
+  DBuf<float> dshift(kIn + kOut), dscale(kIn + kOut), Xs((size_t)n * kIn), Ts((size_t)n * kOut);
+  CKM(cudaMemcpyAsync(dshift.p, shift.data(), shift.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  CKM(cudaMemcpyAsync(dscale.p, scale.data(), scale.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+  k_standardize<<<4 * 148, 256, 0, st>>>(X, n, kIn, dshift.p, dscale.p, Xs.p);
+  k_standardize<<<4 * 148, 256, 0, st>>>(T, n, kOut, dshift.p + kIn, dscale.p + kIn, Ts.p);
+  std::vector<float> w(kMlpParams);
+  mlp_init_params(w.data(), seed);
+  CKM(cudaMemcpyAsync(prm, w.data(), kMlpParams * sizeof(float), cudaMemcpyHostToDevice, st));
+  const double tl = mlp_train_device(prm, Xs.p, Ts.p, n, epochs, batch, lr, seed, val_loss, st);
+  // fold: W1' = W1 / sigma, b1' = b1 - W1 (mu / sigma); W3' = tau W3, b3' = tau b3 + nu
+  CKM(cudaMemcpyAsync(w.data(), prm, kMlpParams * sizeof(float), cudaMemcpyDeviceToHost, st));
+  CKM(cudaStreamSynchronize(st));
+  for (int h = 0; h < kH; ++h) {
+    double b = w[OB1 + h];
+    for (int i = 0; i < kIn; ++i) {
+      const double wi = w[OW1 + h * kIn + i];
+      b -= wi * (double)shift[i] / (double)scale[i];
+      w[OW1 + h * kIn + i] = (float)(wi / (double)scale[i]);
+    }
+    w[OB1 + h] = (float)b;
+  }
+  for (int o = 0; o < kOut; ++o) {
+    const double tau = scale[kIn + o], nu = shift[kIn + o];
+    for (int h = 0; h < kH; ++h) w[OW3 + o * kH + h] = (float)(tau * w[OW3 + o * kH + h]);
+    w[OB3 + o] = (float)(tau * w[OB3 + o] + nu);
+  }
+  CKM(cudaMemcpyAsync(prm, w.data(), kMlpParams * sizeof(float), cudaMemcpyHostToDevice, st));
+  CKM(cudaStreamSynchronize(st));
+  return tl;
+}
+
+// ---------------------------------------------------------------------------
 // In the step loop.  This file is compiled without FMA contraction, so the
 // feature arithmetic below rounds every product and sum separately, in the
 // order written (the CPU oracle evaluates the same expressions).

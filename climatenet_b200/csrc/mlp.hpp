@@ -30,6 +30,17 @@ void mlp_adam_device(float* prm, const float* grad, float* m1, float* m2, double
 double mlp_train_device(float* prm, const float* X, const float* T, int n, int epochs, int batch, double lr,
                         uint64_t seed, double* val_loss, cudaStream_t st);
 
+// Seeded He initialisation of a parameter vector (host; defined in api.cu).
+void mlp_init_params(float* w, uint64_t seed);
+// Same as mlp_train_device on standardised copies of the samples (per-column
+// mean and standard deviation, the constant bias feature left alone),
+// starting from a seeded He initialisation; the standardisation is folded
+// back into the first and last layers of prm, so the network takes raw
+// features and returns raw forces.  Losses are those of the standardised
+// problem (1.0 = predicting the mean).
+double mlp_train_standardized(float* prm, const float* X, const float* T, int n, int epochs, int batch, double lr,
+                              uint64_t seed, double* val_loss, cudaStream_t st);
+
 // Warm-start kernels of the step loop.
 //  features of every obstacle contact (requires c.c_gap, t_n and the r_prev memory)
 void launch_mlp_features(cudaStream_t st, DContacts c, const double* tn, const double* mass, const double* rprev,

@@ -350,8 +350,10 @@ int pdf_mlp_log(pdf_handle* h, int32_t capacity);
 /* Copies the logged samples out (X: n*10, T: n*3 floats; either NULL to query *n). */
 int pdf_mlp_samples(pdf_handle* h, float* X, float* T, int32_t cap, int32_t* n);
 /* Trains the handle's weights on its logged samples without leaving the
- * device (starting from the current weights, or a seeded He initialisation
- * when none were set). */
+ * device: per-feature standardisation of inputs and targets, seeded He
+ * initialisation, Adam, then the standardisation folded back into the first
+ * and last layers.  The losses are those of the standardised problem
+ * (1.0 = predicting the mean). */
 int pdf_mlp_train(pdf_handle* h, int32_t epochs, int32_t batch,
                   double learning_rate, uint64_t seed, double* train_loss,
                   double* val_loss);

@@ -180,3 +180,22 @@ def test_trained_warm_start_lowers_the_residual():
     # lower after twenty (the reference's contact iteration converges slowly)
     assert warm_first < 0.95 * cold_first
     assert warm_last < 0.95 * cold_last
+
+
+def test_handle_trains_on_its_own_log():
+    """pdf_mlp_train: standardised training on the handle's device-resident
+    sample log; the folded network predicts the logged forces from the raw
+    features."""
+    s = scenes.cloth_on_sphere(n=30, side=1.0, z=-0.195, mu=0.4, sphere_center=(0, 0, -0.5),
+                               sphere_radius=0.3, rotating=1.0)
+    g = native.Simulation(s, abi.params(time_step=2.5e-3, iterations=30))
+    g.mlp_log(200000)
+    g.step(120)
+    X, T = g.mlp_samples()
+    tl, vl = g.mlp_train(epochs=40, batch=2048, lr=2e-3, seed=2)
+    assert vl < 0.6
+    w = g.mlp_get_weights()
+    assert np.isfinite(w).all()
+    Y = native.mlp_forward(w, X)
+    r2 = 1.0 - ((Y - T) ** 2).sum() / ((T - T.mean(0)) ** 2).sum()
+    assert r2 > 0.4
