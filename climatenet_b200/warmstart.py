@@ -83,3 +83,34 @@ def train(X, T, epochs=30, batch=4096, lr=2e-3, seed=0, device=0):
     w0 = native.mlp_init(seed)
     w, tl, vl = native.mlp_fit(w0, Xn, Tn, epochs=epochs, batch=batch, lr=lr, seed=seed, device=device)
     return fold(w, mu, sigma, nu, tau), dict(train_loss=tl, val_loss=vl, samples=len(X))
+
+
+def judge(scene, params, weights, tolerance, steps=10, warmup=3, cap=60):
+    """The cold-start solver as judge of the learned warm start.
+
+    Runs the scene twice from the same state in iterate-to-tolerance mode
+    (`tolerance` on the mean Alart-Curnier residual, at most `cap` PD
+    iterations): cold, and with the warm start.  Returns a dict with the mean
+    iterations and residuals of both runs and `use`: whether the warm start
+    needed fewer iterations (ties go to the cold start, the fallback).
+    `params` are abi.params keyword arguments."""
+    out = {}
+    for name, w in (("cold", None), ("warm", weights)):
+        p = dict(params)
+        p.update(iterations=cap, residual_tolerance=tolerance,
+                 warm_start=abi.PDF_WARM_MLP if w is not None else abi.PDF_WARM_NONE)
+        sim = native.Simulation(scene, abi.params(**p))
+        if w is not None:
+            sim.mlp_set_weights(w)
+        sim.step(warmup)
+        its, res = [], []
+        for _ in range(steps):
+            r = sim.step(1)
+            its.append(r.iterations)
+            if r.n_contacts + r.n_self_contacts > 0:
+                res.append(r.residual)
+        sim.close()
+        out[name] = {"mean_pd_iterations": float(np.mean(its)),
+                     "mean_residual": float(np.mean(res)) if res else 0.0}
+    out["use"] = out["warm"]["mean_pd_iterations"] < out["cold"]["mean_pd_iterations"]
+    return out
