@@ -219,6 +219,25 @@ def residual_pass(sim, steps):
     return (float(np.mean(res)) if res else 0.0), curve, float(np.mean(its))
 
 
+def max_over_ranks(value, dist):
+    """The largest `value` over all ranks (every rank gets it); the value
+    itself without a process group.  Runs on the GPU under NCCL, on the CPU
+    under gloo."""
+    if dist is None:
+        return float(value)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, steps, ms_max):
+    """Steps per second of the whole job: every replica runs `steps` steps,
+    the job takes as long as its slowest rank."""
+    return world * steps / (ms_max / 1e3)
+
+
 def timed_steps(sim, steps, barrier, dist, device):
     import torch
     s0 = sim.stats()
@@ -227,10 +246,7 @@ def timed_steps(sim, steps, barrier, dist, device):
         rep = sim.step(steps)
     barrier()
     s1 = sim.stats()
-    t = torch.tensor([rep.device_ms], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item()), int(s1.kernel_launches - s0.kernel_launches), clk.summary()
+    return max_over_ranks(rep.device_ms, dist), int(s1.kernel_launches - s0.kernel_launches), clk.summary()
 
 
 def e2e_steps(sim, steps, barrier, dist, world):
@@ -253,10 +269,7 @@ def e2e_steps(sim, steps, barrier, dist, world):
         qh.copy_(qout)
         vh.copy_(vout)
     barrier()
-    t = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return world * steps / float(t.item())
+    return whole_job_rate(world, steps, 1e3 * max_over_ranks(time.perf_counter() - t0, dist))
 
 
 def roofline(sim, fp32):
@@ -317,7 +330,7 @@ def main():
     sim_r.step(args.warmup)
     ms_r, launches_r, clk_r = timed_steps(sim_r, K, barrier, dist, local)
     res_r, curve_r, _ = residual_pass(sim_r, K)
-    line_extra["fp64_plain_fixed20"] = {"steps_per_s": world * K / (ms_r / 1e3), "ms_per_step": ms_r / K,
+    line_extra["fp64_plain_fixed20"] = {"steps_per_s": whole_job_rate(world, K, ms_r), "ms_per_step": ms_r / K,
                                         "pd_iterations": PLAIN_ITERATIONS, "mean_residual": res_r,
                                         "residual_curve": curve_r, "gpu_launches": launches_r}
     line_extra["roofline_fp64"] = roofline(sim_r, False)
@@ -349,7 +362,7 @@ def main():
             sim.step(args.warmup)
             ms, launches, clk = timed_steps(sim, K, barrier, dist, local)
             res, _, mean_it = residual_pass(sim, K)
-            line_extra[name] = {"steps_per_s": world * K / (ms / 1e3), "ms_per_step": ms / K,
+            line_extra[name] = {"steps_per_s": whole_job_rate(world, K, ms), "ms_per_step": ms / K,
                                 "mean_pd_iterations": mean_it, "mean_residual": res, "tolerance": tol,
                                 "iteration_cap": cap, "gpu_launches": launches}
             if name != arms[-1][0]:
@@ -361,7 +374,7 @@ def main():
         line_extra["speedup_vs_fixed20"] = (line_extra[head]["steps_per_s"] /
                                             line_extra["fp64_plain_fixed20"]["steps_per_s"])
 
-    value = world * K / (ms / 1e3)
+    value = whole_job_rate(world, K, ms)
     e2e_value = e2e_steps(sim, max(3, K // 2), barrier, dist, world)
     roof = roofline(sim, prec == "fp32")
     ms_local, bytes_local = sim.time_phase(1, reps=20)
