@@ -230,6 +230,7 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
     for (int c = 0; c < 3; ++c) {
       ob.c[c] = o.center[c];
       ob.p[c] = o.point[c];
+      ob.s[c] = o.size[c];
     }
     ob.R = o.radius;
     // RotatingSphere ctor (RotatingSphere.cpp:29-37): omega * axis.normalized()

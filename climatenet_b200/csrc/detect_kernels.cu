@@ -10,6 +10,39 @@
 
 namespace pdfb {
 
+// Axis-aligned box (StaticAxisAlignedBox.cpp:41-135): coordinates relative to
+// the box centre; a vertex is in contact when inside (no margin); the contact
+// side is the first of TOP (+y), BOTTOM (-y), LEFT (-x), RIGHT (+x),
+// FRONT (+z), BACK (-z) at the smallest distance.
+__device__ __forceinline__ double3 box_relative(double3 x, const DObstacle& ob) {
+  return make_double3((x.x - ob.c[0]) - 0.5 * ob.s[0], (x.y - ob.c[1]) - 0.5 * ob.s[1],
+                      (x.z - ob.c[2]) - 0.5 * ob.s[2]);
+}
+__device__ __forceinline__ double comp3(double3 v, int i) { return i == 0 ? v.x : (i == 1 ? v.y : v.z); }
+__device__ __forceinline__ bool box_inside(double3 x, const DObstacle& ob) {
+  const double3 r = box_relative(x, ob);
+  for (int i = 0; i < 3; ++i)
+    if (fabs(comp3(r, i)) > ob.s[i] / 2) return false;
+  return true;
+}
+// nearest side: its axis and sign; *dist = distance to it
+__device__ __forceinline__ void box_side(double3 r, const DObstacle& ob, int* axis, double* sign, double* dist) {
+  const int ax[6] = {1, 1, 0, 0, 2, 2};
+  const double sg[6] = {1., -1., -1., 1., 1., -1.};
+  double best = 0.;
+  int b = -1;
+  for (int k = 0; k < 6; ++k) {
+    const double d = fabs(comp3(r, ax[k]) - sg[k] * 0.5 * ob.s[ax[k]]);
+    if (b < 0 || d < best) {
+      best = d;
+      b = k;
+    }
+  }
+  *axis = ax[b];
+  *sign = sg[b];
+  *dist = best;
+}
+
 // Per (obstacle, vertex) flag, obstacle-major so that a stable compaction gives
 // the reference's order (obstacles in scene order, vertices ascending:
 // PhysicScene::getCollisionsInfoExceptFor PhysicScene.cpp:115-181 and
@@ -32,6 +65,8 @@ __global__ void k_obstacle_flags(int N, const double* __restrict__ q, DObstacles
       // StaticPlane::checkCollision StaticPlane.cpp:57-73 (hard-coded 1.5 cm)
       const double d = dot3(x - make_double3(ob.p[0], ob.p[1], ob.p[2]), make_double3(ob.n[0], ob.n[1], ob.n[2]));
       hit = d < 1.5e-2;
+    } else if (ob.type == 4) {
+      hit = box_inside(x, ob);
     } else {
       int tri;
       double3 cp;
@@ -92,6 +127,12 @@ __global__ void k_obstacle_materialize(int N, const double* __restrict__ q, DObs
     } else if (ob.type == 2) {
       nrm = make_double3(ob.n[0], ob.n[1], ob.n[2]);
       gap = dot3(x - make_double3(ob.p[0], ob.p[1], ob.p[2]), nrm);
+    } else if (ob.type == 4) {
+      int axis;
+      double sign, dist;
+      box_side(box_relative(x, ob), ob, &axis, &sign, &dist);
+      nrm = make_double3(axis == 0 ? sign : 0., axis == 1 ? sign : 0., axis == 2 ? sign : 0.);
+      gap = -dist;
     } else {
       int tri;
       double3 cp;

@@ -422,7 +422,13 @@ int pdf_scene_load_json(const char* json_path, pdf_scene** out) {
         ob.angular_speed = req_double(oo, "Radial Speed");
         ob.rotation_start_time = req_double(oo, "Rotation Start Time");
         ob.material = (int)req_uint(oo, "Material Identifier");
-      } else if (type == "Axis Aligned Box" || type == "Moving Mesh") {
+      } else if (type == "Axis Aligned Box") {
+        // getStaticAxisAlignedBoxFromObject (src/scene_building.cpp:205-211)
+        ob.type = PDF_OBSTACLE_BOX;
+        vec3(req_array(oo, "Position"), ob.center);
+        ob.material = (int)req_uint(oo, "Material Identifier");
+        vec3(req_array(oo, "Size"), ob.size);
+      } else if (type == "Moving Mesh") {
         throw std::invalid_argument("obstacle type \"" + type + "\" is not supported by this build");
       } else {
         throw std::invalid_argument("JSON reader - Error : Invalid type for static object type");

@@ -26,6 +26,7 @@ struct DObstacle {
   double rot[3], time_before_start;
   double p[3], n[3];
   double tol;
+  double s[3];  // box: size (c = the corner with the smallest coordinates)
   const double* mv;
   const int* mt;
 };

@@ -309,7 +309,9 @@ void build_model(const pdf_scene_desc& sc, const pdf_params& p, Model& m) {
   // obstacles
   for (int k = 0; k < sc.n_obstacles; ++k) {
     pdf_obstacle o = sc.obstacles[k];
-    if (o.type < 0 || o.type > 3) throw std::invalid_argument("unknown obstacle type");
+    if (o.type < 0 || o.type > 4) throw std::invalid_argument("unknown obstacle type");
+    if (o.type == PDF_OBSTACLE_BOX && !(o.size[0] >= 0. && o.size[1] >= 0. && o.size[2] >= 0.))
+      throw std::invalid_argument("box obstacle with a negative size");
     if (o.material < 0 || o.material >= sc.n_materials) throw std::invalid_argument("obstacle material out of range");
     std::vector<double> ov;
     std::vector<int> ot;

@@ -90,6 +90,10 @@ class Scene:
         self.obstacles.append(dict(type=abi.PDF_OBSTACLE_PLANE, point=point, normal=normal,
                                    material=material))
 
+    def add_box(self, position, size, material=0):
+        """Axis-aligned box; `position` is its corner with the smallest coordinates."""
+        self.obstacles.append(dict(type=abi.PDF_OBSTACLE_BOX, center=position, size=size, material=material))
+
     def add_mesh_obstacle(self, vertices, triangles, threshold, material=0):
         self.obstacles.append(dict(type=abi.PDF_OBSTACLE_MESH,
                                    vertices=np.ascontiguousarray(vertices, dtype=np.float64),
@@ -140,7 +144,7 @@ class Scene:
             ob.type = o["type"]
             ob.material = o.get("material", 0)
             ob.mesh = o.get("mesh", -1)
-            for key in ("center", "axis", "point", "normal"):
+            for key in ("center", "axis", "point", "normal", "size"):
                 if key in o:
                     for c in range(3):
                         getattr(ob, key)[c] = float(o[key][c])

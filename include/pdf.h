@@ -41,7 +41,9 @@ enum pdf_obstacle_type {
   PDF_OBSTACLE_SPHERE = 0,          /* StaticSphere   (src/physics/StaticSphere.cpp:35-47)   */
   PDF_OBSTACLE_ROTATING_SPHERE = 1, /* RotatingSphere (src/physics/RotatingSphere.cpp:71-93) */
   PDF_OBSTACLE_PLANE = 2,           /* StaticPlane    (src/physics/StaticPlane.cpp:57-73)    */
-  PDF_OBSTACLE_MESH = 3             /* StaticMesh     (src/physics/StaticMesh.cpp:33-56)     */
+  PDF_OBSTACLE_MESH = 3,            /* StaticMesh     (src/physics/StaticMesh.cpp:33-56)     */
+  PDF_OBSTACLE_BOX = 4              /* StaticAxisAlignedBox
+                                       (src/physics/StaticAxisAlignedBox.cpp:41-201) */
 };
 
 typedef struct pdf_obstacle {
@@ -62,6 +64,8 @@ typedef struct pdf_obstacle {
   int32_t mesh;                 /* -1: acts on every dynamic mesh (the
                                    reference's behaviour); >= 0: only on that
                                    mesh (batches of independent cloths)       */
+  double size[3];               /* box: "Size"; its "Position" (the corner
+                                   with the smallest coordinates) is center  */
 } pdf_obstacle;
 
 /* ---- dynamic meshes (include/physics/PhysicMesh.hpp, PhysicParameters) -- */

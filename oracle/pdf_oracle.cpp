@@ -584,6 +584,7 @@ struct Obstacle {
   std::vector<std::array<int, 3>> mtris;
   double threshold;
   int mesh; /* -1: every dynamic mesh; else only vertices of that mesh */
+  V3 size;  /* box: extents; center = the corner with the smallest coordinates */
 };
 
 struct CInfo {
@@ -835,6 +836,44 @@ static void detect_obstacles(Sim& s) {
         c.gap = d;
         c.cp = verts[i] - ob.normal * d;
         c.normal = ob.normal;
+        c.speed = {0, 0, 0};
+        found.push_back(c);
+      }
+    } else if (ob.type == PDF_OBSTACLE_BOX) {
+      /* StaticAxisAlignedBox::checkCollision StaticAxisAlignedBox.cpp:41-58:
+       * relative = x - position - size/2; inside when |relative_i| <= size_i/2
+       * for every axis; nearest side by std::min_element over TOP, BOTTOM,
+       * LEFT, RIGHT, FRONT, BACK (:67-80, first of equal distances) with
+       * distance |relative[axis] - sign size[axis]/2| (:96-105); contact point
+       * the projection on that side (:84-94), normal the side's axis vector. */
+      const int ax[6] = {1, 1, 0, 0, 2, 2};
+      const double sg[6] = {1., -1., -1., 1., 1., -1.};
+      for (int i = 0; i < N; ++i) {
+        const V3 x = verts[i];
+        const double r[3] = {(x.x - ob.center.x) - 0.5 * ob.size.x, (x.y - ob.center.y) - 0.5 * ob.size.y,
+                             (x.z - ob.center.z) - 0.5 * ob.size.z};
+        const double sz[3] = {ob.size.x, ob.size.y, ob.size.z};
+        bool in = true;
+        for (int k = 0; k < 3; ++k)
+          if (std::abs(r[k]) > sz[k] / 2) in = false;
+        if (!in) continue;
+        int b = 0;
+        double best = std::abs(r[ax[0]] - sg[0] * 0.5 * sz[ax[0]]);
+        for (int k = 1; k < 6; ++k) {
+          const double d = std::abs(r[ax[k]] - sg[k] * 0.5 * sz[ax[k]]);
+          if (d < best) {
+            best = d;
+            b = k;
+          }
+        }
+        double cpr[3] = {r[0], r[1], r[2]};
+        cpr[ax[b]] = sg[b] * 0.5 * sz[ax[b]];
+        CInfo c;
+        c.vertex = i;
+        c.cp = {(cpr[0] + ob.center.x) + 0.5 * sz[0], (cpr[1] + ob.center.y) + 0.5 * sz[1],
+                (cpr[2] + ob.center.z) + 0.5 * sz[2]};
+        c.normal = {ax[b] == 0 ? sg[b] : 0., ax[b] == 1 ? sg[b] : 0., ax[b] == 2 ? sg[b] : 0.};
+        c.gap = -best;
         c.speed = {0, 0, 0};
         found.push_back(c);
       }
@@ -1451,12 +1490,13 @@ static void build(Sim& s, const pdf_scene_desc* sc, const pdf_params* p) {
     ob.normal = normalized(V3{o.normal[0], o.normal[1], o.normal[2]});
     ob.threshold = o.threshold;
     ob.mesh = o.mesh;
+    ob.size = {o.size[0], o.size[1], o.size[2]};
     if (ob.mesh >= sc->n_meshes) throw std::invalid_argument("obstacle mesh out of range");
     if (o.type == PDF_OBSTACLE_MESH) {
       for (int i = 0; i < o.n_vertices; ++i) ob.mverts.push_back(ld(o.vertices, i));
       for (int t = 0; t < o.n_triangles; ++t)
         ob.mtris.push_back({o.triangles[3 * t], o.triangles[3 * t + 1], o.triangles[3 * t + 2]});
-    } else if (o.type < 0 || o.type > 3) {
+    } else if (o.type < 0 || o.type > 4) {
       throw std::invalid_argument("unknown obstacle type");
     }
     s.obstacles.push_back(ob);
