@@ -26,6 +26,7 @@ PDF_OBSTACLE_ROTATING_SPHERE = 1
 PDF_OBSTACLE_PLANE = 2
 PDF_OBSTACLE_MESH = 3
 PDF_OBSTACLE_BOX = 4
+PDF_OBSTACLE_MOVING_MESH = 5
 
 PDF_FP64 = 0
 PDF_FP32_REFINE = 1
@@ -49,6 +50,7 @@ class pdf_obstacle(C.Structure):
         ("n_vertices", C.c_int32), ("n_triangles", C.c_int32),
         ("vertices", _dp), ("triangles", _ip), ("threshold", C.c_double),
         ("mesh", C.c_int32), ("size", C.c_double * 3),
+        ("n_frames", C.c_int32), ("frame_interval", C.c_double),
     ]
 
 

@@ -220,6 +220,7 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   // obstacles
   h->obs.n = (int)m.obstacles.size();
   h->host_obs.assign(h->obs.n, DObstacle{});
+  h->moving.assign(h->obs.n, MovingClock{});
   for (int k = 0; k < h->obs.n; ++k) {
     const pdf_obstacle& o = m.obstacles[k];
     DObstacle& ob = h->host_obs[k];
@@ -259,12 +260,24 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
     ob.n[2] = nz;
     // StaticMesh keeps tol^2 and passes sqrt(tol^2) (StaticMesh.cpp:25-31)
     ob.tol = std::sqrt(o.threshold * o.threshold);
-    if (o.type == PDF_OBSTACLE_MESH) {
+    if (o.type == PDF_OBSTACLE_MESH || o.type == PDF_OBSTACLE_MOVING_MESH) {
       d.obstacle_v.push_back(upload(m.obstacle_vertices[k]));
       d.obstacle_t.push_back(upload(m.obstacle_triangles[k]));
       ob.mv = d.obstacle_v.back();
       ob.mt = d.obstacle_t.back();
       ob.n_tri = (int)m.obstacle_triangles[k].size() / 3;
+    }
+    if (o.type == PDF_OBSTACLE_MOVING_MESH) {
+      // every key frame resident; the current mesh starts as key frame 0
+      MovingClock& mc = h->moving[k];
+      mc.n_frames = o.n_frames;
+      mc.n_vertices = o.n_vertices;
+      mc.interval = o.frame_interval;
+      mc.frames = ob.mv;
+      mc.cur = dalloc<double>(3 * (size_t)o.n_vertices);
+      d.obstacle_v.push_back(mc.cur);
+      CK(cudaMemcpy(mc.cur, mc.frames, 3 * (size_t)o.n_vertices * sizeof(double), cudaMemcpyDeviceToDevice));
+      ob.mv = mc.cur;
     }
     h->host_time_before_start.push_back(o.rotation_start_time);
   }
@@ -561,7 +574,17 @@ void step_once(pdf_handle* h, bool want_report) {
                                                   h->prm.gravity[1], h->prm.gravity[2], dt);
   // obstacle detection on the start-of-step positions (SimulationBase.cpp:333-366)
   if (h->obs.n > 0) {
-    for (int k = 0; k < h->obs.n; ++k) h->host_obs[k].time_before_start = h->host_time_before_start[k];
+    for (int k = 0; k < h->obs.n; ++k) {
+      DObstacle& ob = h->host_obs[k];
+      ob.time_before_start = h->host_time_before_start[k];
+      const MovingClock& mc = h->moving[k];
+      if (mc.n_frames > 0) {
+        ob.fprev = mc.frames + 3 * (size_t)mc.n_vertices * (mc.next - 1);
+        ob.fnext = mc.frames + 3 * (size_t)mc.n_vertices * mc.next;
+        ob.frame_dt = mc.frame_time(mc.next) - mc.frame_time(mc.next - 1);
+        ob.moving = mc.in_movement() ? 1 : 0;
+      }
+    }
     CK(cudaMemcpyAsync(d.obstacles, h->host_obs.data(), h->obs.n * sizeof(DObstacle), cudaMemcpyHostToDevice, st));
     k_obstacle_flags<<<blocks_for(N), kThreads, 0, st>>>(N, d.q, h->obs, d.flags);
     thrust::counting_iterator<int> it(0);
@@ -649,6 +672,20 @@ void step_once(pdf_handle* h, bool want_report) {
   CK(cudaGetLastError());
   // RotatingSphere::update (RotatingSphere.cpp:39-43)
   for (auto& t : h->host_time_before_start) t -= dt;
+  // MovingMesh::update (MovingMesh.cpp:43-84): advance the clock, at most one
+  // key frame, then interpolate the current mesh while in movement
+  for (MovingClock& mc : h->moving) {
+    if (mc.n_frames == 0) continue;
+    mc.clock += dt;
+    if (mc.frame_time(mc.next) < mc.clock && mc.next + 1 < mc.n_frames) mc.next += 1;
+    if (mc.in_movement()) {
+      const double t0 = mc.frame_time(mc.next - 1), t1 = mc.frame_time(mc.next);
+      const size_t nv3 = 3 * (size_t)mc.n_vertices;
+      launch_moving_mesh_lerp(st, (int)nv3, mc.frames + nv3 * (mc.next - 1), mc.frames + nv3 * mc.next,
+                              (mc.clock - t0) / (t1 - t0), mc.cur);
+      h->launches_outside += 1;
+    }
+  }
   h->time += dt;
   h->stats.steps += 1;
   h->launches_outside += launches_per_step_extra(h);

@@ -4,6 +4,8 @@
 // (inside / outside, closest-point region) must come out bit-identical.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "device.cuh"
 #include "geometry.cuh"
 #include "kernels.hpp"
@@ -76,6 +78,18 @@ __global__ void k_obstacle_flags(int N, const double* __restrict__ q, DObstacles
   }
 }
 
+// MovingMesh::updateCurrentMesh MovingMesh.cpp:67-84: the current mesh is
+// prev * (1 - a) + next * a, componentwise.
+__global__ void k_moving_mesh_lerp(int n3, const double* __restrict__ prev, const double* __restrict__ next, double a,
+                                   double* __restrict__ cur) {
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n3; k += gridDim.x * blockDim.x)
+    cur[k] = prev[k] * (1 - a) + next[k] * a;
+}
+
+void launch_moving_mesh_lerp(cudaStream_t st, int n3, const double* prev, const double* next, double a, double* cur) {
+  k_moving_mesh_lerp<<<std::min((n3 + 255) / 256, 1184), 256, 0, st>>>(n3, prev, next, a, cur);
+}
+
 // Obstacle contacts beyond the capacity are dropped: the count is clamped and
 // bit 1 of the handle's error word is set (the step then reports
 // PDF_CAPACITY_EXCEEDED).
@@ -135,11 +149,19 @@ __global__ void k_obstacle_materialize(int N, const double* __restrict__ q, DObs
       gap = -dist;
     } else {
       int tri;
-      double3 cp;
-      mesh_obstacle_closest(x, ob.mv, ob.mt, ob.n_tri, ob.tol, &tri, &cp);
-      const double3 a = ld3(ob.mv, ob.mt[3 * tri]), b = ld3(ob.mv, ob.mt[3 * tri + 1]), cc = ld3(ob.mv, ob.mt[3 * tri + 2]);
+      double3 cp, w;
+      mesh_obstacle_closest(x, ob.mv, ob.mt, ob.n_tri, ob.tol, &tri, &cp, &w);
+      const int i0 = ob.mt[3 * tri], i1 = ob.mt[3 * tri + 1], i2 = ob.mt[3 * tri + 2];
+      const double3 a = ld3(ob.mv, i0), b = ld3(ob.mv, i1), cc = ld3(ob.mv, i2);
       nrm = normalized3(cross3(b - a, cc - a));  // Mesh::getTriangleNormal Mesh.cpp:120-126
       gap = dot3(x - cp, nrm);
+      if (ob.type == 5 && ob.moving) {
+        // MovingMesh::getPointSpeed MovingMesh.cpp:232-249
+        const double3 pn = tri_point(ld3(ob.fnext, i0), ld3(ob.fnext, i1), ld3(ob.fnext, i2), w);
+        const double3 pp = tri_point(ld3(ob.fprev, i0), ld3(ob.fprev, i1), ld3(ob.fprev, i2), w);
+        const double3 dp = pn - pp;
+        sp = make_double3(dp.x / ob.frame_dt, dp.y / ob.frame_dt, dp.z / ob.frame_dt);
+      }
     }
     c.c_gap[k] = gap;
     c.c_vertex[k] = i;

@@ -89,11 +89,11 @@ __device__ __forceinline__ void tri_box(double3 a, double3 b, double3 c, double3
 // closest point, kept if |c - x|^2 < tol^2, closest kept triangle (first on
 // ties, triangles ascending), contact if its distance^2 < tol^2.
 __device__ __forceinline__ bool mesh_obstacle_closest(double3 x, const double* mv, const int* mt, int nt, double tol,
-                                                      int* tri_out, double3* cp_out) {
+                                                      int* tri_out, double3* cp_out, double3* w_out = nullptr) {
   const double t = 1.1 * tol, tol_sq = tol * tol;
   double best = __longlong_as_double(0x7ff0000000000000LL);  // +inf
   int bt = -1;
-  double3 bp = make_double3(0., 0., 0.);
+  double3 bp = make_double3(0., 0., 0.), bw = bp;
   for (int k = 0; k < nt; ++k) {
     const double3 a = ld3(mv, mt[3 * k]), b = ld3(mv, mt[3 * k + 1]), c = ld3(mv, mt[3 * k + 2]);
     double3 lo, hi;
@@ -110,10 +110,12 @@ __device__ __forceinline__ bool mesh_obstacle_closest(double3 x, const double* m
       best = d2;
       bt = k;
       bp = p;
+      bw = w;
     }
   }
   *tri_out = bt;
   *cp_out = bp;
+  if (w_out) *w_out = bw;
   return best < tol_sq;
 }
 

@@ -59,6 +59,18 @@ struct DeviceBuffers {
 
 }  // namespace pdfb
 
+// Clock of one key-framed moving-mesh obstacle (MovingMesh.cpp:28-84):
+// every key frame stays resident on the device; `cur` is the interpolated mesh
+// that detection reads.
+struct MovingClock {
+  int n_frames = 0, n_vertices = 0, next = 1;
+  double interval = 0., clock = 0.;
+  const double* frames = nullptr;
+  double* cur = nullptr;
+  double frame_time(int f) const { return (double)f * interval; }
+  bool in_movement() const { return clock >= frame_time(next - 1) && clock <= frame_time(next); }
+};
+
 struct pdf_handle {
   pdfb::Model model;
   pdfb::Factor fac;
@@ -67,6 +79,7 @@ struct pdf_handle {
   pdfb::DModel dm{};
   pdfb::DObstacles obs{};
   std::vector<pdfb::DObstacle> host_obs;
+  std::vector<MovingClock> moving;  // one per obstacle (n_frames = 0: not moving)
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[8] = {};
   cudaGraphExec_t graph = nullptr;

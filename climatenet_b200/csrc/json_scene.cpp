@@ -11,6 +11,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <iomanip>
 #include <map>
 #include <memory>
 #include <sstream>
@@ -429,7 +430,35 @@ int pdf_scene_load_json(const char* json_path, pdf_scene** out) {
         ob.material = (int)req_uint(oo, "Material Identifier");
         vec3(req_array(oo, "Size"), ob.size);
       } else if (type == "Moving Mesh") {
-        throw std::invalid_argument("obstacle type \"" + type + "\" is not supported by this build");
+        // getMovingMeshFromObject (src/scene_building.cpp:248-276): key frame f
+        // is "<Obj Prefix><f, zero-padded to Suffix Size>.obj" at time
+        // f * "Time Between Frame".  Every key frame is read here, at load
+        // time (the reference reads them as its clock reaches them).
+        ob.type = PDF_OBSTACLE_MOVING_MESH;
+        const std::string prefix = req_string(oo, "Obj Prefix");
+        const uint64_t suffix = req_uint(oo, "Suffix Size");
+        const uint64_t frames = req_uint(oo, "Number Frame");
+        ob.material = (int)req_uint(oo, "Material Identifier");
+        ob.frame_interval = req_double(oo, "Time Between Frame");
+        ob.threshold = req_double(oo, "Collision tolerance");
+        if (frames < 2) throw std::invalid_argument("Moving Mesh needs at least two frames");
+        if (frames > (1u << 20)) throw std::invalid_argument("Moving Mesh frame count too large");
+        ob.n_frames = (int)frames;
+        std::vector<double> fv;
+        std::vector<int> ft;
+        for (uint64_t f = 0; f < frames; ++f) {
+          std::ostringstream name;
+          name << prefix;
+          if (suffix > 0) name << std::setfill('0') << std::setw((int)suffix);
+          name << f << ".obj";
+          read_obj(resolve(base, name.str()), fv, ft);
+          if (f == 0) {
+            ot = ft;
+          } else if (fv.size() != ov.size() / f) {
+            throw std::invalid_argument("Moving Mesh key frame " + name.str() + " has a different vertex count");
+          }
+          ov.insert(ov.end(), fv.begin(), fv.end());
+        }
       } else {
         throw std::invalid_argument("JSON reader - Error : Invalid type for static object type");
       }
@@ -447,8 +476,9 @@ int pdf_scene_load_json(const char* json_path, pdf_scene** out) {
     return PDF_INVALID_ARG;
   }
   for (size_t k = 0; k < sc->obstacles.size(); ++k) {
-    if (sc->obstacles[k].type == PDF_OBSTACLE_MESH) {
-      sc->obstacles[k].n_vertices = (int)(sc->ob_v[k].size() / 3);
+    if (sc->obstacles[k].type == PDF_OBSTACLE_MESH || sc->obstacles[k].type == PDF_OBSTACLE_MOVING_MESH) {
+      const size_t frames = sc->obstacles[k].type == PDF_OBSTACLE_MOVING_MESH ? sc->obstacles[k].n_frames : 1;
+      sc->obstacles[k].n_vertices = (int)(sc->ob_v[k].size() / 3 / frames);
       sc->obstacles[k].n_triangles = (int)(sc->ob_t[k].size() / 3);
       sc->obstacles[k].vertices = sc->ob_v[k].data();
       sc->obstacles[k].triangles = sc->ob_t[k].data();

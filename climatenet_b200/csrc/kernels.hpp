@@ -27,8 +27,14 @@ struct DObstacle {
   double p[3], n[3];
   double tol;
   double s[3];  // box: size (c = the corner with the smallest coordinates)
-  const double* mv;
+  const double* mv;  // mesh obstacles: current vertex positions
   const int* mt;
+  // moving mesh: the key frames around its clock, their time span, and
+  // whether the clock lies between them (contact speed is zero otherwise)
+  const double* fprev;
+  const double* fnext;
+  double frame_dt;
+  int moving;
 };
 struct DObstacles {
   int n;
@@ -90,6 +96,7 @@ __global__ void k_obstacle_flags(int N, const double* q, DObstacles obs, unsigne
 __global__ void k_obstacle_materialize(int N, const double* q, DObstacles obs, const int* idx, const int* vmat,
                                        const double* friction, int n_mat, DContacts c);
 __global__ void k_clamp_contacts(int* n, int cap, int* err);
+void launch_moving_mesh_lerp(cudaStream_t st, int n3, const double* prev, const double* next, double a, double* cur);
 __global__ void k_contact_slots(DContacts c);
 __global__ void k_contact_slots_fill(DContacts c);
 __global__ void k_contact_slots_reset(DContacts c);

@@ -309,16 +309,19 @@ void build_model(const pdf_scene_desc& sc, const pdf_params& p, Model& m) {
   // obstacles
   for (int k = 0; k < sc.n_obstacles; ++k) {
     pdf_obstacle o = sc.obstacles[k];
-    if (o.type < 0 || o.type > 4) throw std::invalid_argument("unknown obstacle type");
+    if (o.type < 0 || o.type > 5) throw std::invalid_argument("unknown obstacle type");
     if (o.type == PDF_OBSTACLE_BOX && !(o.size[0] >= 0. && o.size[1] >= 0. && o.size[2] >= 0.))
       throw std::invalid_argument("box obstacle with a negative size");
     if (o.material < 0 || o.material >= sc.n_materials) throw std::invalid_argument("obstacle material out of range");
     std::vector<double> ov;
     std::vector<int> ot;
-    if (o.type == PDF_OBSTACLE_MESH) {
+    if (o.type == PDF_OBSTACLE_MOVING_MESH && (o.n_frames < 2 || !(o.frame_interval > 0.)))
+      throw std::invalid_argument("moving mesh needs at least two key frames and a positive interval");
+    if (o.type == PDF_OBSTACLE_MESH || o.type == PDF_OBSTACLE_MOVING_MESH) {
       if (o.n_vertices <= 0 || o.n_triangles <= 0 || !o.vertices || !o.triangles)
         throw std::invalid_argument("mesh obstacle without geometry");
-      ov.assign(o.vertices, o.vertices + 3 * (size_t)o.n_vertices);
+      const size_t frames = o.type == PDF_OBSTACLE_MOVING_MESH ? (size_t)o.n_frames : 1;
+      ov.assign(o.vertices, o.vertices + 3 * (size_t)o.n_vertices * frames);
       ot.assign(o.triangles, o.triangles + 3 * (size_t)o.n_triangles);
       for (int x : ot)
         if (x < 0 || x >= o.n_vertices) throw std::invalid_argument("mesh obstacle index out of range");

@@ -100,6 +100,17 @@ class Scene:
                                    triangles=np.ascontiguousarray(triangles, dtype=np.int32),
                                    threshold=threshold, material=material))
 
+    def add_moving_mesh(self, frames, triangles, frame_interval, tolerance, material=0):
+        """Key-framed moving mesh: `frames` (F, V, 3), key frame f reached at
+        time f * frame_interval, linear interpolation in between."""
+        frames = np.ascontiguousarray(frames, dtype=np.float64)
+        if frames.ndim != 3 or frames.shape[0] < 2 or frames.shape[2] != 3:
+            raise ValueError("frames must be (F >= 2, V, 3)")
+        self.obstacles.append(dict(type=abi.PDF_OBSTACLE_MOVING_MESH, frames=frames,
+                                   triangles=np.ascontiguousarray(triangles, dtype=np.int32),
+                                   frame_interval=frame_interval, threshold=tolerance,
+                                   material=material))
+
     @property
     def n_vertices(self):
         return len(self.rest)
@@ -148,13 +159,19 @@ class Scene:
                 if key in o:
                     for c in range(3):
                         getattr(ob, key)[c] = float(o[key][c])
-            for key in ("radius", "angular_speed", "rotation_start_time", "threshold"):
+            for key in ("radius", "angular_speed", "rotation_start_time", "threshold", "frame_interval"):
                 if key in o:
                     setattr(ob, key, float(o[key]))
             if o["type"] == abi.PDF_OBSTACLE_MESH:
                 ob.n_vertices = len(o["vertices"])
                 ob.n_triangles = len(o["triangles"])
                 ob.vertices = dptr(o["vertices"])
+                ob.triangles = iptr(o["triangles"])
+            elif o["type"] == abi.PDF_OBSTACLE_MOVING_MESH:
+                ob.n_frames = o["frames"].shape[0]
+                ob.n_vertices = o["frames"].shape[1]
+                ob.n_triangles = len(o["triangles"])
+                ob.vertices = dptr(o["frames"])
                 ob.triangles = iptr(o["triangles"])
         self._keep.append(obs)
         d.n_obstacles = len(self.obstacles)

@@ -42,8 +42,9 @@ enum pdf_obstacle_type {
   PDF_OBSTACLE_ROTATING_SPHERE = 1, /* RotatingSphere (src/physics/RotatingSphere.cpp:71-93) */
   PDF_OBSTACLE_PLANE = 2,           /* StaticPlane    (src/physics/StaticPlane.cpp:57-73)    */
   PDF_OBSTACLE_MESH = 3,            /* StaticMesh     (src/physics/StaticMesh.cpp:33-56)     */
-  PDF_OBSTACLE_BOX = 4              /* StaticAxisAlignedBox
+  PDF_OBSTACLE_BOX = 4,             /* StaticAxisAlignedBox
                                        (src/physics/StaticAxisAlignedBox.cpp:41-201) */
+  PDF_OBSTACLE_MOVING_MESH = 5      /* MovingMesh     (src/physics/MovingMesh.cpp:28-264) */
 };
 
 typedef struct pdf_obstacle {
@@ -56,16 +57,23 @@ typedef struct pdf_obstacle {
   double rotation_start_time;   /* rotating sphere: "Rotation Start Time" (s) */
   double point[3];              /* plane: "Point"                             */
   double normal[3];             /* plane: "Normal"                            */
-  int32_t n_vertices;           /* mesh obstacle: vertex count                */
+  int32_t n_vertices;           /* mesh obstacle: vertex count (of one key
+                                   frame for a moving mesh)                   */
   int32_t n_triangles;          /* mesh obstacle: triangle count              */
-  const double* vertices;       /* mesh obstacle: 3*n_vertices doubles        */
+  const double* vertices;       /* mesh obstacle: 3*n_vertices doubles; moving
+                                   mesh: n_frames key frames one after the
+                                   other, 3*n_vertices*n_frames doubles       */
   const int32_t* triangles;     /* mesh obstacle: 3*n_triangles indices       */
-  double threshold;             /* mesh obstacle: "Threshold"                 */
+  double threshold;             /* mesh obstacle: "Threshold"; moving mesh:
+                                   "Collision tolerance"                      */
   int32_t mesh;                 /* -1: acts on every dynamic mesh (the
                                    reference's behaviour); >= 0: only on that
                                    mesh (batches of independent cloths)       */
   double size[3];               /* box: "Size"; its "Position" (the corner
                                    with the smallest coordinates) is center  */
+  int32_t n_frames;             /* moving mesh: "Number Frame" (>= 2)         */
+  double frame_interval;        /* moving mesh: "Time Between Frame" (s); key
+                                   frame f is reached at time f*interval      */
 } pdf_obstacle;
 
 /* ---- dynamic meshes (include/physics/PhysicMesh.hpp, PhysicParameters) -- */

@@ -585,6 +585,14 @@ struct Obstacle {
   double threshold;
   int mesh; /* -1: every dynamic mesh; else only vertices of that mesh */
   V3 size;  /* box: extents; center = the corner with the smallest coordinates */
+  /* moving mesh (MovingMesh.cpp:28-41): every key frame, the clock, the index
+   * of the next key frame; mverts is the current (interpolated) mesh */
+  std::vector<std::vector<V3>> frames;
+  double interval = 0., clock = 0.;
+  int next = 1;
+  double frame_time(int f) const { return (double)f * interval; }
+  /* MovingMesh::isInMovement MovingMesh.cpp:253-257 */
+  bool in_movement() const { return clock >= frame_time(next - 1) && clock <= frame_time(next); }
 };
 
 struct CInfo {
@@ -877,8 +885,9 @@ static void detect_obstacles(Sim& s) {
         c.speed = {0, 0, 0};
         found.push_back(c);
       }
-    } else if (ob.type == PDF_OBSTACLE_MESH) {
-      /* StaticMesh::checkCollision StaticMesh.cpp:33-48 -> checkMeshCollision
+    } else if (ob.type == PDF_OBSTACLE_MESH || ob.type == PDF_OBSTACLE_MOVING_MESH) {
+      /* StaticMesh::checkCollision StaticMesh.cpp:33-48 and
+       * MovingMesh::checkCollision MovingMesh.cpp:164-192 -> checkMeshCollision
        * (vector form) geometry_util.cpp:32-92 */
       double tol = std::sqrt(ob.threshold * ob.threshold);
       std::vector<std::vector<Hit>> hits;
@@ -886,7 +895,7 @@ static void detect_obstacles(Sim& s) {
       double tol_sq = tol * tol;
       for (int i = 0; i < N; ++i) {
         double best = INFINITY;
-        V3 bp{0, 0, 0};
+        V3 bp{0, 0, 0}, bw{0, 0, 0};
         int bt = -1;
         for (const Hit& h : hits[i]) {
           const auto& t = ob.mtris[h.tri];
@@ -895,6 +904,7 @@ static void detect_obstacles(Sim& s) {
           if (d2 < best) {
             best = d2;
             bp = p;
+            bw = h.bary;
             bt = h.tri;
           }
         }
@@ -906,6 +916,17 @@ static void detect_obstacles(Sim& s) {
           c.normal = normalized(cross(ob.mverts[t[1]] - ob.mverts[t[0]], ob.mverts[t[2]] - ob.mverts[t[0]]));
           c.gap = dot(verts[i] - bp, c.normal);
           c.speed = {0, 0, 0};
+          if (ob.type == PDF_OBSTACLE_MOVING_MESH && ob.in_movement()) {
+            /* MovingMesh::getPointSpeed MovingMesh.cpp:232-249: the contact's
+             * barycentric point on the two key frames around the clock */
+            const std::vector<V3>& fp = ob.frames[ob.next - 1];
+            const std::vector<V3>& fn = ob.frames[ob.next];
+            const V3 pn = tri_point(fn[t[0]], fn[t[1]], fn[t[2]], bw);
+            const V3 pp = tri_point(fp[t[0]], fp[t[1]], fp[t[2]], bw);
+            const double span = ob.frame_time(ob.next) - ob.frame_time(ob.next - 1);
+            const V3 dp = pn - pp;
+            c.speed = {dp.x / span, dp.y / span, dp.z / span};
+          }
           found.push_back(c);
         }
       }
@@ -1292,8 +1313,22 @@ static void step(Sim& s) {
   /* SFE::updateScene SFE:64-87 */
   s.q = s.qnext;
   s.v = s.vnext;
-  for (auto& ob : s.obstacles)
+  for (auto& ob : s.obstacles) {
     if (ob.type == PDF_OBSTACLE_ROTATING_SPHERE) ob.time_before_start -= dt;
+    if (ob.type == PDF_OBSTACLE_MOVING_MESH) {
+      /* MovingMesh::update MovingMesh.cpp:43-84: advance the clock, at most
+       * one key frame, then interpolate the current mesh while in movement */
+      ob.clock += dt;
+      if (ob.frame_time(ob.next) < ob.clock && ob.next + 1 < (int)ob.frames.size()) ob.next += 1;
+      if (ob.in_movement()) {
+        const double t0 = ob.frame_time(ob.next - 1), t1 = ob.frame_time(ob.next);
+        const double a = (ob.clock - t0) / (t1 - t0);
+        const std::vector<V3>& fp = ob.frames[ob.next - 1];
+        const std::vector<V3>& fn = ob.frames[ob.next];
+        for (size_t k = 0; k < ob.mverts.size(); ++k) ob.mverts[k] = fp[k] * (1 - a) + fn[k] * a;
+      }
+    }
+  }
   if (self) {
     s.cur = 0;
     s.nxt = 1;
@@ -1492,11 +1527,27 @@ static void build(Sim& s, const pdf_scene_desc* sc, const pdf_params* p) {
     ob.mesh = o.mesh;
     ob.size = {o.size[0], o.size[1], o.size[2]};
     if (ob.mesh >= sc->n_meshes) throw std::invalid_argument("obstacle mesh out of range");
-    if (o.type == PDF_OBSTACLE_MESH) {
+    if (o.type == PDF_OBSTACLE_MESH || o.type == PDF_OBSTACLE_MOVING_MESH) {
+      if (o.n_vertices <= 0 || o.n_triangles <= 0 || !o.vertices || !o.triangles)
+        throw std::invalid_argument("mesh obstacle without geometry");
       for (int i = 0; i < o.n_vertices; ++i) ob.mverts.push_back(ld(o.vertices, i));
-      for (int t = 0; t < o.n_triangles; ++t)
+      for (int t = 0; t < o.n_triangles; ++t) {
         ob.mtris.push_back({o.triangles[3 * t], o.triangles[3 * t + 1], o.triangles[3 * t + 2]});
-    } else if (o.type < 0 || o.type > 4) {
+        for (int c = 0; c < 3; ++c)
+          if (o.triangles[3 * t + c] < 0 || o.triangles[3 * t + c] >= o.n_vertices)
+            throw std::invalid_argument("mesh obstacle index out of range");
+      }
+      if (o.type == PDF_OBSTACLE_MOVING_MESH) {
+        if (o.n_frames < 2 || !(o.frame_interval > 0.))
+          throw std::invalid_argument("moving mesh needs at least two key frames and a positive interval");
+        ob.interval = o.frame_interval;
+        for (int f = 0; f < o.n_frames; ++f) {
+          std::vector<V3> fr;
+          for (int i = 0; i < o.n_vertices; ++i) fr.push_back(ld(o.vertices, (size_t)f * o.n_vertices + i));
+          ob.frames.push_back(std::move(fr));
+        }
+      }
+    } else if (o.type < 0 || o.type > 5) {
       throw std::invalid_argument("unknown obstacle type");
     }
     s.obstacles.push_back(ob);
