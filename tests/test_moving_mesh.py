@@ -191,7 +191,10 @@ def test_moving_mesh_steps_match_oracle():
         cg, co = g.contacts(), o.contacts()
         assert np.array_equal(cg["vertex"], co["vertex"])
         assert np.array_equal(cg["normal"], co["normal"])
-        assert np.allclose(cg["speed"], co["speed"], rtol=0, atol=1e-15)
+        # the speed is (next - previous key-frame point) / interval: positions
+        # that agree to rounding give barycentric weights that agree to
+        # rounding, and the frame difference amplifies that by |p| / interval
+        assert np.allclose(cg["speed"], co["speed"], rtol=0, atol=1e-12)
         moved |= bool(np.abs(co["speed"]).max() > 0)
     assert moved and rg.n_contacts > 0
     qg, vg = g.state()
