@@ -86,7 +86,16 @@ class pdf_params(C.Structure):
         ("refine_tolerance", C.c_double), ("device", C.c_int32),
         ("contact_capacity", C.c_int32), ("use_graph", C.c_int32),
         ("mlp_weights", C.c_char * 256),
+        ("trace_alart_curnier", C.c_int32),
     ]
+
+
+PDF_LOG_POSITION = 0
+PDF_LOG_VELOCITY = 1
+
+
+class pdf_log_entry(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n_vertices", C.c_int32), ("vertices", _ip)]
 
 
 class pdf_step_report(C.Structure):
@@ -127,7 +136,8 @@ class pdf_contact(C.Structure):
 def params(time_step=5e-3, iterations=20, self_collision=False, self_tol=0.0,
            gravity=(0.0, 0.0, -9.81), air_damping=0.0, precision=PDF_FP64,
            residual_tolerance=0.0, warm_start=PDF_WARM_NONE, refine_max=4,
-           refine_tolerance=1e-10, device=0, contact_capacity=0, use_graph=1, mlp_weights=""):
+           refine_tolerance=1e-10, device=0, contact_capacity=0, use_graph=1, mlp_weights="",
+           trace_alart_curnier=0):
     """Build a pdf_params with the reference's meaning for each field."""
     p = pdf_params()
     p.time_step = time_step
@@ -146,6 +156,7 @@ def params(time_step=5e-3, iterations=20, self_collision=False, self_tol=0.0,
     p.contact_capacity = contact_capacity
     p.use_graph = use_graph
     p.mlp_weights = mlp_weights.encode() if isinstance(mlp_weights, str) else bytes(mlp_weights)
+    p.trace_alart_curnier = trace_alart_curnier
     return p
 
 

@@ -11,6 +11,8 @@
 #include <thrust/iterator/counting_iterator.h>
 #include <fstream>
 #include <ios>
+#include <limits>
+#include <ostream>
 #include <random>
 #include <stdexcept>
 #include <string>
@@ -56,6 +58,7 @@ constexpr int kStrideBlocks = 592;  // 4 x 148 SMs for grid-stride kernels
 // Work items of one sweep are at most 32 x chunk elements; the chunk is
 // chosen per scene by the autotuner in create_impl among these.
 constexpr int kChunk = 64;  // host emulation check (pdf_factor_check)
+constexpr int kRecords = 64;  // step records in flight before the oldest is harvested
 constexpr int kChunkCandidates[3] = {32, 64, 128};
 
 // Work-item lists of the two sweeps in elimination-tree order (forward:
@@ -93,6 +96,7 @@ void build_schedule(pdf_handle* h, int chunk) {
   CK(cudaMemset(sy.fchild, 0, f.n_sn * sizeof(unsigned long long)));
   CK(cudaMemset(sy.bdone, 0, f.n_sn * sizeof(unsigned long long)));
   CK(cudaMemset(sy.err, 0, sizeof(int)));
+  sy.trace = DTrace{h->d.iter, h->d.stamps, std::max(1, h->prm.local_global_iterations)};
 }
 
 void autotune_schedule(pdf_handle* h);
@@ -164,7 +168,9 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   h->prm = *p;
   h->fp32 = p->precision == PDF_FP32_REFINE;
   if (p->precision != PDF_FP64 && p->precision != PDF_FP32_REFINE) throw std::invalid_argument("unknown precision mode");
+  const auto tl = std::chrono::steady_clock::now();
   build_model(*sc, *p, h->model);
+  h->lhs_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tl).count();
   const Model& m = h->model;
   std::string ferr;
   if (!factorize(m, p->time_step, 40, h->fac, ferr)) throw std::range_error(ferr);
@@ -321,6 +327,11 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   c.cap = h->cap_contacts;
   c.slot_cap = N;
   c.self_cap = h->cap_self;
+  if (p->trace_alart_curnier) {
+    c.trace_stride = c.cap + c.self_cap;
+    c.trace_k = std::max(1, p->local_global_iterations);
+    c.ac_trace = dalloc<double>(2 * (size_t)c.trace_stride * c.trace_k);
+  }
   c.n_contacts = dalloc<int>(1);
   c.n_self = dalloc<int>(1);
   c.n_levels = dalloc<int>(1);
@@ -374,6 +385,28 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   CK(cudaMemset(d.iter, 0, sizeof(int)));
   CK(cudaMemset(d.iter_total, 0, sizeof(long long)));
   CK(cudaMemset(d.blocks_done, 0, sizeof(unsigned int)));
+  // iteration clock and the step records that carry it to the host
+  {
+    const int K = std::max(1, p->local_global_iterations);
+    const size_t nst = (size_t)DTrace::kRows * K;
+    d.stamps = dalloc<unsigned long long>(nst);
+    CK(cudaMemset(d.stamps, 0, nst * sizeof(unsigned long long)));
+    h->dm.trace = DTrace{d.iter, d.stamps, K};
+    h->d.sync.trace = h->dm.trace;
+    const size_t per = 64 + nst * sizeof(unsigned long long);  // counts padded to 64 bytes
+    h->ring.resize(kRecords);
+    CK(cudaHostAlloc(&h->ring_host, per * kRecords, cudaHostAllocMapped));
+    std::memset(h->ring_host, 0, per * kRecords);
+    for (int r = 0; r < kRecords; ++r) {
+      StepRecord& rec = h->ring[r];
+      char* base = static_cast<char*>(h->ring_host) + per * r;
+      rec.counts = reinterpret_cast<int*>(base);
+      rec.stamps = reinterpret_cast<unsigned long long*>(base + 64);
+      CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&rec.counts_dev), rec.counts, 0));
+      CK(cudaHostGetDevicePointer(reinterpret_cast<void**>(&rec.stamps_dev), rec.stamps, 0));
+      for (auto& e : rec.ev) CK(cudaEventCreate(&e));
+    }
+  }
   if (h->obs.n > 0) {
     const int nitems = h->obs.n * N;
     d.flags = dalloc<unsigned char>(nitems);
@@ -505,7 +538,7 @@ void launch_iteration(pdf_handle* h, T* b, T* y, T* x, const T* Wf, const T* Wb,
   if (self_mode) launch_friction_self<T>(1, 1024, st, dm, d.c, b, d.newf, d.iter);
   launch_solve<T>(h, b, y, x, Wf, Wb, mode);
   IterCtl ctl{d.iter, d.iter_total, d.blocks_done, h->prm.residual_tolerance, h->prm.local_global_iterations,
-              h->capturing_cond ? 1 : 0, h->cond};
+              h->capturing_cond ? 1 : 0, h->cond, h->dm.trace};
   k_alart_curnier<<<kStrideBlocks, kThreads, 0, st>>>(d.c, d.v, d.ac_hist, ctl);
 }
 
@@ -562,6 +595,64 @@ void build_tolerance_graph(pdf_handle* h) {
   CK(cudaGraphDestroy(g));
 }
 
+// Reads one finished step record into the per-sample statistics and the
+// cumulative phase times (the reference's timers: SimulationBase.cpp:103-173,
+// 333-405; SFE:135-151, 307-426, 430-572).
+void harvest_record(pdf_handle* h, StepRecord& rec) {
+  CK(cudaEventSynchronize(rec.ev[6]));
+  float e[7] = {0.f};
+  for (int k = 1; k < 7; ++k) CK(cudaEventElapsedTime(&e[k], rec.ev[0], rec.ev[k]));
+  const bool self = h->prm.self_collision != 0;
+  const int C = rec.counts[0], S = rec.counts[1], iters = rec.counts[3];
+  const int K = std::max(1, h->prm.local_global_iterations);
+  StatSamples& sm = h->samples;
+  pdf_stats& st = h->stats;
+  sm.detection.push_back(1e3 * e[1]);
+  st.detection_ms += e[1];
+  if (C > 0) sm.collisions.push_back(C);
+  if (self) {
+    sm.self_detection.push_back(1e3 * (e[2] - e[1]));
+    st.self_detection_ms += e[2] - e[1];
+    if (S > 0) {
+      sm.self_collisions.push_back(S);
+      sm.ordering.push_back(1e3 * (e[3] - e[2]));
+      st.ordering_ms += e[3] - e[2];
+    }
+  }
+  st.solve_ms += e[5] - e[4];
+  st.step_ms += e[6];
+  sm.step.push_back(1e3 * e[6]);
+  const unsigned long long* t = rec.stamps;
+  auto us = [](unsigned long long a, unsigned long long b) { return b >= a ? 1e-3 * (double)(b - a) : 0.; };
+  for (int k = 0; k < std::min(iters, K); ++k) {
+    const unsigned long long t0 = t[DTrace::kLocal * K + k], tf = t[DTrace::kFriction * K + k],
+                             ts = t[DTrace::kSelfFriction * K + k], tv = t[DTrace::kSolve * K + k],
+                             ta = t[DTrace::kAcBegin * K + k], te = t[DTrace::kAcEnd * K + k];
+    sm.iteration.push_back(us(t0, te));
+    sm.rhs.push_back(us(t0, tv));
+    sm.solver.push_back(us(tv, ta));
+    sm.rhs_base.push_back(us(t0, tf));
+    st.rhs_ms += 1e-3 * us(t0, tf);
+    if (C + S > 0) {
+      sm.friction.push_back(us(tf, self ? ts : tv));
+      st.friction_ms += 1e-3 * us(tf, self ? ts : tv);
+    }
+    if (self && S > 0) {
+      sm.self_friction.push_back(us(ts, tv));
+      st.self_friction_ms += 1e-3 * us(ts, tv);
+    }
+  }
+  rec.pending = false;
+}
+
+// Harvests every pending record, oldest first.
+void harvest_all(pdf_handle* h) {
+  for (int k = 0; k < kRecords; ++k) {
+    StepRecord& rec = h->ring[(h->ring_head + k) % kRecords];
+    if (rec.pending) harvest_record(h, rec);
+  }
+}
+
 void step_once(pdf_handle* h, bool want_report) {
   DeviceBuffers& d = h->d;
   const DModel& dm = h->dm;
@@ -569,7 +660,9 @@ void step_once(pdf_handle* h, bool want_report) {
   const double dt = h->prm.time_step;
   const int N = dm.N;
   const int K = h->prm.local_global_iterations;
-  CK(cudaEventRecord(h->ev[0], st));
+  StepRecord& rec = h->ring[h->ring_head];
+  if (rec.pending) harvest_record(h, rec);
+  CK(cudaEventRecord(rec.ev[0], st));
   k_step_init<<<blocks_for(N), kThreads, 0, st>>>(dm, d.q, d.v, d.tn, d.qk, d.cstep, h->prm.gravity[0],
                                                   h->prm.gravity[1], h->prm.gravity[2], dt);
   // obstacle detection on the start-of-step positions (SimulationBase.cpp:333-366)
@@ -596,7 +689,7 @@ void step_once(pdf_handle* h, bool want_report) {
   } else {
     CK(cudaMemsetAsync(d.c.n_contacts, 0, sizeof(int), st));
   }
-  CK(cudaEventRecord(h->ev[1], st));
+  CK(cudaEventRecord(rec.ev[1], st));
   if (h->prm.self_collision) {
     int sst = self_detect_step(h);
     if (sst != PDF_OK) throw std::overflow_error(h->err);
@@ -604,10 +697,12 @@ void step_once(pdf_handle* h, bool want_report) {
     CK(cudaMemsetAsync(d.c.n_self, 0, sizeof(int), st));
     CK(cudaMemsetAsync(d.c.n_levels, 0, sizeof(int), st));
   }
+  CK(cudaEventRecord(rec.ev[2], st));
   // compact slots of every vertex touched by a contact (force buffers of SFE:45-60)
   k_contact_slots<<<kStrideBlocks, kThreads, 0, st>>>(d.c);
   k_contact_slots_fill<<<kStrideBlocks, kThreads, 0, st>>>(d.c);
   if (h->prm.self_collision) self_levels_step(h);
+  CK(cudaEventRecord(rec.ev[3], st));
   // learned warm start: features of every obstacle contact, predicted forces
   const bool warm = h->prm.warm_start == PDF_WARM_MLP;
   const bool mlp_features = warm || h->log_cap > 0;
@@ -615,7 +710,7 @@ void step_once(pdf_handle* h, bool want_report) {
     launch_mlp_features(st, d.c, d.tn, d.mass, h->rprev, h->rprev_tag, h->mlp_tag - 1, h->prm.gravity, dt, h->mlp_X);
     if (warm) mlp_forward_counted(h->mlp_w, h->mlp_X, d.c.n_contacts, h->cap_contacts, h->mlp_Y, st);
   }
-  CK(cudaEventRecord(h->ev[2], st));
+  CK(cudaEventRecord(rec.ev[4], st));
   CK(cudaMemsetAsync(d.ac_hist, 0, 4 * (size_t)K * sizeof(double), st));
   CK(cudaMemsetAsync(d.iter, 0, sizeof(int), st));
   // iterations
@@ -658,7 +753,7 @@ void step_once(pdf_handle* h, bool want_report) {
     launch_iterations(h, K);
     iters = K;
   }
-  CK(cudaEventRecord(h->ev[3], st));
+  CK(cudaEventRecord(rec.ev[5], st));
   if (mlp_features) {
     const bool log = h->log_cap > 0;
     launch_mlp_record(st, d.c, d.mass, h->rprev, h->rprev_tag, h->mlp_tag, h->prm.gravity, dt, h->mlp_X,
@@ -667,8 +762,17 @@ void step_once(pdf_handle* h, bool want_report) {
   h->mlp_tag += 1;
   k_contact_slots_reset<<<kStrideBlocks, kThreads, 0, st>>>(d.c);
   CK(cudaMemsetAsync(d.c.n_slots, 0, sizeof(int), st));
-  k_finalize<<<blocks_for(3 * (int64_t)N), kThreads, 0, st>>>(3 * N, d.qk, d.q);
-  CK(cudaEventRecord(h->ev[4], st));
+  // a frame copy of q still in flight must end before q is overwritten
+  if (h->frame_guard >= 0) {
+    CK(cudaStreamWaitEvent(st, h->frame_ev[h->frame_guard], 0));
+    h->frame_guard = -1;
+  }
+  const StepOut out{d.c.n_contacts, d.c.n_self, d.c.n_levels, d.iter, d.stamps,
+                    DTrace::kRows * std::max(1, K), rec.counts_dev, rec.stamps_dev};
+  k_finalize<<<blocks_for(3 * (int64_t)N), kThreads, 0, st>>>(3 * N, d.qk, d.q, out);
+  CK(cudaEventRecord(rec.ev[6], st));
+  rec.pending = true;
+  h->ring_head = (h->ring_head + 1) % kRecords;
   CK(cudaGetLastError());
   // RotatingSphere::update (RotatingSphere.cpp:39-43)
   for (auto& t : h->host_time_before_start) t -= dt;
@@ -691,20 +795,9 @@ void step_once(pdf_handle* h, bool want_report) {
   h->launches_outside += launches_per_step_extra(h);
   if (want_report) {
     CK(cudaStreamSynchronize(st));
-    float a, b, cc, dd;
-    CK(cudaEventElapsedTime(&a, h->ev[0], h->ev[1]));
-    CK(cudaEventElapsedTime(&b, h->ev[1], h->ev[2]));
-    CK(cudaEventElapsedTime(&cc, h->ev[2], h->ev[3]));
-    CK(cudaEventElapsedTime(&dd, h->ev[0], h->ev[4]));
-    h->stats.detection_ms += a;
-    h->stats.self_detection_ms += b;
-    h->stats.solve_ms += cc;
-    h->stats.step_ms += dd;
-    int counts[3];
-    CK(cudaMemcpy(&counts[0], d.c.n_contacts, sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&counts[1], d.c.n_self, sizeof(int), cudaMemcpyDeviceToHost));
-    CK(cudaMemcpy(&counts[2], d.c.n_levels, sizeof(int), cudaMemcpyDeviceToHost));
-    if (iters < 0) CK(cudaMemcpy(&iters, d.iter, sizeof(int), cudaMemcpyDeviceToHost));
+    harvest_all(h);
+    const int counts[3] = {rec.counts[0], rec.counts[1], rec.counts[2]};
+    if (iters < 0) iters = rec.counts[3];
     std::vector<double> hist(4 * (size_t)K);
     CK(cudaMemcpy(hist.data(), d.ac_hist, hist.size() * sizeof(double), cudaMemcpyDeviceToHost));
     const int nc = counts[0] + counts[1];
@@ -772,13 +865,24 @@ void free_handle(pdf_handle* h) {
                   d.c.s_ac, d.c.s_slota, d.c.s_slotb, d.c.s_remember, d.c.n_levels, d.c.level_ptr,
                   d.c.level_order, d.c.slot_of, d.c.n_slots, d.c.slot_vertex, d.c.f, d.c.cf[0], d.c.cf[1],
                   d.c.sf[0], d.c.sf[1], d.c.c_gap, d.c.c_active, h->mlp_w, h->mlp_X, h->mlp_Y, h->rprev,
-                  h->rprev_tag, h->log_X, h->log_T, h->log_n, d.iter, d.iter_total, d.blocks_done};
+                  h->rprev_tag, h->log_X, h->log_T, h->log_n, d.iter, d.iter_total, d.blocks_done, d.stamps,
+                  d.c.ac_trace, h->gather_idx, h->gather_out};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto p : d.obstacle_v) cudaFree(p);
   for (auto p : d.obstacle_t) cudaFree(p);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);
+  for (StepRecord& rec : h->ring)
+    for (auto& e : rec.ev)
+      if (e) cudaEventDestroy(e);
+  if (h->ring_host) cudaFreeHost(h->ring_host);
+  for (int k = 0; k < 2; ++k) {
+    if (h->frame_host[k]) cudaFreeHost(h->frame_host[k]);
+    if (h->frame_ev[k]) cudaEventDestroy(h->frame_ev[k]);
+  }
+  if (h->frame_ready) cudaEventDestroy(h->frame_ready);
+  if (h->copy_stream) cudaStreamDestroy(h->copy_stream);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -848,6 +952,7 @@ int pdf_step(pdf_handle* h, int32_t nsteps, pdf_step_report* report) {
     for (int s = 0; s < nsteps; ++s) step_once(h, (s == nsteps - 1) || h->prm.self_collision);
     CK(cudaEventRecord(h->ev[6], h->stream));
     CK(cudaStreamSynchronize(h->stream));
+    harvest_all(h);
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]));
     h->last.device_ms = ms;
@@ -972,6 +1077,7 @@ int pdf_set_state(pdf_handle* h, const double* q, const double* v) {
       if ((q && !std::isfinite(q[i])) || (v && !std::isfinite(v[i])))
         return fail(h, PDF_NAN_DETECTED, "non-finite value in the state passed to pdf_set_state");
     CK(cudaStreamSynchronize(h->stream));
+    if (h->copy_stream) CK(cudaStreamSynchronize(h->copy_stream));
     if (q) CK(cudaMemcpy(h->d.q, q, n3 * sizeof(double), cudaMemcpyHostToDevice));
     if (v) CK(cudaMemcpy(h->d.v, v, n3 * sizeof(double), cudaMemcpyHostToDevice));
     h->mlp_tag += 2;  // the previous step's contact impulses no longer apply
@@ -1071,26 +1177,165 @@ int pdf_get_stats(pdf_handle* h, pdf_stats* out) {
   });
 }
 
+}  // extern "C"
+
+namespace {
+// computeAndWriteStats (template/physics/io.tpp:23-63): a title line, then
+// "(No data)", " Value : x" for one sample, or the number, minimum, mean and
+// maximum of the samples (default stream formatting), then a dashed separator.
+// Counts are integers: their mean is truncated like the reference's
+// conversion of the double mean to the element type.
+template <typename T>
+void write_stats_section(std::ostream& of, const char* name, const std::vector<T>& v) {
+  of << name << std::endl;
+  if (v.empty()) {
+    of << "\t(No data)" << std::endl;
+  } else if (v.size() == 1) {
+    of << "\t Value : " << v[0] << std::endl;
+  } else {
+    double mn = std::numeric_limits<double>::max(), mx = std::numeric_limits<double>::min(), sum = 0.;
+    for (const T& x : v) {
+      mn = std::min(mn, (double)x);
+      mx = std::max(mx, (double)x);
+      sum += (double)x;
+    }
+    of << "\t Number      : " << v.size() << std::endl
+       << "\t Min value   : " << (T)mn << std::endl
+       << "\t Mean value  : " << (T)(sum / (double)v.size()) << std::endl
+       << "\t Max value   : " << (T)mx << std::endl;
+  }
+  of << std::endl << "-------------------" << std::endl << std::endl;
+}
+}  // namespace
+
+extern "C" {
+
 int pdf_export_stats(pdf_handle* h, const char* path) {
   if (!h || !path) return fail(h, PDF_INVALID_ARG, "null argument");
   std::ofstream of(path);
   if (!of) return fail(h, PDF_IO_ERROR, std::string("cannot open ") + path);
-  const pdf_stats& s = h->stats;
-  auto section = [&](const char* name, double value, int64_t number) {
-    of << name << "\n";
-    if (number == 0)
-      of << "\t(No data)\n";
-    else
-      of << "\t Number      : " << number << "\n\t Mean value  : " << value / (double)number << "\n";
-    of << "\n-------------------\n\n";
-  };
-  of << "LHS computation time (µs)\n\t Value : " << 1e3 * (s.setup_ms - s.factor_ms) << "\n\n-------------------\n\n";
-  of << "Cholesky computation time (µs)\n\t Value : " << 1e3 * s.factor_ms << "\n\n-------------------\n\n";
-  section("Collision detection time (µs)", 1e3 * s.detection_ms, s.steps);
-  section("Self collision detection time (µs)", 1e3 * s.self_detection_ms, s.steps);
-  section("Iteration time (µs)", 1e3 * s.solve_ms, s.iterations);
-  section("Step time (µs)", 1e3 * s.step_ms, s.steps);
-  return PDF_OK;
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    CK(cudaStreamSynchronize(h->stream));
+    harvest_all(h);
+    const StatSamples& sm = h->samples;
+    const bool self = h->prm.self_collision != 0;
+    // SimulationFrictionEstimation::exportStats (SFE:756-771) around
+    // SimulationBase::exportStats (SimulationBase.cpp:474-494)
+    write_stats_section(of, "LHS computation time (µs)", std::vector<double>{1e3 * h->lhs_ms});
+    write_stats_section(of, "Cholesky computation time (µs)", std::vector<double>{1e3 * h->stats.factor_ms});
+    write_stats_section(of, "Iteration time (µs)", sm.iteration);
+    write_stats_section(of, "Collision detection time (µs)", sm.detection);
+    if (self) {
+      write_stats_section(of, "Number of collisions", sm.collisions);
+      write_stats_section(of, "Self collision detection time (µs)", sm.self_detection);
+    }
+    write_stats_section(of, "Number of self collisions", sm.self_collisions);
+    write_stats_section(of, "Solver time (µs)", sm.solver);
+    write_stats_section(of, "Full RHS computation time (µs)", sm.rhs);
+    write_stats_section(of, "Step time (µs)", sm.step);
+    write_stats_section(of, "RHS base computation time (µs)", sm.rhs_base);
+    write_stats_section(of, "RHS friction overhead (µs)", sm.friction);
+    if (self) {
+      write_stats_section(of, "Self collision time (µs)", sm.self_friction);
+      write_stats_section(of, "Self collision ordering time (µs)", sm.ordering);
+    }
+    if (!of) return fail(h, PDF_IO_ERROR, std::string("cannot write ") + path);
+    return PDF_OK;
+  });
+}
+
+int pdf_frame_capture(pdf_handle* h, int32_t slot) {
+  if (!h || slot < 0 || slot > 1) return fail(h, PDF_INVALID_ARG, "invalid handle or frame slot");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    const size_t bytes = 3 * (size_t)h->dm.N * sizeof(double);
+    if (!h->copy_stream) {
+      CK(cudaStreamCreateWithFlags(&h->copy_stream, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&h->frame_ready, cudaEventDisableTiming));
+      for (int k = 0; k < 2; ++k) {
+        CK(cudaHostAlloc(reinterpret_cast<void**>(&h->frame_host[k]), bytes, cudaHostAllocDefault));
+        CK(cudaEventCreateWithFlags(&h->frame_ev[k], cudaEventDisableTiming));
+      }
+    }
+    // the slot's previous copy has been waited for by the caller or is
+    // ordered before this one on the copy stream
+    CK(cudaEventRecord(h->frame_ready, h->stream));
+    CK(cudaStreamWaitEvent(h->copy_stream, h->frame_ready, 0));
+    CK(cudaMemcpyAsync(h->frame_host[slot], h->d.q, bytes, cudaMemcpyDeviceToHost, h->copy_stream));
+    CK(cudaEventRecord(h->frame_ev[slot], h->copy_stream));
+    h->frame_guard = slot;
+    return PDF_OK;
+  });
+}
+
+int pdf_frame_wait(pdf_handle* h, int32_t slot, const double** q) {
+  if (!h || slot < 0 || slot > 1 || !q) return fail(h, PDF_INVALID_ARG, "invalid handle, frame slot or output");
+  if (!h->frame_host[slot]) return fail(h, PDF_INVALID_ARG, "frame slot never captured");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    CK(cudaEventSynchronize(h->frame_ev[slot]));
+    *q = h->frame_host[slot];
+    return PDF_OK;
+  });
+}
+
+int pdf_get_vertices(pdf_handle* h, const int32_t* vertices, int32_t n, double* q, double* v) {
+  if (!h || n < 0 || (n > 0 && !vertices)) return fail(h, PDF_INVALID_ARG, "invalid vertex list");
+  for (int k = 0; k < n; ++k)
+    if (vertices[k] < 0 || vertices[k] >= h->dm.N) return fail(h, PDF_INVALID_ARG, "vertex index out of range");
+  if (n == 0) return PDF_OK;
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    cudaStream_t st = h->stream;
+    if (n > h->gather_cap) {
+      if (h->gather_idx) CK(cudaFree(h->gather_idx));
+      if (h->gather_out) CK(cudaFree(h->gather_out));
+      h->gather_idx = nullptr;
+      h->gather_out = nullptr;
+      h->gather_idx = dalloc<int>(n);
+      h->gather_out = dalloc<double>(6 * (size_t)n);
+      h->gather_cap = n;
+    }
+    CK(cudaMemcpyAsync(h->gather_idx, vertices, n * sizeof(int), cudaMemcpyHostToDevice, st));
+    k_gather_vertices<<<(n + kThreads - 1) / kThreads, kThreads, 0, st>>>(n, h->gather_idx, h->d.q, h->d.v,
+                                                                          h->gather_out);
+    CK(cudaGetLastError());
+    h->launches_outside += 1;
+    std::vector<double> out(6 * (size_t)n);
+    CK(cudaMemcpyAsync(out.data(), h->gather_out, out.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (q) std::copy(out.begin(), out.begin() + 3 * (size_t)n, q);
+    if (v) std::copy(out.begin() + 3 * (size_t)n, out.end(), v);
+    return PDF_OK;
+  });
+}
+
+int pdf_get_alart_curnier_trace(pdf_handle* h, double* out, int64_t cap, int32_t* iterations, int32_t* n_contacts,
+                                int32_t* n_self) {
+  if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
+  if (!h->d.c.ac_trace) return fail(h, PDF_INVALID_ARG, "created without trace_alart_curnier");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    CK(cudaStreamSynchronize(h->stream));
+    int counts[3];
+    CK(cudaMemcpy(&counts[0], h->d.c.n_contacts, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&counts[1], h->d.c.n_self, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&counts[2], h->d.iter, sizeof(int), cudaMemcpyDeviceToHost));
+    const int C = std::min(counts[0], h->d.c.cap), S = std::min(counts[1], h->d.c.self_cap);
+    const int it = std::min(counts[2], h->d.c.trace_k);
+    if (iterations) *iterations = it;
+    if (n_contacts) *n_contacts = C;
+    if (n_self) *n_self = S;
+    const int64_t need = 2 * (int64_t)it * (C + S);
+    if (!out) return PDF_OK;
+    if (cap < need) return fail(h, PDF_CAPACITY_EXCEEDED, "trace buffer too small");
+    if (need == 0) return PDF_OK;
+    const size_t row = 2 * sizeof(double) * (size_t)(C + S);
+    CK(cudaMemcpy2D(out, row, h->d.c.ac_trace, 2 * sizeof(double) * (size_t)h->d.c.trace_stride, row, it,
+                    cudaMemcpyDeviceToHost));
+    return PDF_OK;
+  });
 }
 
 int pdf_get_residual_history(pdf_handle* h, double* out, int32_t cap, int32_t* n) {

@@ -5,6 +5,34 @@
 
 namespace pdfb {
 
+// Per-iteration device clock of the current step: the first thread of block 0
+// of a few kernels writes %globaltimer (ns) at entry, indexed by the PD
+// iteration the kernel belongs to.  Rows of stamps[kRows * k]: local step
+// start, obstacle friction entry, self friction entry, forward sweep entry,
+// Alart-Curnier entry, Alart-Curnier end (written by its last block).
+struct DTrace {
+  const int* iter;               // PD iterations completed in this step
+  unsigned long long* stamps;    // kRows * k, or null (no trace)
+  int k;                         // iteration capacity
+  static constexpr int kRows = 6;
+  enum Row { kLocal = 0, kFriction = 1, kSelfFriction = 2, kSolve = 3, kAcBegin = 4, kAcEnd = 5 };
+};
+
+#ifdef __CUDACC__
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// called by every thread; only thread 0 of block 0 writes
+__device__ __forceinline__ void trace_stamp(const DTrace& t, int row) {
+  if (t.stamps && blockIdx.x == 0 && threadIdx.x == 0) {
+    const int it = *t.iter;
+    if (it >= 0 && it < t.k) t.stamps[(int64_t)row * t.k + it] = global_ns();
+  }
+}
+#endif
+
 // Read-only model tables (original vertex order unless stated).
 struct DModel {
   int N, B;                 // vertices, bending rows
@@ -26,6 +54,7 @@ struct DModel {
   const double* ata_val;
   const int* perm;          // pivot position -> vertex
   const int* iperm;         // vertex -> pivot position
+  DTrace trace;             // iteration clock (local step and friction rows)
 };
 
 // Contacts of the current step (device-resident, counts on the device).
@@ -63,6 +92,11 @@ struct DContacts {
   double* cf[2];            // contact forces per slot (self mode)
   double* sf[2];            // self contact forces per slot
   int cap, slot_cap, self_cap;
+  // per-iteration Alart-Curnier norms (tangential, |normal|) of every
+  // contact, [iteration][contact][2] with contact stride trace_stride; null
+  // unless tracing is on
+  double* ac_trace;
+  int trace_stride, trace_k;
 };
 
 __device__ __forceinline__ double3 ld3(const double* p, int64_t i) {

@@ -51,6 +51,7 @@ struct DeviceBuffers {
   // device iteration control (IterCtl): iterations of the current step, of
   // the handle's lifetime, and the AC kernel's block-completion counter
   int* iter = nullptr;
+  unsigned long long* stamps = nullptr;  // DTrace::kRows * K iteration clock
   long long* iter_total = nullptr;
   unsigned int* blocks_done = nullptr;
   // self-collision detection scratch (selfdetect.cu)
@@ -69,6 +70,28 @@ struct MovingClock {
   double* cur = nullptr;
   double frame_time(int f) const { return (double)f * interval; }
   bool in_movement() const { return clock >= frame_time(next - 1) && clock <= frame_time(next); }
+};
+
+// One step's timing record: CUDA events around its phases, and the
+// host-mapped counters and iteration clock that k_finalize fills.  Events:
+// 0 step start, 1 after obstacle detection, 2 after self detection, 3 after
+// self-contact ordering, 4 iterations begin, 5 iterations end, 6 step end.
+struct StepRecord {
+  cudaEvent_t ev[7] = {};
+  int* counts = nullptr;                 // contacts, self contacts, levels, iterations
+  unsigned long long* stamps = nullptr;  // DTrace::kRows * K, ns
+  int* counts_dev = nullptr;             // device views of the same memory
+  unsigned long long* stamps_dev = nullptr;
+  bool pending = false;
+};
+
+// Per-sample statistics, in microseconds, of the reference's stats file
+// (SimulationBase::exportStats SimulationBase.cpp:474-494 and
+// SimulationFrictionEstimation::exportStats SFE:756-771).
+struct StatSamples {
+  std::vector<double> iteration, detection, self_detection, solver, rhs, step, rhs_base, friction, self_friction,
+      ordering;
+  std::vector<int64_t> collisions, self_collisions;
 };
 
 struct pdf_handle {
@@ -92,6 +115,24 @@ struct pdf_handle {
   pdf_stats stats{};
   std::vector<double> residual_hist;
   int64_t launches_outside = 0;  // kernels launched outside PD iterations so far
+  // step records, reused round-robin; a record is harvested (its events
+  // waited for) before reuse and at the end of every pdf_step call
+  std::vector<StepRecord> ring;
+  int ring_head = 0;
+  void* ring_host = nullptr;  // host-mapped memory of all records
+  StatSamples samples;
+  double lhs_ms = 0.;  // model and LHS assembly (host)
+  // frame output: two pinned copies of q filled on a copy stream; frame_guard
+  // is the slot whose copy the next write-back of q must wait for (-1: none)
+  double* frame_host[2] = {nullptr, nullptr};
+  cudaEvent_t frame_ev[2] = {nullptr, nullptr};
+  cudaEvent_t frame_ready = nullptr;
+  cudaStream_t copy_stream = nullptr;
+  int frame_guard = -1;
+  // log reads: device index list and gathered q, v
+  int* gather_idx = nullptr;
+  double* gather_out = nullptr;
+  int gather_cap = 0;
   // iterate-to-tolerance graph: the iterations are one conditional WHILE node
   cudaGraphConditionalHandle cond{};
   bool capturing_cond = false;

@@ -312,6 +312,12 @@ void read_obj(const std::string& path, std::vector<double>& pos, std::vector<int
 
 }  // namespace
 
+struct pdf_log {
+  std::vector<int> kinds;
+  std::vector<std::vector<int32_t>> vertices;
+  std::vector<pdf_log_entry> entries;
+};
+
 struct pdf_scene {
   std::vector<double> rest, pos;
   std::vector<int> tris;
@@ -547,5 +553,61 @@ int pdf_params_load_json(const char* json_path, pdf_params* out, int32_t* frame_
   }
   return PDF_OK;
 }
+
+int pdf_log_load_json(const char* json_path, pdf_log** out) {
+  if (!json_path || !out) return PDF_INVALID_ARG;
+  *out = nullptr;
+  try {
+    const JVal root = load_json(json_path);
+    if (root.kind != JVal::Object) throw std::invalid_argument("JSON reader - Error : root must be an object");
+    std::unique_ptr<pdf_log> lg(new pdf_log);
+    const JVal* la = root.find("log");
+    if (la) {
+      const JVal& arr = req_array(root, "log");
+      for (const JVal& lo : arr.a) {
+        // getLogTypeFromObject (log_building.cpp:73-87), STRING_TO_LOG_TYPE
+        const std::string& kind = req_string(lo, "type");
+        int k;
+        if (kind == "position")
+          k = PDF_LOG_POSITION;
+        else if (kind == "velocity")
+          k = PDF_LOG_VELOCITY;
+        else
+          throw std::invalid_argument("Log type \"" + kind + "\" is unsupported");
+        // getIndicesFromArray (log_building.cpp:120-129)
+        std::vector<int32_t> idx;
+        for (const JVal& x : req_array(lo, "vertices").a) {
+          if (x.kind != JVal::Int || x.i < 0 || x.i > 0x7fffffffLL) type_error("vertices");
+          idx.push_back((int32_t)x.i);
+        }
+        lg->kinds.push_back(k);
+        lg->vertices.push_back(std::move(idx));
+      }
+    }
+    lg->entries.resize(lg->kinds.size());
+    for (size_t e = 0; e < lg->kinds.size(); ++e) {
+      lg->entries[e].kind = lg->kinds[e];
+      lg->entries[e].n_vertices = (int32_t)lg->vertices[e].size();
+      lg->entries[e].vertices = lg->vertices[e].data();
+    }
+    *out = lg.release();
+  } catch (const std::ios_base::failure& e) {
+    g_load_error = e.what();
+    return PDF_IO_ERROR;
+  } catch (const std::exception& e) {
+    g_load_error = e.what();
+    return PDF_INVALID_ARG;
+  }
+  return PDF_OK;
+}
+
+int pdf_log_view(const pdf_log* lg, int32_t* n_entries, const pdf_log_entry** entries) {
+  if (!lg) return PDF_INVALID_ARG;
+  if (n_entries) *n_entries = (int32_t)lg->entries.size();
+  if (entries) *entries = lg->entries.data();
+  return PDF_OK;
+}
+
+void pdf_log_free(pdf_log* lg) { delete lg; }
 
 }  // extern "C"

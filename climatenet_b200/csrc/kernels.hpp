@@ -16,6 +16,7 @@ struct SweepSync {
   unsigned long long* fchild;  // per supernode: children whose forward finished
   unsigned long long* bdone;   // per supernode: backward work items finished
   int* err;                    // set when a dependency wait gives up
+  DTrace trace;                // iteration clock (forward sweep row)
 };
 
 // Analytic and mesh obstacles (device array, refreshed every step for the
@@ -59,9 +60,23 @@ struct IterCtl {
   int kmax;
   int set_cond;
   cudaGraphConditionalHandle cond;
+  DTrace trace;  // iteration clock (Alart-Curnier rows)
 };
 __global__ void k_alart_curnier(DContacts c, const double* v, double* hist, IterCtl ctl);
-__global__ void k_finalize(int n3, const double* qk, double* q);
+// End-of-step record that k_finalize copies into host-mapped memory: the
+// step's counters and its iteration clock (null counts: no record).
+struct StepOut {
+  const int* n_contacts;
+  const int* n_self;
+  const int* n_levels;
+  const int* iter;
+  const unsigned long long* stamps;
+  int n_stamps;
+  int* counts;                     // contacts, self contacts, levels, iterations
+  unsigned long long* stamps_out;  // n_stamps
+};
+__global__ void k_finalize(int n3, const double* qk, double* q, StepOut o);
+__global__ void k_gather_vertices(int n, const int* idx, const double* q, const double* v, double* out);
 
 // Templated kernels are launched through host wrappers defined (and
 // instantiated for float and double) next to the kernels, so that every

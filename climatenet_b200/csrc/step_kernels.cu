@@ -49,6 +49,7 @@ __global__ void k_step_init(DModel m, const double* __restrict__ q, double* __re
 // BendingConstraint.cpp:106-138): p_b = sqrt(b) * (rest/|L x|) L x, or 0 when
 // |L x| <= 1e-25, with L x the mean-value Laplacian at the current iterate.
 __global__ void k_bend_proj(DModel m, const double* __restrict__ qk, double* __restrict__ bp) {
+  trace_stamp(m.trace, DTrace::kLocal);
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= m.B) return;
   double3 lb = make_double3(0., 0., 0.);
@@ -78,6 +79,7 @@ __global__ void k_vertex_rhs(DModel m, const double* __restrict__ qk, const doub
                              const double* __restrict__ cstep, const double* __restrict__ bp,
                              double air_damping, const int* __restrict__ slot_of,
                              double* __restrict__ fslot, T* __restrict__ b, double dt, int residual_mode) {
+  if (m.B == 0) trace_stamp(m.trace, DTrace::kLocal);
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m.N) return;
   const double3 qi = ld3(qk, i);
@@ -176,6 +178,7 @@ __device__ __forceinline__ double3 cone_project(double3 fl, double mu) {
 template <typename T>
 __global__ void k_friction_obstacle(DModel m, DContacts c, T* __restrict__ b, int self_mode, const int* __restrict__ iter,
                                     const float* __restrict__ pred, double pred_sv) {
+  trace_stamp(m.trace, DTrace::kFriction);
   const int C = *c.n_contacts;
   const int S = self_mode ? *c.n_self : 0;
   const int it = *iter;
@@ -244,6 +247,7 @@ template void launch_friction_obstacle<float>(dim3, dim3, cudaStream_t, DModel, 
 template <typename T>
 __global__ void k_friction_self(DModel m, DContacts c, T* __restrict__ b, double* __restrict__ newf,
                                 const int* __restrict__ iter) {
+  trace_stamp(m.trace, DTrace::kSelfFriction);
   const int cur = (*iter) & 1, nxt = 1 - cur;
   const int S = *c.n_self;
   const int C = *c.n_contacts;
@@ -344,6 +348,7 @@ __device__ __forceinline__ void atomic_max_pos(double* addr, double val) {
 }
 
 __global__ void k_alart_curnier(DContacts c, const double* __restrict__ v, double* __restrict__ hist, IterCtl ctl) {
+  trace_stamp(ctl.trace, DTrace::kAcBegin);
   const int C = *c.n_contacts, S = *c.n_self;
   const int it = *ctl.iter;
   double* acc = hist + 4 * (int64_t)it;
@@ -361,6 +366,11 @@ __global__ void k_alart_curnier(DContacts c, const double* __restrict__ v, doubl
       const double3 u = basis_t(B, ld3(v, c.s_vertex[q]) - ld3(v, c.s_partner[q]));
       n = ac_norm(u, ld3(c.s_force, q), c.s_mu[q], &an, &at);
       c.s_ac[q] = n;
+    }
+    if (c.ac_trace && it < c.trace_k) {
+      double* tr = c.ac_trace + 2 * ((int64_t)it * c.trace_stride + k);
+      tr[0] = at;
+      tr[1] = an;
     }
     s += n;
     mx = fmax(mx, n);
@@ -401,6 +411,8 @@ __global__ void k_alart_curnier(DContacts c, const double* __restrict__ v, doubl
     const unsigned int prev = atomicAdd(ctl.blocks_done, 1u);
     if (prev == gridDim.x - 1) {
       *ctl.blocks_done = 0u;
+      if (ctl.trace.stamps && it >= 0 && it < ctl.trace.k)
+        ctl.trace.stamps[(int64_t)DTrace::kAcEnd * ctl.trace.k + it] = global_ns();
       const int k1 = it + 1;
       *ctl.iter = k1;
       *ctl.iter_total += 1;
@@ -414,10 +426,29 @@ __global__ void k_alart_curnier(DContacts c, const double* __restrict__ v, doubl
   }
 }
 
-// End of step (SFE::updateScene SFE:64-87): q <- q^K.
-__global__ void k_finalize(int n3, const double* __restrict__ qk, double* __restrict__ q) {
+// Positions and velocities of listed vertices: out[0 .. 3n) = q, out[3n .. 6n) = v.
+__global__ void k_gather_vertices(int n, const int* __restrict__ idx, const double* __restrict__ q,
+                                  const double* __restrict__ v, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  st3(out, k, ld3(q, idx[k]));
+  st3(out + 3 * (int64_t)n, k, ld3(v, idx[k]));
+}
+
+// End of step (SFE::updateScene SFE:64-87): q <- q^K.  Block 0 also copies
+// the step's counters and iteration clock to the host-mapped record.
+__global__ void k_finalize(int n3, const double* __restrict__ qk, double* __restrict__ q, StepOut o) {
   const int d = blockIdx.x * blockDim.x + threadIdx.x;
   if (d < n3) q[d] = qk[d];
+  if (o.counts && blockIdx.x == 0) {
+    if (threadIdx.x == 0) {
+      o.counts[0] = *o.n_contacts;
+      o.counts[1] = *o.n_self;
+      o.counts[2] = *o.n_levels;
+      o.counts[3] = *o.iter;
+    }
+    for (int k = threadIdx.x; k < o.n_stamps; k += blockDim.x) o.stamps_out[k] = o.stamps[k];
+  }
 }
 
 }  // namespace pdfb

@@ -69,6 +69,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_sweep_forward(const SweepTask* __restrict__ tasks, int ntasks,
                                                        const SnInfo* __restrict__ sn, const int* __restrict__ rows,
                                                        const T* __restrict__ W, T* b, T* y, int n, SweepSync sy) {
+  trace_stamp(sy.trace, DTrace::kSolve);
   const int lane = threadIdx.x & 31;
   const unsigned long long ep = *reinterpret_cast<const volatile unsigned long long*>(sy.epoch);
   // tickets are taken kTicketBatch at a time and processed in order: every

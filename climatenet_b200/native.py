@@ -73,6 +73,13 @@ def lib():
     L.pdf_mlp_samples.argtypes = [vp, vp, vp, i32, C.POINTER(i32)]
     L.pdf_mlp_train.argtypes = [vp, i32, i32, C.c_double, C.c_uint64, C.POINTER(C.c_double),
                                 C.POINTER(C.c_double)]
+    L.pdf_frame_capture.argtypes = [vp, i32]
+    L.pdf_frame_wait.argtypes = [vp, i32, C.POINTER(C.POINTER(C.c_double))]
+    L.pdf_get_vertices.argtypes = [vp, vp, i32, vp, vp]
+    L.pdf_get_alart_curnier_trace.argtypes = [vp, vp, C.c_int64, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
+    L.pdf_log_load_json.argtypes = [C.c_char_p, C.POINTER(vp)]
+    L.pdf_log_view.argtypes = [vp, C.POINTER(i32), C.POINTER(C.POINTER(abi.pdf_log_entry))]
+    L.pdf_log_free.argtypes = [vp]
     _lib = L
     return L
 
@@ -205,6 +212,35 @@ class Simulation:
         _check(lib().pdf_time_phase(self.h, phase, reps, C.byref(ms), C.byref(by)), self.h)
         return ms.value, by.value
 
+    def frame_capture(self, slot):
+        """Start an asynchronous copy of q into pinned frame buffer `slot`."""
+        _check(lib().pdf_frame_capture(self.h, slot), self.h)
+
+    def frame_wait(self, slot):
+        """Positions (N, 3) of the copy started by frame_capture(slot)."""
+        p = C.POINTER(C.c_double)()
+        _check(lib().pdf_frame_wait(self.h, slot, C.byref(p)), self.h)
+        return np.ctypeslib.as_array(p, shape=(self.n, 3)).copy()
+
+    def vertices(self, idx):
+        """(q, v) of the listed vertices, gathered on the device."""
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        q = np.empty((len(idx), 3))
+        v = np.empty((len(idx), 3))
+        _check(lib().pdf_get_vertices(self.h, _ptr(idx), len(idx), _ptr(q), _ptr(v)), self.h)
+        return q, v
+
+    def alart_curnier_trace(self):
+        """Per-iteration (tangential, |normal|) AC norms of the last step's
+        contacts: array (iterations, contacts + self contacts, 2), and the
+        obstacle-contact count."""
+        it, nc, ns = C.c_int32(), C.c_int32(), C.c_int32()
+        _check(lib().pdf_get_alart_curnier_trace(self.h, None, 0, C.byref(it), C.byref(nc), C.byref(ns)), self.h)
+        out = np.zeros((it.value, nc.value + ns.value, 2))
+        _check(lib().pdf_get_alart_curnier_trace(self.h, _ptr(out), out.size, C.byref(it), C.byref(nc),
+                                                 C.byref(ns)), self.h)
+        return out, nc.value
+
     def residual_history(self):
         n = C.c_int32()
         lib().pdf_get_residual_history(self.h, None, 0, C.byref(n))
@@ -288,6 +324,22 @@ def mlp_fit(w, X, T, epochs=20, batch=4096, lr=1e-3, seed=0, device=0):
     _check(lib().pdf_mlp_fit(_ptr(w), _ptr(X), _ptr(T), X.shape[0], epochs, batch, lr, seed, device,
                              C.byref(tl), C.byref(vl)))
     return w, tl.value, vl.value
+
+
+def load_log(path):
+    """The scene JSON's "log" entries: [(kind, vertex indices)] with kind
+    "position" or "velocity" (getLogCallBacksFromJSONDocument)."""
+    h = C.c_void_p()
+    _check(lib().pdf_log_load_json(os.fsencode(path), C.byref(h)))
+    try:
+        n = C.c_int32()
+        ent = C.POINTER(abi.pdf_log_entry)()
+        _check(lib().pdf_log_view(h, C.byref(n), C.byref(ent)))
+        names = {abi.PDF_LOG_POSITION: "position", abi.PDF_LOG_VELOCITY: "velocity"}
+        return [(names[ent[k].kind], [ent[k].vertices[i] for i in range(ent[k].n_vertices)])
+                for k in range(n.value)]
+    finally:
+        lib().pdf_log_free(h)
 
 
 def getSceneFromJSONFileName(path):

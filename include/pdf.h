@@ -140,6 +140,11 @@ typedef struct pdf_params {
   char mlp_weights[256];            /* PDF_WARM_MLP: weights file loaded at create
                                        ("" = set later with pdf_mlp_set_weights
                                        or pdf_mlp_train)                        */
+  int32_t trace_alart_curnier;      /* 1: record every iteration's per-contact
+                                       Alart-Curnier norms for
+                                       pdf_get_alart_curnier_trace (the
+                                       reference's PRINT_ALART_CURNIER_ERROR
+                                       build option, SFE:720-752)              */
 } pdf_params;
 
 /* Fills p with the reference defaults (air damping 0, FP64, fixed iterations). */
@@ -246,10 +251,61 @@ int pdf_get_self_contacts(pdf_handle* h, pdf_contact* out, int32_t capacity,
 int pdf_get_self_levels(pdf_handle* h, int32_t* level_ptr, int32_t level_cap,
                         int32_t* order, int32_t order_cap, int32_t* n_levels);
 
-/* Per-phase statistics; exportStats (SimulationBase.cpp:473-494, SFE:755-770)
- * as a stats.txt-like text written to path. */
+/* Per-phase statistics.  pdf_export_stats replaces exportStats
+ * (SimulationBase.cpp:474-494 inside SFE:756-771, sections written by
+ * computeAndWriteStats, template/physics/io.tpp:23-63): the reference's
+ * sections in its order, one sample per step (detection, self detection,
+ * ordering, step) or per PD iteration (iteration, solver, full RHS, base RHS,
+ * friction, self friction) in microseconds of device time.  Per-iteration
+ * times come from the device clock (%globaltimer) read at the entry of the
+ * iteration's kernels, since the iterations run inside a CUDA graph. */
 int pdf_get_stats(pdf_handle* h, pdf_stats* out);
 int pdf_export_stats(pdf_handle* h, const char* path);
+
+/* ---- frame output and per-step logs (src/main.cpp:86-114) -------------- */
+/* Enqueues a copy of the current positions (3N doubles) into the handle's
+ * pinned frame buffer `slot` (0 or 1) on a copy stream and returns at once;
+ * the copy overlaps the following steps (the next step's write-back of q
+ * waits for it).  No counterpart in the reference, whose frame writer
+ * (Mesh::writeObj, src/geometry/Mesh.cpp:95-109) reads the state
+ * synchronously. */
+int pdf_frame_capture(pdf_handle* h, int32_t slot);
+/* Waits for the copy of `slot`; *q receives its 3N positions (valid until the
+ * slot is captured again or the handle is destroyed: capture a slot again
+ * only once its previous positions have been consumed). */
+int pdf_frame_wait(pdf_handle* h, int32_t slot, const double** q);
+/* Positions and velocities (3 doubles each per listed vertex; either output
+ * may be NULL) of n scene vertices: the reads of the reference's log
+ * callbacks (getVertexPosition / getVertexSpeed, src/log_building.cpp:89-118),
+ * gathered on the device. */
+int pdf_get_vertices(pdf_handle* h, const int32_t* vertices, int32_t n,
+                     double* q, double* v);
+/* Per-iteration Alart-Curnier norms of every contact of the last step, when
+ * the handle was created with trace_alart_curnier = 1
+ * (SimulationFrictionEstimation::updateIterationData SFE:720-752).  out holds
+ * iterations x (n_contacts + n_self) x 2 doubles: per iteration, the obstacle
+ * contacts then the self contacts, each (tangential norm, |normal|).  out may
+ * be NULL to query the sizes; PDF_CAPACITY_EXCEEDED when cap is too small. */
+int pdf_get_alart_curnier_trace(pdf_handle* h, double* out, int64_t cap,
+                                int32_t* iterations, int32_t* n_contacts,
+                                int32_t* n_self);
+
+/* The scene JSON's optional "log" array (getLogCallBacksFromJSONDocument,
+ * src/log_building.cpp:28-129): each entry prints, after every step, the
+ * positions ("position") or velocities ("velocity") of listed vertices of
+ * mesh 0. */
+enum pdf_log_kind { PDF_LOG_POSITION = 0, PDF_LOG_VELOCITY = 1 };
+typedef struct pdf_log_entry {
+  int32_t kind;               /* pdf_log_kind              */
+  int32_t n_vertices;
+  const int32_t* vertices;    /* "vertices", mesh-0 indices */
+} pdf_log_entry;
+typedef struct pdf_log pdf_log;
+/* No "log" member: an empty list.  Errors as the reference's reader. */
+int pdf_log_load_json(const char* json_path, pdf_log** out);
+int pdf_log_view(const pdf_log* log, int32_t* n_entries,
+                 const pdf_log_entry** entries);
+void pdf_log_free(pdf_log* log);
 
 /* Per-iteration mean AC residuals of the last step (n <= cap written). */
 int pdf_get_residual_history(pdf_handle* h, double* out, int32_t cap,

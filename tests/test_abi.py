@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_struct_layout_matches_c(tmp_path):
     structs = ["pdf_obstacle", "pdf_mesh_desc", "pdf_scene_desc", "pdf_params", "pdf_step_report",
-               "pdf_stats", "pdf_contact"]
+               "pdf_stats", "pdf_contact", "pdf_log_entry"]
     prog = ['#include <stdio.h>', '#include "%s"' % HEADER, "int main(void){"]
     for s in structs:
         prog.append('printf("%%s %%zu\\n", "%s", sizeof(%s));' % (s, s))
