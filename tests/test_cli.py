@@ -214,7 +214,8 @@ def read_log_blocks(text):
 @pytest.mark.gpu
 def test_cli_grid_run_frames_logs_trace(tmp_path):
     frames, spf = 3, 2
-    js = grid_scene_json(tmp_path, frames=frames, spf=spf,
+    # odd grid: the centre vertex starts within the sphere's 1 cm margin
+    js = grid_scene_json(tmp_path, frames=frames, spf=spf, n=7,
                          log=[{"type": "position", "vertices": [0, 7]}, {"type": "velocity", "vertices": [3]}])
     r = subprocess.run([PDF_RUN, str(js), "--print-alart-curnier"], capture_output=True, text=True, cwd=tmp_path,
                        timeout=300)
@@ -241,7 +242,7 @@ def test_cli_grid_run_frames_logs_trace(tmp_path):
         obj = (tmp_path / "data0" / "output" / ("out_%06d.obj" % f)).read_text().split("\n")
         vs = np.array([[float(x) for x in ln.split()[1:]] for ln in obj if ln.startswith("v ")])
         fs = [ln for ln in obj if ln.startswith("f ")]
-        assert len(fs) == 2 * 5 * 5 and fs[0] == "f 1 2 8"
+        assert len(fs) == 2 * 6 * 6 and fs[0] == "f 1 2 9"
         # default stream formatting keeps 6 significant digits
         assert np.allclose(vs, states[f * spf][0], rtol=1e-5, atol=1e-6)
     logs = read_log_blocks(out)
@@ -256,6 +257,7 @@ def test_cli_grid_run_frames_logs_trace(tmp_path):
     assert len(tang) == len(norm) == steps * p.local_global_iterations
     vals = [list(map(float, ln.split(" ")[1:-1])) for ln in norm]
     assert all(len(x) > 0 and min(x) >= 0 for x in vals)
+    assert not any(ln.startswith("SelfTangentialAlartCurnier") for ln in out.split("\n"))
     st = parse_stats((tmp_path / "data0" / "stats.txt").read_text())
     assert st["Step time (µs)"]["Number"] == steps
     assert (tmp_path / "data0" / "scene.json").exists()
