@@ -200,4 +200,6 @@ def test_moving_mesh_steps_match_oracle():
     qg, vg = g.state()
     qo, vo = o.state()
     assert np.abs(qg - qo).max() / np.abs(qo).max() < 1e-6
-    assert np.abs(vg - vo).max() <= 1e-5 * max(np.abs(vo).max(), 1e-12)
+    # the cloth ends at rest on the floor: velocities near zero, compared
+    # against the run's velocity scale (the floor moved at up to 0.75 m/s)
+    assert np.abs(vg - vo).max() <= 1e-5 * max(np.abs(vo).max(), 1e-3)
