@@ -550,10 +550,10 @@ int64_t launches_per_iteration(const pdf_handle* h) {
 
 // Per step outside the iterations: predictor, obstacle flags + clamp + materialise,
 // slots (2), slot reset, finalize; self-collision: register reset, per mesh
-// bbox/keys/build/refit/traverse/pair, bases, levels.
+// bbox/keys/build/refit/traverse/compact/pair, bases, levels.
 int64_t launches_per_step_extra(const pdf_handle* h) {
   int64_t n = 1 + (h->obs.n > 0 ? 3 : 0) + 2 + 1 + 1;
-  if (h->prm.self_collision) n += 1 + 6 * (int64_t)h->model.meshes.size() + 1 + 1;
+  if (h->prm.self_collision) n += 1 + 7 * (int64_t)h->model.meshes.size() + 1 + 1;
   // warm start: features, forward; record (clear + accumulate [+ count])
   const bool warm = h->prm.warm_start == PDF_WARM_MLP;
   if (warm || h->log_cap > 0) n += 1 + 2 + (h->log_cap > 0 ? 1 : 0) + (warm ? 1 : 0);
@@ -949,7 +949,7 @@ int pdf_step(pdf_handle* h, int32_t nsteps, pdf_step_report* report) {
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->prm.device));
     CK(cudaEventRecord(h->ev[5], h->stream));
-    for (int s = 0; s < nsteps; ++s) step_once(h, (s == nsteps - 1) || h->prm.self_collision);
+    for (int s = 0; s < nsteps; ++s) step_once(h, s == nsteps - 1);
     CK(cudaEventRecord(h->ev[6], h->stream));
     CK(cudaStreamSynchronize(h->stream));
     harvest_all(h);
@@ -959,7 +959,15 @@ int pdf_step(pdf_handle* h, int32_t nsteps, pdf_step_report* report) {
     if (report) *report = h->last;
     int derr = 0;
     CK(cudaMemcpy(&derr, h->d.sync.err, sizeof(int), cudaMemcpyDeviceToHost));
+    // error word bits: 1 sweep wait gave up, 2 obstacle contacts, 4 self
+    // contacts or partners, 8 self-collision hits, 16 BVH stack
     if (derr & 2) return fail(h, PDF_CAPACITY_EXCEEDED, "more obstacle contacts than contact_capacity");
+    if (derr & 4)
+      return fail(h, PDF_CAPACITY_EXCEEDED,
+                  "more self contacts than the self-contact buffer, or a vertex with more than 16 partners");
+    if (derr & 8)
+      return fail(h, PDF_CAPACITY_EXCEEDED, "more than 16 self-collision hits at a vertex, or hit buffer full");
+    if (derr & 16) return fail(h, PDF_CAPACITY_EXCEEDED, "self-collision BVH deeper than the traversal stack");
     if (derr) return fail(h, PDF_DEVICE_TIMEOUT, "a supernodal sweep gave up waiting for a dependency");
     return PDF_OK;
   });

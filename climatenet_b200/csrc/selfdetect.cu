@@ -37,7 +37,22 @@
 namespace pdfb {
 namespace {
 
-constexpr int kRegCap = 16;  // pairing partners remembered per vertex
+constexpr int kRegCap = 16;   // pairing partners remembered per vertex
+constexpr int kHitSlots = 16; // step path: pairable hits kept per vertex
+
+// Error bits of the handle's device error word set by the step path (read at
+// the end of pdf_step): more partners or self contacts than the buffers hold,
+// more hits than kHitSlots per vertex or than the hit buffer, BVH stack.
+constexpr int kErrSelfContacts = 4, kErrSelfHits = 8, kErrSelfStack = 16;
+
+// LBVH node of the step path: both children's boxes and ids in one 112-byte
+// record, so a traversal tests both children with one node load.  Child id
+// >= 0: internal node; < 0: ~triangle (leaf).
+struct __align__(16) WNode {
+  double b[12];  // child 0 lo xyz, hi xyz; child 1 lo xyz, hi xyz
+  int ch[2];
+  int pad[2];
+};
 
 struct SelfWS {
   int max_nt = 0, max_nv = 0, hit_cap = 0;
@@ -58,6 +73,9 @@ struct SelfWS {
       *cmin = nullptr, *elev = nullptr, *lcount = nullptr;
   void* cub_tmp = nullptr;
   size_t cub_bytes = 0;
+  // step path: wide nodes, per-vertex hit slots and counts, their offsets
+  WNode* wnodes = nullptr;
+  int *hcount = nullptr, *hoff = nullptr, *slot_tri = nullptr, *n_total = nullptr;
 };
 
 #define CKS(x)                                                                                    \
@@ -225,6 +243,148 @@ __global__ void k_refit(int n, const int* __restrict__ mval, const double* tlo, 
   }
 }
 
+// Bottom-up refit into wide nodes: each finished box (a leaf's triangle box,
+// or the union of a node's two children) is written into its slot of the
+// parent's record; the second child to arrive at a node computes its union.
+__device__ __forceinline__ void put_child(WNode* nodes, const int* left, int p, int self_id, int enc, double3 lo,
+                                          double3 hi) {
+  const int side = left[p] == self_id ? 0 : 1;
+  double* b = nodes[p].b + 6 * side;
+  __stcg(b + 0, lo.x);
+  __stcg(b + 1, lo.y);
+  __stcg(b + 2, lo.z);
+  __stcg(b + 3, hi.x);
+  __stcg(b + 4, hi.y);
+  __stcg(b + 5, hi.z);
+  __stcg(nodes[p].ch + side, enc);
+}
+
+__global__ void k_refit_wide(int n, const int* __restrict__ mval, const double* __restrict__ tlo,
+                             const double* __restrict__ thi, const int* __restrict__ left, const int* __restrict__ parent,
+                             const int* __restrict__ leaf_parent, WNode* nodes, int* visits) {
+  const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+  if (leaf >= n) return;
+  const int tri = mval[leaf];
+  int p = leaf_parent[leaf];
+  put_child(nodes, left, p, ~leaf, ~tri, ld3(tlo, tri), ld3(thi, tri));
+  while (p >= 0) {
+    __threadfence();
+    if (atomicAdd(visits + p, 1) == 0) return;
+    __threadfence();
+    const double* b = nodes[p].b;
+    double v[12];
+    for (int k = 0; k < 12; ++k) v[k] = __ldcg(b + k);
+    const double3 lo = make_double3(fmin(v[0], v[6]), fmin(v[1], v[7]), fmin(v[2], v[8]));
+    const double3 hi = make_double3(fmax(v[3], v[9]), fmax(v[4], v[10]), fmax(v[5], v[11]));
+    const int pp = parent[p];
+    if (pp >= 0) put_child(nodes, left, pp, p, p, lo, hi);
+    p = pp;
+  }
+}
+
+// Step-path traversal: both children tested at their parent; every hit that
+// survives the closest-point filter and can pair (as in mode 1 below) goes to
+// the vertex's own slots, unordered.
+__global__ void k_traverse_slots(int nv, int nt, const double* __restrict__ q, const int* __restrict__ tris, int v0,
+                                 double tol, const WNode* __restrict__ nodes, const double* __restrict__ tlo,
+                                 const double* __restrict__ thi, int* __restrict__ hcount, int* __restrict__ slot_tri,
+                                 int* err) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const double t = 1.1 * tol;
+  const double tol_sq = tol * tol;
+  const double3 x = ld3(q, v0 + v);
+  int count = 0;
+  auto leaf = [&](int tri) {
+    const int ia = tris[3 * tri] - v0, ib = tris[3 * tri + 1] - v0, ic = tris[3 * tri + 2] - v0;
+    if (ia == v || ib == v || ic == v) return;
+    double3 cp, w;
+    closest_point(x, ld3(q, v0 + ia), ld3(q, v0 + ib), ld3(q, v0 + ic), tol, &cp, &w);
+    const double3 dd = cp - x;
+    if (!(dot3(dd, dd) < tol_sq)) return;
+    if (w.x == 0 || w.y == 0 || w.z == 0) return;
+    if (count < kHitSlots) slot_tri[(int64_t)v * kHitSlots + count] = tri;
+    ++count;
+  };
+  if (nt == 1) {
+    if (box_overlap(x, t, ld3(tlo, 0), ld3(thi, 0))) leaf(0);
+  } else {
+    int stack[64];
+    int sp = 0;
+    int node = 0;
+    while (true) {
+      const WNode& nd = nodes[node];
+      double b[12];
+      for (int k = 0; k < 12; ++k) b[k] = __ldg(nd.b + k);
+      const int c0 = __ldg(nd.ch), c1 = __ldg(nd.ch + 1);
+      const bool o0 = box_overlap(x, t, make_double3(b[0], b[1], b[2]), make_double3(b[3], b[4], b[5]));
+      const bool o1 = box_overlap(x, t, make_double3(b[6], b[7], b[8]), make_double3(b[9], b[10], b[11]));
+      if (o0) {
+        if (c0 < 0)
+          leaf(~c0);
+        else
+          stack[sp++] = c0;
+      }
+      if (o1) {
+        if (c1 < 0)
+          leaf(~c1);
+        else
+          stack[sp++] = c1;
+      }
+      if (sp == 0) break;
+      if (sp > 62) {
+        atomicOr(err, kErrSelfStack);
+        break;
+      }
+      node = stack[--sp];
+    }
+  }
+  if (count > kHitSlots) {
+    atomicOr(err, kErrSelfHits);
+    count = kHitSlots;
+  }
+  hcount[v] = count;
+}
+
+// Hits in canonical (vertex, triangle) order without a global sort: vertex v
+// owns [hoff[v], hoff[v] + hcount[v]); its triangles are sorted in place and
+// the barycentric coordinates recomputed (same arithmetic as the traversal).
+__global__ void k_compact_hits(int nv, const double* __restrict__ q, const int* __restrict__ tris, int v0, double tol,
+                               const int* __restrict__ hcount, const int* __restrict__ hoff,
+                               const int* __restrict__ slot_tri, int cap, unsigned long long* hkey, int* hval,
+                               double* hbary, int* n_total, int* err) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const int cnt = hcount[v], o = hoff[v];
+  if (v == nv - 1) {
+    const int total = o + cnt;
+    if (total > cap) atomicOr(err, kErrSelfHits);
+    *n_total = min(total, cap);
+  }
+  if (cnt == 0) return;
+  int tl[kHitSlots];
+  for (int k = 0; k < cnt; ++k) {
+    const int tv = slot_tri[(int64_t)v * kHitSlots + k];
+    int j = k;
+    while (j > 0 && tl[j - 1] > tv) {
+      tl[j] = tl[j - 1];
+      --j;
+    }
+    tl[j] = tv;
+  }
+  const double3 x = ld3(q, v0 + v);
+  for (int k = 0; k < cnt; ++k) {
+    const int h = o + k;
+    if (h >= cap) return;
+    const int tri = tl[k];
+    double3 cp, w;
+    closest_point(x, ld3(q, tris[3 * tri]), ld3(q, tris[3 * tri + 1]), ld3(q, tris[3 * tri + 2]), tol, &cp, &w);
+    hkey[h] = ((unsigned long long)v << 32) | (unsigned int)tri;
+    hval[h] = h;
+    st3(hbary, h, w);
+  }
+}
+
 // Per-vertex traversal.  mode 0: emit every box candidate (v, t);
 // mode 1: emit hits that survive the closest-point filter and can pair.
 __global__ void k_traverse(int nv, int nt, const double* __restrict__ q, const int* __restrict__ tris, int v0,
@@ -282,13 +442,18 @@ __global__ void k_traverse(int nv, int nt, const double* __restrict__ q, const i
 
 // Greedy node-node pairing (checkMeshSelfCollisions, geometry_util.cpp:94-219)
 // over hits in canonical order; emits self contacts in the order found.
+// n_hits_dev (if not null) holds the hit count on the device; err_word (if
+// not null) receives kErrSelfContacts instead of *err being set, and the
+// contacts paired so far are kept.
 __global__ void k_pair(int n_hits, const unsigned long long* __restrict__ hkey, const int* __restrict__ hval,
                        const double* __restrict__ hbary, const double* __restrict__ q, const int* __restrict__ tris,
                        int v0, const int* __restrict__ ring_ptr, const int* __restrict__ ring_idx, double mu,
-                       int* reg, int* reg_n, int* touched, int* n_touched, int touched_cap, DContacts c, int* err) {
+                       int* reg, int* reg_n, int* touched, int* n_touched, int touched_cap, DContacts c, int* err,
+                       const int* n_hits_dev = nullptr, int* err_word = nullptr) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   int S = *c.n_self;
   int nt = *n_touched;
+  if (n_hits_dev) n_hits = *n_hits_dev;
   for (int h = 0; h < n_hits; ++h) {
     const int v = (int)(hkey[h] >> 32);
     const int tri = (int)(hkey[h] & 0xffffffffu);
@@ -333,6 +498,10 @@ __global__ void k_pair(int n_hits, const unsigned long long* __restrict__ hkey, 
     const double3 nrm = normalized3(ld3(q, gv) - cpt);
     const int paired = tv[best];
     if (reg_n[paired] >= kRegCap || reg_n[gv] >= kRegCap) {
+      if (err_word) {
+        atomicOr(err_word, kErrSelfContacts);
+        break;
+      }
       *err = 3;
       return;
     }
@@ -341,6 +510,10 @@ __global__ void k_pair(int n_hits, const unsigned long long* __restrict__ hkey, 
     if (reg_n[gv] == 0 && nt < touched_cap) touched[nt++] = gv;
     reg[gv * kRegCap + reg_n[gv]++] = paired;
     if (S >= c.self_cap) {
+      if (err_word) {
+        atomicOr(err_word, kErrSelfContacts);
+        break;
+      }
       *err = 4;
       return;
     }
@@ -525,10 +698,16 @@ void ws_alloc(SelfWS& w, int nv, int nt, int hit_cap, int slot_cap) {
   w.hval2 = salloc<int>(hit_cap);
   w.hbary = salloc<double>(3 * (size_t)hit_cap);
   w.err = salloc<int>(1);
-  size_t b1 = 0, b2 = 0;
+  w.wnodes = salloc<WNode>(nt);
+  w.hcount = salloc<int>(nv);
+  w.hoff = salloc<int>(nv);
+  w.slot_tri = salloc<int>((size_t)nv * kHitSlots);
+  w.n_total = salloc<int>(1);
+  size_t b1 = 0, b2 = 0, b3 = 0;
+  CKS(cub::DeviceScan::ExclusiveSum(nullptr, b3, w.hcount, w.hoff, nv));
   CKS(cub::DeviceRadixSort::SortPairs(nullptr, b1, w.mkey, w.mkey2, w.mval, w.mval2, nt));
   CKS(cub::DeviceRadixSort::SortPairs(nullptr, b2, w.hkey, w.hkey2, w.hval, w.hval2, hit_cap));
-  w.cub_bytes = std::max(b1, b2);
+  w.cub_bytes = std::max(std::max(b1, b2), b3);
   w.cub_tmp = salloc<char>(w.cub_bytes);
   (void)slot_cap;
 }
@@ -537,7 +716,7 @@ void ws_free(SelfWS& w) {
   void* ptrs[] = {w.tlo, w.thi, w.mkey, w.mkey2, w.mval, w.mval2, w.left, w.right, w.parent, w.leaf_parent,
                   w.nlo, w.nhi, w.visits, w.bbox, w.n_hits, w.hkey, w.hkey2, w.hval, w.hval2, w.hbary,
                   w.reg, w.reg_n, w.touched, w.n_touched, w.err, w.deg, w.uf, w.dist, w.seed, w.cobst, w.cdeg1,
-                  w.cmin, w.elev, w.lcount, w.cub_tmp};
+                  w.cmin, w.elev, w.lcount, w.cub_tmp, w.wnodes, w.hcount, w.hoff, w.slot_tri, w.n_total};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   w = SelfWS{};
@@ -576,6 +755,32 @@ int detect_mesh(SelfWS& w, const double* q, const int* tris_global, int v0, int 
     CKS(cub::DeviceRadixSort::SortPairs(w.cub_tmp, bytes, w.hkey, w.hkey2, w.hval, w.hval2, nh, 0, bits, st));
   }
   return nh;
+}
+
+// Step path of detect_mesh: same candidate semantics, no host round trip.
+// The hits of mesh [v0, v0+nv) end in hkey2 / hval2 / hbary in canonical
+// order with their count in *w.n_total; errors go to err_word.
+void detect_mesh_step(SelfWS& w, const double* q, const int* tris_global, int v0, int nv, int nt, double tol,
+                      cudaStream_t st, int* err_word) {
+  const int tb = 256;
+  const unsigned long long init[6] = {~0ULL, ~0ULL, ~0ULL, 0ULL, 0ULL, 0ULL};
+  CKS(cudaMemcpyAsync(w.bbox, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  k_bbox<<<std::min(1024, (nv + tb - 1) / tb), tb, 0, st>>>(nv, q + 3 * (size_t)v0, w.bbox);
+  k_tri_keys<<<(nt + tb - 1) / tb, tb, 0, st>>>(nt, q, tris_global, v0, w.bbox, w.tlo, w.thi, w.mkey, w.mval);
+  size_t bytes = w.cub_bytes;
+  CKS(cub::DeviceRadixSort::SortPairs(w.cub_tmp, bytes, w.mkey, w.mkey2, w.mval, w.mval2, nt, 0, 64, st));
+  if (nt > 1) {
+    k_build<<<(nt - 1 + tb - 1) / tb, tb, 0, st>>>(nt, w.mkey2, w.left, w.right, w.parent, w.leaf_parent);
+    CKS(cudaMemsetAsync(w.visits, 0, sizeof(int) * nt, st));
+    k_refit_wide<<<(nt + tb - 1) / tb, tb, 0, st>>>(nt, w.mval2, w.tlo, w.thi, w.left, w.parent, w.leaf_parent,
+                                                    w.wnodes, w.visits);
+  }
+  k_traverse_slots<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, nt, q, tris_global, v0, tol, w.wnodes, w.tlo, w.thi,
+                                                      w.hcount, w.slot_tri, err_word);
+  bytes = w.cub_bytes;
+  CKS(cub::DeviceScan::ExclusiveSum(w.cub_tmp, bytes, w.hcount, w.hoff, nv, st));
+  k_compact_hits<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, q, tris_global, v0, tol, w.hcount, w.hoff, w.slot_tri,
+                                                    w.hit_cap, w.hkey2, w.hval2, w.hbary, w.n_total, err_word);
 }
 
 // pairing / level scratch sized by the scene
@@ -635,25 +840,15 @@ int self_detect_step(pdf_handle* h) {
   CKS(cudaMemsetAsync(c.n_self, 0, sizeof(int), st));
   k_reset_registered<<<64, 256, 0, st>>>(w.reg_n, w.touched, w.n_touched);
   CKS(cudaMemsetAsync(w.n_touched, 0, sizeof(int), st));
+  // no host round trip: counts stay on the device, errors go to the handle's
+  // error word (read at the end of pdf_step)
   for (const auto& md : h->model.meshes) {
-    const int nh = detect_mesh(w, h->d.q, h->d.tris + 3 * (size_t)md.triangle_offset, md.vertex_offset,
-                               md.n_vertices, md.n_triangles, tol, 1, st);
-    if (nh > w.hit_cap) {
-      h->err = "self-collision hit buffer too small (" + std::to_string(nh) + " hits)";
-      return PDF_CAPACITY_EXCEEDED;
-    }
+    const int* mtris = h->d.tris + 3 * (size_t)md.triangle_offset;
+    detect_mesh_step(w, h->d.q, mtris, md.vertex_offset, md.n_vertices, md.n_triangles, tol, st, h->d.sync.err);
     const double mu = h->model.friction[(size_t)md.material * h->model.n_materials + md.material];
-    if (nh > 0)
-      k_pair<<<1, 1, 0, st>>>(nh, w.hkey2, w.hval2, w.hbary, h->d.q, h->d.tris + 3 * (size_t)md.triangle_offset,
-                              md.vertex_offset, h->d.ring_ptr, h->d.ring_idx, mu, w.reg, w.reg_n, w.touched,
-                              w.n_touched, h->model.N, c, w.err);
-  }
-  int err = 0;
-  CKS(cudaMemcpyAsync(&err, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
-  CKS(cudaStreamSynchronize(st));
-  if (err) {
-    h->err = err == 3 ? "a vertex has more than 16 self-contact partners" : "self-contact buffer too small";
-    return PDF_CAPACITY_EXCEEDED;
+    k_pair<<<1, 1, 0, st>>>(0, w.hkey2, w.hval2, w.hbary, h->d.q, mtris, md.vertex_offset, h->d.ring_ptr,
+                            h->d.ring_idx, mu, w.reg, w.reg_n, w.touched, w.n_touched, h->model.N, c, w.err, w.n_total,
+                            h->d.sync.err);
   }
   k_self_bases<<<64, 256, 0, st>>>(c);
   return PDF_OK;

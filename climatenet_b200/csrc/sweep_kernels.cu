@@ -47,7 +47,7 @@ __device__ __forceinline__ bool wait_counter(const unsigned long long* ctr, unsi
   int spins = 0;
   while (ld_volatile_u64(ctr) < target) {
     if (++spins > kMaxSpins) {
-      atomicExch(err, 1);
+      atomicOr(err, 1);
       return false;
     }
     __nanosleep(32);
