@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 
 #include <cub/cub.cuh>
+#include <cuda/atomic>
 #include <algorithm>
 #include <cstring>
 #include <stdexcept>
@@ -39,6 +40,7 @@ namespace {
 
 constexpr int kRegCap = 16;   // pairing partners remembered per vertex
 constexpr int kHitSlots = 16; // step path: pairable hits kept per vertex
+constexpr int kRebuildEvery = 8;  // step path: hierarchy rebuilt every k steps, refit in between
 
 // Error bits of the handle's device error word set by the step path (read at
 // the end of pdf_step): more partners or self contacts than the buffers hold,
@@ -73,9 +75,14 @@ struct SelfWS {
       *cmin = nullptr, *elev = nullptr, *lcount = nullptr;
   void* cub_tmp = nullptr;
   size_t cub_bytes = 0;
-  // step path: wide nodes, per-vertex hit slots and counts, their offsets
+  // step path: one persistent hierarchy per mesh (regions at the mesh's
+  // triangle offset, all meshes' triangles in total), per-vertex hit slots
+  // and counts (shared by the meshes, consumed within the step)
   WNode* wnodes = nullptr;
+  int *s_mval = nullptr, *s_left = nullptr, *s_right = nullptr, *s_parent = nullptr, *s_leaf_parent = nullptr,
+      *s_visits = nullptr;
   int *hcount = nullptr, *hoff = nullptr, *slot_tri = nullptr, *n_total = nullptr;
+  std::vector<int> since_build;  // per mesh: steps since its hierarchy was built (0 = never)
 };
 
 #define CKS(x)                                                                                    \
@@ -259,18 +266,22 @@ __device__ __forceinline__ void put_child(WNode* nodes, const int* left, int p, 
   __stcg(nodes[p].ch + side, enc);
 }
 
-__global__ void k_refit_wide(int n, const int* __restrict__ mval, const double* __restrict__ tlo,
-                             const double* __restrict__ thi, const int* __restrict__ left, const int* __restrict__ parent,
+// Leaf boxes come straight from the positions (a triangle's own bounding
+// box, as tri_box computes it everywhere else).
+__global__ void k_refit_wide(int n, const int* __restrict__ mval, const double* __restrict__ q,
+                             const int* __restrict__ tris, const int* __restrict__ left, const int* __restrict__ parent,
                              const int* __restrict__ leaf_parent, WNode* nodes, int* visits) {
   const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
   if (leaf >= n) return;
   const int tri = mval[leaf];
   int p = leaf_parent[leaf];
-  put_child(nodes, left, p, ~leaf, ~tri, ld3(tlo, tri), ld3(thi, tri));
+  double3 tl, th;
+  tri_box(ld3(q, tris[3 * tri]), ld3(q, tris[3 * tri + 1]), ld3(q, tris[3 * tri + 2]), &tl, &th);
+  put_child(nodes, left, p, ~leaf, ~tri, tl, th);
   while (p >= 0) {
-    __threadfence();
-    if (atomicAdd(visits + p, 1) == 0) return;
-    __threadfence();
+    // release our child box, acquire the sibling's
+    cuda::atomic_ref<int, cuda::thread_scope_device> arrivals(visits[p]);
+    if (arrivals.fetch_add(1, cuda::memory_order_acq_rel) == 0) return;
     const double* b = nodes[p].b;
     double v[12];
     for (int k = 0; k < 12; ++k) v[k] = __ldcg(b + k);
@@ -286,9 +297,8 @@ __global__ void k_refit_wide(int n, const int* __restrict__ mval, const double* 
 // survives the closest-point filter and can pair (as in mode 1 below) goes to
 // the vertex's own slots, unordered.
 __global__ void k_traverse_slots(int nv, int nt, const double* __restrict__ q, const int* __restrict__ tris, int v0,
-                                 double tol, const WNode* __restrict__ nodes, const double* __restrict__ tlo,
-                                 const double* __restrict__ thi, int* __restrict__ hcount, int* __restrict__ slot_tri,
-                                 int* err) {
+                                 double tol, const WNode* __restrict__ nodes, int* __restrict__ hcount,
+                                 int* __restrict__ slot_tri, int* err) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   const double t = 1.1 * tol;
@@ -307,7 +317,9 @@ __global__ void k_traverse_slots(int nv, int nt, const double* __restrict__ q, c
     ++count;
   };
   if (nt == 1) {
-    if (box_overlap(x, t, ld3(tlo, 0), ld3(thi, 0))) leaf(0);
+    double3 tl, th;
+    tri_box(ld3(q, tris[0]), ld3(q, tris[1]), ld3(q, tris[2]), &tl, &th);
+    if (box_overlap(x, t, tl, th)) leaf(0);
   } else {
     int stack[64];
     int sp = 0;
@@ -698,7 +710,6 @@ void ws_alloc(SelfWS& w, int nv, int nt, int hit_cap, int slot_cap) {
   w.hval2 = salloc<int>(hit_cap);
   w.hbary = salloc<double>(3 * (size_t)hit_cap);
   w.err = salloc<int>(1);
-  w.wnodes = salloc<WNode>(nt);
   w.hcount = salloc<int>(nv);
   w.hoff = salloc<int>(nv);
   w.slot_tri = salloc<int>((size_t)nv * kHitSlots);
@@ -716,7 +727,8 @@ void ws_free(SelfWS& w) {
   void* ptrs[] = {w.tlo, w.thi, w.mkey, w.mkey2, w.mval, w.mval2, w.left, w.right, w.parent, w.leaf_parent,
                   w.nlo, w.nhi, w.visits, w.bbox, w.n_hits, w.hkey, w.hkey2, w.hval, w.hval2, w.hbary,
                   w.reg, w.reg_n, w.touched, w.n_touched, w.err, w.deg, w.uf, w.dist, w.seed, w.cobst, w.cdeg1,
-                  w.cmin, w.elev, w.lcount, w.cub_tmp, w.wnodes, w.hcount, w.hoff, w.slot_tri, w.n_total};
+                  w.cmin, w.elev, w.lcount, w.cub_tmp, w.wnodes, w.hcount, w.hoff, w.slot_tri, w.n_total,
+                  w.s_mval, w.s_left, w.s_right, w.s_parent, w.s_leaf_parent, w.s_visits};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   w = SelfWS{};
@@ -760,24 +772,34 @@ int detect_mesh(SelfWS& w, const double* q, const int* tris_global, int v0, int 
 // Step path of detect_mesh: same candidate semantics, no host round trip.
 // The hits of mesh [v0, v0+nv) end in hkey2 / hval2 / hbary in canonical
 // order with their count in *w.n_total; errors go to err_word.
-void detect_mesh_step(SelfWS& w, const double* q, const int* tris_global, int v0, int nv, int nt, double tol,
-                      cudaStream_t st, int* err_word) {
+void detect_mesh_step(SelfWS& w, const double* q, const int* tris_global, int v0, int nv, int nt, int t0,
+                      bool rebuild, double tol, cudaStream_t st, int* err_word) {
   const int tb = 256;
-  const unsigned long long init[6] = {~0ULL, ~0ULL, ~0ULL, 0ULL, 0ULL, 0ULL};
-  CKS(cudaMemcpyAsync(w.bbox, init, sizeof(init), cudaMemcpyHostToDevice, st));
-  k_bbox<<<std::min(1024, (nv + tb - 1) / tb), tb, 0, st>>>(nv, q + 3 * (size_t)v0, w.bbox);
-  k_tri_keys<<<(nt + tb - 1) / tb, tb, 0, st>>>(nt, q, tris_global, v0, w.bbox, w.tlo, w.thi, w.mkey, w.mval);
-  size_t bytes = w.cub_bytes;
-  CKS(cub::DeviceRadixSort::SortPairs(w.cub_tmp, bytes, w.mkey, w.mkey2, w.mval, w.mval2, nt, 0, 64, st));
-  if (nt > 1) {
-    k_build<<<(nt - 1 + tb - 1) / tb, tb, 0, st>>>(nt, w.mkey2, w.left, w.right, w.parent, w.leaf_parent);
-    CKS(cudaMemsetAsync(w.visits, 0, sizeof(int) * nt, st));
-    k_refit_wide<<<(nt + tb - 1) / tb, tb, 0, st>>>(nt, w.mval2, w.tlo, w.thi, w.left, w.parent, w.leaf_parent,
-                                                    w.wnodes, w.visits);
+  int* mval = w.s_mval + t0;
+  int* left = w.s_left + t0;
+  int* parent = w.s_parent + t0;
+  int* leaf_parent = w.s_leaf_parent + t0;
+  WNode* nodes = w.wnodes + t0;
+  if (rebuild) {
+    const unsigned long long init[6] = {~0ULL, ~0ULL, ~0ULL, 0ULL, 0ULL, 0ULL};
+    CKS(cudaMemcpyAsync(w.bbox, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    k_bbox<<<std::min(1024, (nv + tb - 1) / tb), tb, 0, st>>>(nv, q + 3 * (size_t)v0, w.bbox);
+    k_tri_keys<<<(nt + tb - 1) / tb, tb, 0, st>>>(nt, q, tris_global, v0, w.bbox, w.tlo, w.thi, w.mkey, w.mval);
+    // key = morton << 32 | triangle and the sort is stable on triangles in
+    // ascending order: the 30 Morton bits give the full key order
+    size_t bytes = w.cub_bytes;
+    CKS(cub::DeviceRadixSort::SortPairs(w.cub_tmp, bytes, w.mkey, w.mkey2, w.mval, mval, nt, 32, 62, st));
+    if (nt > 1)
+      k_build<<<(nt - 1 + tb - 1) / tb, tb, 0, st>>>(nt, w.mkey2, left, w.s_right + t0, parent, leaf_parent);
   }
-  k_traverse_slots<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, nt, q, tris_global, v0, tol, w.wnodes, w.tlo, w.thi,
-                                                      w.hcount, w.slot_tri, err_word);
-  bytes = w.cub_bytes;
+  if (nt > 1) {
+    CKS(cudaMemsetAsync(w.s_visits + t0, 0, sizeof(int) * nt, st));
+    k_refit_wide<<<(nt + tb - 1) / tb, tb, 0, st>>>(nt, mval, q, tris_global, left, parent, leaf_parent, nodes,
+                                                    w.s_visits + t0);
+  }
+  k_traverse_slots<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, nt, q, tris_global, v0, tol, nodes, w.hcount, w.slot_tri,
+                                                      err_word);
+  size_t bytes = w.cub_bytes;
   CKS(cub::DeviceScan::ExclusiveSum(w.cub_tmp, bytes, w.hcount, w.hoff, nv, st));
   k_compact_hits<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, q, tris_global, v0, tol, w.hcount, w.hoff, w.slot_tri,
                                                     w.hit_cap, w.hkey2, w.hval2, w.hbary, w.n_total, err_word);
@@ -814,6 +836,15 @@ int self_detect_init(pdf_handle* h) {
     }
     ws_alloc(*w, max_nv, max_nt, std::max(1024, 4 * max_nv), h->model.N);
     ws_alloc_pairing(*w, h->model.N, h->model.N, h->cap_self);
+    const size_t T = std::max<size_t>(1, h->model.tris.size() / 3);
+    w->wnodes = salloc<WNode>(T);
+    w->s_mval = salloc<int>(T);
+    w->s_left = salloc<int>(T);
+    w->s_right = salloc<int>(T);
+    w->s_parent = salloc<int>(T);
+    w->s_leaf_parent = salloc<int>(T);
+    w->s_visits = salloc<int>(T);
+    w->since_build.assign(h->model.meshes.size(), 0);
     h->d.self_ws = w;
   } catch (const std::exception& e) {
     h->err = e.what();
@@ -842,9 +873,16 @@ int self_detect_step(pdf_handle* h) {
   CKS(cudaMemsetAsync(w.n_touched, 0, sizeof(int), st));
   // no host round trip: counts stay on the device, errors go to the handle's
   // error word (read at the end of pdf_step)
-  for (const auto& md : h->model.meshes) {
+  for (size_t mi = 0; mi < h->model.meshes.size(); ++mi) {
+    const auto& md = h->model.meshes[mi];
     const int* mtris = h->d.tris + 3 * (size_t)md.triangle_offset;
-    detect_mesh_step(w, h->d.q, mtris, md.vertex_offset, md.n_vertices, md.n_triangles, tol, st, h->d.sync.err);
+    // the hierarchy only steers the search: its boxes are refit exactly every
+    // step, so rebuilding it every step or every k steps finds the same set
+    int& since = w.since_build[mi];
+    const bool rebuild = since == 0 || since >= kRebuildEvery;
+    since = rebuild ? 1 : since + 1;
+    detect_mesh_step(w, h->d.q, mtris, md.vertex_offset, md.n_vertices, md.n_triangles, md.triangle_offset, rebuild,
+                     tol, st, h->d.sync.err);
     const double mu = h->model.friction[(size_t)md.material * h->model.n_materials + md.material];
     k_pair<<<1, 1, 0, st>>>(0, w.hkey2, w.hval2, w.hbary, h->d.q, mtris, md.vertex_offset, h->d.ring_ptr,
                             h->d.ring_idx, mu, w.reg, w.reg_n, w.touched, w.n_touched, h->model.N, c, w.err, w.n_total,
