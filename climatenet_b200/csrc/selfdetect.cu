@@ -39,7 +39,7 @@ namespace pdfb {
 namespace {
 
 constexpr int kRegCap = 16;   // pairing partners remembered per vertex
-constexpr int kHitSlots = 16; // step path: pairable hits kept per vertex
+constexpr int kHitSlots = 32; // step path: candidate triangles kept per vertex
 constexpr int kRebuildEvery = 8;  // step path: hierarchy rebuilt every k steps, refit in between
 
 // Error bits of the handle's device error word set by the step path (read at
@@ -293,62 +293,73 @@ __global__ void k_refit_wide(int n, const int* __restrict__ mval, const double* 
   }
 }
 
-// Step-path traversal: both children tested at their parent; every hit that
-// survives the closest-point filter and can pair (as in mode 1 below) goes to
-// the vertex's own slots, unordered.
+// Step-path traversal, stackless: both children are tested at their parent,
+// overlapping leaf children are handled on the spot, the walk descends into
+// the first overlapping internal child and, when a subtree is done, climbs
+// through the parent links, descending into a right sibling it has not seen.
+// A candidate is a triangle whose box overlaps the vertex's query box and
+// that does not contain the vertex; candidates go to the vertex's slots,
+// unordered, and the closest-point filter runs in k_compact_hits.
 __global__ void k_traverse_slots(int nv, int nt, const double* __restrict__ q, const int* __restrict__ tris, int v0,
-                                 double tol, const WNode* __restrict__ nodes, int* __restrict__ hcount,
-                                 int* __restrict__ slot_tri, int* err) {
+                                 double tol, const WNode* __restrict__ nodes, const int* __restrict__ parent,
+                                 int* __restrict__ hcount, int* __restrict__ slot_tri, int* err) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   const double t = 1.1 * tol;
-  const double tol_sq = tol * tol;
   const double3 x = ld3(q, v0 + v);
   int count = 0;
-  auto leaf = [&](int tri) {
-    const int ia = tris[3 * tri] - v0, ib = tris[3 * tri + 1] - v0, ic = tris[3 * tri + 2] - v0;
-    if (ia == v || ib == v || ic == v) return;
-    double3 cp, w;
-    closest_point(x, ld3(q, v0 + ia), ld3(q, v0 + ib), ld3(q, v0 + ic), tol, &cp, &w);
-    const double3 dd = cp - x;
-    if (!(dot3(dd, dd) < tol_sq)) return;
-    if (w.x == 0 || w.y == 0 || w.z == 0) return;
-    if (count < kHitSlots) slot_tri[(int64_t)v * kHitSlots + count] = tri;
+  int* slots = slot_tri + (int64_t)v * kHitSlots;
+  auto candidate = [&](int tri) {
+    const int gv = v0 + v;
+    if (__ldg(tris + 3 * tri) == gv || __ldg(tris + 3 * tri + 1) == gv || __ldg(tris + 3 * tri + 2) == gv) return;
+    if (count < kHitSlots) slots[count] = tri;
     ++count;
   };
   if (nt == 1) {
     double3 tl, th;
     tri_box(ld3(q, tris[0]), ld3(q, tris[1]), ld3(q, tris[2]), &tl, &th);
-    if (box_overlap(x, t, tl, th)) leaf(0);
+    if (box_overlap(x, t, tl, th)) candidate(0);
   } else {
-    int stack[64];
-    int sp = 0;
     int node = 0;
+    int guard = 0;  // each node is entered at most once and left at most once
+    const int max_moves = 4 * nt;
+    bool down = true;
+    int from = -1;
     while (true) {
-      const WNode& nd = nodes[node];
-      double b[12];
-      for (int k = 0; k < 12; ++k) b[k] = __ldg(nd.b + k);
-      const int c0 = __ldg(nd.ch), c1 = __ldg(nd.ch + 1);
-      const bool o0 = box_overlap(x, t, make_double3(b[0], b[1], b[2]), make_double3(b[3], b[4], b[5]));
-      const bool o1 = box_overlap(x, t, make_double3(b[6], b[7], b[8]), make_double3(b[9], b[10], b[11]));
-      if (o0) {
-        if (c0 < 0)
-          leaf(~c0);
-        else
-          stack[sp++] = c0;
-      }
-      if (o1) {
-        if (c1 < 0)
-          leaf(~c1);
-        else
-          stack[sp++] = c1;
-      }
-      if (sp == 0) break;
-      if (sp > 62) {
+      if (++guard > max_moves) {
         atomicOr(err, kErrSelfStack);
         break;
       }
-      node = stack[--sp];
+      const WNode& nd = nodes[node];
+      const int c0 = __ldg(nd.ch), c1 = __ldg(nd.ch + 1);
+      int next = -1;
+      if (down) {
+        const bool o0 = box_overlap(x, t, make_double3(__ldg(nd.b), __ldg(nd.b + 1), __ldg(nd.b + 2)),
+                                    make_double3(__ldg(nd.b + 3), __ldg(nd.b + 4), __ldg(nd.b + 5)));
+        const bool o1 = box_overlap(x, t, make_double3(__ldg(nd.b + 6), __ldg(nd.b + 7), __ldg(nd.b + 8)),
+                                    make_double3(__ldg(nd.b + 9), __ldg(nd.b + 10), __ldg(nd.b + 11)));
+        if (o0 && c0 < 0) candidate(~c0);
+        if (o1 && c1 < 0) candidate(~c1);
+        if (o0 && c0 >= 0)
+          next = c0;
+        else if (o1 && c1 >= 0)
+          next = c1;
+      } else if (from == c0 && c1 >= 0 &&
+                 box_overlap(x, t, make_double3(__ldg(nd.b + 6), __ldg(nd.b + 7), __ldg(nd.b + 8)),
+                             make_double3(__ldg(nd.b + 9), __ldg(nd.b + 10), __ldg(nd.b + 11)))) {
+        next = c1;  // back from the left subtree: the right one is still to do
+      }
+      if (next >= 0) {
+        node = next;
+        down = true;
+        continue;
+      }
+      // subtree done: climb
+      const int p = __ldg(parent + node);
+      if (p < 0) break;
+      from = node;
+      node = p;
+      down = false;
     }
   }
   if (count > kHitSlots) {
@@ -358,9 +369,11 @@ __global__ void k_traverse_slots(int nv, int nt, const double* __restrict__ q, c
   hcount[v] = count;
 }
 
-// Hits in canonical (vertex, triangle) order without a global sort: vertex v
-// owns [hoff[v], hoff[v] + hcount[v]); its triangles are sorted in place and
-// the barycentric coordinates recomputed (same arithmetic as the traversal).
+// Candidates in canonical (vertex, triangle) order without a global sort:
+// vertex v owns [hoff[v], hoff[v] + hcount[v]); its triangles are sorted in
+// place, then each goes through the closest-point filter and the pairing
+// precondition of mode 1 below.  A candidate that fails them stays as a dead
+// record (key ~0) that k_pair skips.
 __global__ void k_compact_hits(int nv, const double* __restrict__ q, const int* __restrict__ tris, int v0, double tol,
                                const int* __restrict__ hcount, const int* __restrict__ hoff,
                                const int* __restrict__ slot_tri, int cap, unsigned long long* hkey, int* hval,
@@ -385,13 +398,16 @@ __global__ void k_compact_hits(int nv, const double* __restrict__ q, const int* 
     tl[j] = tv;
   }
   const double3 x = ld3(q, v0 + v);
+  const double tol_sq = tol * tol;
   for (int k = 0; k < cnt; ++k) {
     const int h = o + k;
     if (h >= cap) return;
     const int tri = tl[k];
     double3 cp, w;
     closest_point(x, ld3(q, tris[3 * tri]), ld3(q, tris[3 * tri + 1]), ld3(q, tris[3 * tri + 2]), tol, &cp, &w);
-    hkey[h] = ((unsigned long long)v << 32) | (unsigned int)tri;
+    const double3 dd = cp - x;
+    const bool hit = dot3(dd, dd) < tol_sq && w.x != 0 && w.y != 0 && w.z != 0;
+    hkey[h] = hit ? (((unsigned long long)v << 32) | (unsigned int)tri) : ~0ULL;
     hval[h] = h;
     st3(hbary, h, w);
   }
@@ -467,6 +483,7 @@ __global__ void k_pair(int n_hits, const unsigned long long* __restrict__ hkey, 
   int nt = *n_touched;
   if (n_hits_dev) n_hits = *n_hits_dev;
   for (int h = 0; h < n_hits; ++h) {
+    if (hkey[h] == ~0ULL) continue;  // dead record of the step path
     const int v = (int)(hkey[h] >> 32);
     const int tri = (int)(hkey[h] & 0xffffffffu);
     const int gv = v0 + v;
@@ -797,8 +814,8 @@ void detect_mesh_step(SelfWS& w, const double* q, const int* tris_global, int v0
     k_refit_wide<<<(nt + tb - 1) / tb, tb, 0, st>>>(nt, mval, q, tris_global, left, parent, leaf_parent, nodes,
                                                     w.s_visits + t0);
   }
-  k_traverse_slots<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, nt, q, tris_global, v0, tol, nodes, w.hcount, w.slot_tri,
-                                                      err_word);
+  k_traverse_slots<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, nt, q, tris_global, v0, tol, nodes, parent, w.hcount,
+                                                      w.slot_tri, err_word);
   size_t bytes = w.cub_bytes;
   CKS(cub::DeviceScan::ExclusiveSum(w.cub_tmp, bytes, w.hcount, w.hoff, nv, st));
   k_compact_hits<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, q, tris_global, v0, tol, w.hcount, w.hoff, w.slot_tri,
@@ -834,7 +851,7 @@ int self_detect_init(pdf_handle* h) {
       max_nt = std::max(max_nt, md.n_triangles);
       max_nv = std::max(max_nv, md.n_vertices);
     }
-    ws_alloc(*w, max_nv, max_nt, std::max(1024, 4 * max_nv), h->model.N);
+    ws_alloc(*w, max_nv, max_nt, std::max(1024, 8 * max_nv), h->model.N);
     ws_alloc_pairing(*w, h->model.N, h->model.N, h->cap_self);
     const size_t T = std::max<size_t>(1, h->model.tris.size() / 3);
     w->wnodes = salloc<WNode>(T);
