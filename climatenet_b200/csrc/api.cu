@@ -550,10 +550,10 @@ int64_t launches_per_iteration(const pdf_handle* h) {
 
 // Per step outside the iterations: predictor, obstacle flags + clamp + materialise,
 // slots (2), slot reset, finalize; self-collision: register reset, per mesh
-// bbox/keys/build/refit/traverse/compact/pair, bases, levels.
+// bbox/keys/build/refit/traverse/filter/compact/pair, bases, levels.
 int64_t launches_per_step_extra(const pdf_handle* h) {
   int64_t n = 1 + (h->obs.n > 0 ? 3 : 0) + 2 + 1 + 1;
-  if (h->prm.self_collision) n += 1 + 7 * (int64_t)h->model.meshes.size() + 1 + 1;
+  if (h->prm.self_collision) n += 1 + 8 * (int64_t)h->model.meshes.size() + 1 + 1;
   // warm start: features, forward; record (clear + accumulate [+ count])
   const bool warm = h->prm.warm_start == PDF_WARM_MLP;
   if (warm || h->log_cap > 0) n += 1 + 2 + (h->log_cap > 0 ? 1 : 0) + (warm ? 1 : 0);
@@ -966,7 +966,7 @@ int pdf_step(pdf_handle* h, int32_t nsteps, pdf_step_report* report) {
       return fail(h, PDF_CAPACITY_EXCEEDED,
                   "more self contacts than the self-contact buffer, or a vertex with more than 16 partners");
     if (derr & 8)
-      return fail(h, PDF_CAPACITY_EXCEEDED, "more than 16 self-collision hits at a vertex, or hit buffer full");
+      return fail(h, PDF_CAPACITY_EXCEEDED, "more than 32 self-collision candidates at a vertex, or hit buffer full");
     if (derr & 16) return fail(h, PDF_CAPACITY_EXCEEDED, "self-collision BVH deeper than the traversal stack");
     if (derr) return fail(h, PDF_DEVICE_TIMEOUT, "a supernodal sweep gave up waiting for a dependency");
     return PDF_OK;

@@ -299,7 +299,7 @@ __global__ void k_refit_wide(int n, const int* __restrict__ mval, const double* 
 // through the parent links, descending into a right sibling it has not seen.
 // A candidate is a triangle whose box overlaps the vertex's query box and
 // that does not contain the vertex; candidates go to the vertex's slots,
-// unordered, and the closest-point filter runs in k_compact_hits.
+// unordered, and the closest-point filter runs in k_filter_candidates.
 __global__ void k_traverse_slots(int nv, int nt, const double* __restrict__ q, const int* __restrict__ tris, int v0,
                                  double tol, const WNode* __restrict__ nodes, const int* __restrict__ parent,
                                  int* __restrict__ hcount, int* __restrict__ slot_tri, int* err) {
@@ -369,11 +369,34 @@ __global__ void k_traverse_slots(int nv, int nt, const double* __restrict__ q, c
   hcount[v] = count;
 }
 
-// Candidates in canonical (vertex, triangle) order without a global sort:
-// vertex v owns [hoff[v], hoff[v] + hcount[v]); its triangles are sorted in
-// place, then each goes through the closest-point filter and the pairing
-// precondition of mode 1 below.  A candidate that fails them stays as a dead
-// record (key ~0) that k_pair skips.
+// The closest-point filter and the pairing precondition of mode 1 below on
+// each vertex's candidates; survivors stay in the vertex's slots (in place,
+// order kept) and hcount becomes their number.
+__global__ void k_filter_candidates(int nv, const double* __restrict__ q, const int* __restrict__ tris, int v0,
+                                    double tol, int* __restrict__ hcount, int* __restrict__ slot_tri) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= nv) return;
+  const int cnt = hcount[v];
+  if (cnt == 0) return;
+  int* slots = slot_tri + (int64_t)v * kHitSlots;
+  const double3 x = ld3(q, v0 + v);
+  const double tol_sq = tol * tol;
+  int kept = 0;
+  for (int k = 0; k < cnt; ++k) {
+    const int tri = slots[k];
+    double3 cp, w;
+    closest_point(x, ld3(q, tris[3 * tri]), ld3(q, tris[3 * tri + 1]), ld3(q, tris[3 * tri + 2]), tol, &cp, &w);
+    const double3 dd = cp - x;
+    if (!(dot3(dd, dd) < tol_sq)) continue;
+    if (w.x == 0 || w.y == 0 || w.z == 0) continue;
+    slots[kept++] = tri;
+  }
+  hcount[v] = kept;
+}
+
+// Hits in canonical (vertex, triangle) order without a global sort: vertex v
+// owns [hoff[v], hoff[v] + hcount[v]); its triangles are sorted in place and
+// the barycentric coordinates recomputed (same arithmetic as the filter).
 __global__ void k_compact_hits(int nv, const double* __restrict__ q, const int* __restrict__ tris, int v0, double tol,
                                const int* __restrict__ hcount, const int* __restrict__ hoff,
                                const int* __restrict__ slot_tri, int cap, unsigned long long* hkey, int* hval,
@@ -398,16 +421,13 @@ __global__ void k_compact_hits(int nv, const double* __restrict__ q, const int* 
     tl[j] = tv;
   }
   const double3 x = ld3(q, v0 + v);
-  const double tol_sq = tol * tol;
   for (int k = 0; k < cnt; ++k) {
     const int h = o + k;
     if (h >= cap) return;
     const int tri = tl[k];
     double3 cp, w;
     closest_point(x, ld3(q, tris[3 * tri]), ld3(q, tris[3 * tri + 1]), ld3(q, tris[3 * tri + 2]), tol, &cp, &w);
-    const double3 dd = cp - x;
-    const bool hit = dot3(dd, dd) < tol_sq && w.x != 0 && w.y != 0 && w.z != 0;
-    hkey[h] = hit ? (((unsigned long long)v << 32) | (unsigned int)tri) : ~0ULL;
+    hkey[h] = ((unsigned long long)v << 32) | (unsigned int)tri;
     hval[h] = h;
     st3(hbary, h, w);
   }
@@ -483,7 +503,6 @@ __global__ void k_pair(int n_hits, const unsigned long long* __restrict__ hkey, 
   int nt = *n_touched;
   if (n_hits_dev) n_hits = *n_hits_dev;
   for (int h = 0; h < n_hits; ++h) {
-    if (hkey[h] == ~0ULL) continue;  // dead record of the step path
     const int v = (int)(hkey[h] >> 32);
     const int tri = (int)(hkey[h] & 0xffffffffu);
     const int gv = v0 + v;
@@ -816,6 +835,7 @@ void detect_mesh_step(SelfWS& w, const double* q, const int* tris_global, int v0
   }
   k_traverse_slots<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, nt, q, tris_global, v0, tol, nodes, parent, w.hcount,
                                                       w.slot_tri, err_word);
+  k_filter_candidates<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, q, tris_global, v0, tol, w.hcount, w.slot_tri);
   size_t bytes = w.cub_bytes;
   CKS(cub::DeviceScan::ExclusiveSum(w.cub_tmp, bytes, w.hcount, w.hoff, nv, st));
   k_compact_hits<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, q, tris_global, v0, tol, w.hcount, w.hoff, w.slot_tri,
