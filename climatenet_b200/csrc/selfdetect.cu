@@ -293,24 +293,27 @@ __global__ void k_refit_wide(int n, const int* __restrict__ mval, const double* 
   }
 }
 
-// Step-path traversal, stackless: both children are tested at their parent,
-// overlapping leaf children are handled on the spot, the walk descends into
-// the first overlapping internal child and, when a subtree is done, climbs
-// through the parent links, descending into a right sibling it has not seen.
-// A candidate is a triangle whose box overlaps the vertex's query box and
-// that does not contain the vertex; candidates go to the vertex's slots,
+// Step-path traversal: both children are tested at their parent (one node
+// record load), overlapping leaf children are handled on the spot, the walk
+// continues into the first overlapping internal child and keeps the other on
+// a per-thread stack in shared memory (column-major: no bank conflicts).  A
+// candidate is a triangle whose box overlaps the vertex's query box and that
+// does not contain the vertex; candidates go to the vertex's slots,
 // unordered, and the closest-point filter runs in k_filter_candidates.
-__global__ void k_traverse_slots(int nv, int nt, const double* __restrict__ q, const int* __restrict__ tris, int v0,
-                                 double tol, const WNode* __restrict__ nodes, const int* __restrict__ parent,
-                                 int* __restrict__ hcount, int* __restrict__ slot_tri, int* err) {
+constexpr int kTraverseThreads = 128, kTraverseStack = 48;
+__global__ void __launch_bounds__(kTraverseThreads)
+    k_traverse_slots(int nv, int nt, const double* __restrict__ q, const int* __restrict__ tris, int v0, double tol,
+                     const WNode* __restrict__ nodes, int* __restrict__ hcount, int* __restrict__ slot_tri,
+                     int* err) {
+  __shared__ int stack[kTraverseStack * kTraverseThreads];
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
   if (v >= nv) return;
   const double t = 1.1 * tol;
   const double3 x = ld3(q, v0 + v);
   int count = 0;
   int* slots = slot_tri + (int64_t)v * kHitSlots;
+  const int gv = v0 + v;
   auto candidate = [&](int tri) {
-    const int gv = v0 + v;
     if (__ldg(tris + 3 * tri) == gv || __ldg(tris + 3 * tri + 1) == gv || __ldg(tris + 3 * tri + 2) == gv) return;
     if (count < kHitSlots) slots[count] = tri;
     ++count;
@@ -320,46 +323,33 @@ __global__ void k_traverse_slots(int nv, int nt, const double* __restrict__ q, c
     tri_box(ld3(q, tris[0]), ld3(q, tris[1]), ld3(q, tris[2]), &tl, &th);
     if (box_overlap(x, t, tl, th)) candidate(0);
   } else {
+    int* st = stack + threadIdx.x;
+    int sp = 0;
     int node = 0;
-    int guard = 0;  // each node is entered at most once and left at most once
-    const int max_moves = 4 * nt;
-    bool down = true;
-    int from = -1;
-    while (true) {
-      if (++guard > max_moves) {
-        atomicOr(err, kErrSelfStack);
-        break;
-      }
+    while (node >= 0) {
       const WNode& nd = nodes[node];
       const int c0 = __ldg(nd.ch), c1 = __ldg(nd.ch + 1);
-      int next = -1;
-      if (down) {
-        const bool o0 = box_overlap(x, t, make_double3(__ldg(nd.b), __ldg(nd.b + 1), __ldg(nd.b + 2)),
-                                    make_double3(__ldg(nd.b + 3), __ldg(nd.b + 4), __ldg(nd.b + 5)));
-        const bool o1 = box_overlap(x, t, make_double3(__ldg(nd.b + 6), __ldg(nd.b + 7), __ldg(nd.b + 8)),
-                                    make_double3(__ldg(nd.b + 9), __ldg(nd.b + 10), __ldg(nd.b + 11)));
-        if (o0 && c0 < 0) candidate(~c0);
-        if (o1 && c1 < 0) candidate(~c1);
-        if (o0 && c0 >= 0)
-          next = c0;
-        else if (o1 && c1 >= 0)
-          next = c1;
-      } else if (from == c0 && c1 >= 0 &&
-                 box_overlap(x, t, make_double3(__ldg(nd.b + 6), __ldg(nd.b + 7), __ldg(nd.b + 8)),
-                             make_double3(__ldg(nd.b + 9), __ldg(nd.b + 10), __ldg(nd.b + 11)))) {
-        next = c1;  // back from the left subtree: the right one is still to do
+      const bool o0 = box_overlap(x, t, make_double3(__ldg(nd.b), __ldg(nd.b + 1), __ldg(nd.b + 2)),
+                                  make_double3(__ldg(nd.b + 3), __ldg(nd.b + 4), __ldg(nd.b + 5)));
+      const bool o1 = box_overlap(x, t, make_double3(__ldg(nd.b + 6), __ldg(nd.b + 7), __ldg(nd.b + 8)),
+                                  make_double3(__ldg(nd.b + 9), __ldg(nd.b + 10), __ldg(nd.b + 11)));
+      if (o0 && c0 < 0) candidate(~c0);
+      if (o1 && c1 < 0) candidate(~c1);
+      const bool d0 = o0 && c0 >= 0, d1 = o1 && c1 >= 0;
+      if (d0 && d1) {
+        if (sp >= kTraverseStack) {
+          atomicOr(err, kErrSelfStack);
+          break;
+        }
+        st[sp++ * kTraverseThreads] = c1;
+        node = c0;
+      } else if (d0) {
+        node = c0;
+      } else if (d1) {
+        node = c1;
+      } else {
+        node = sp > 0 ? st[--sp * kTraverseThreads] : -1;
       }
-      if (next >= 0) {
-        node = next;
-        down = true;
-        continue;
-      }
-      // subtree done: climb
-      const int p = __ldg(parent + node);
-      if (p < 0) break;
-      from = node;
-      node = p;
-      down = false;
     }
   }
   if (count > kHitSlots) {
@@ -833,8 +823,8 @@ void detect_mesh_step(SelfWS& w, const double* q, const int* tris_global, int v0
     k_refit_wide<<<(nt + tb - 1) / tb, tb, 0, st>>>(nt, mval, q, tris_global, left, parent, leaf_parent, nodes,
                                                     w.s_visits + t0);
   }
-  k_traverse_slots<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, nt, q, tris_global, v0, tol, nodes, parent, w.hcount,
-                                                      w.slot_tri, err_word);
+  k_traverse_slots<<<(nv + kTraverseThreads - 1) / kTraverseThreads, kTraverseThreads, 0, st>>>(
+      nv, nt, q, tris_global, v0, tol, nodes, w.hcount, w.slot_tri, err_word);
   k_filter_candidates<<<(nv + tb - 1) / tb, tb, 0, st>>>(nv, q, tris_global, v0, tol, w.hcount, w.slot_tri);
   size_t bytes = w.cub_bytes;
   CKS(cub::DeviceScan::ExclusiveSum(w.cub_tmp, bytes, w.hcount, w.hoff, nv, st));
