@@ -866,7 +866,7 @@ void free_handle(pdf_handle* h) {
                   d.c.level_order, d.c.slot_of, d.c.n_slots, d.c.slot_vertex, d.c.f, d.c.cf[0], d.c.cf[1],
                   d.c.sf[0], d.c.sf[1], d.c.c_gap, d.c.c_active, h->mlp_w, h->mlp_X, h->mlp_Y, h->rprev,
                   h->rprev_tag, h->log_X, h->log_T, h->log_n, d.iter, d.iter_total, d.blocks_done, d.stamps,
-                  d.c.ac_trace, h->gather_idx, h->gather_out};
+                  d.c.ac_trace, h->gather_idx, h->gather_out, h->stage, h->bad_dev};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto p : d.obstacle_v) cudaFree(p);
@@ -877,6 +877,7 @@ void free_handle(pdf_handle* h) {
     for (auto& e : rec.ev)
       if (e) cudaEventDestroy(e);
   if (h->ring_host) cudaFreeHost(h->ring_host);
+  if (h->bad_host) cudaFreeHost(h->bad_host);
   for (int k = 0; k < 2; ++k) {
     if (h->frame_host[k]) cudaFreeHost(h->frame_host[k]);
     if (h->frame_ev[k]) cudaEventDestroy(h->frame_ev[k]);
@@ -1069,25 +1070,45 @@ int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms_out, d
 int pdf_get_state(pdf_handle* h, double* q, double* v) {
   if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
   return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
     const size_t n = 3 * (size_t)h->dm.N * sizeof(double);
+    // ordered after the enqueued steps on the handle's stream; pinned
+    // destinations make these true asynchronous DMA copies
+    if (q) CK(cudaMemcpyAsync(q, h->d.q, n, cudaMemcpyDeviceToHost, h->stream));
+    if (v) CK(cudaMemcpyAsync(v, h->d.v, n, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    if (q) CK(cudaMemcpy(q, h->d.q, n, cudaMemcpyDeviceToHost));
-    if (v) CK(cudaMemcpy(v, h->d.v, n, cudaMemcpyDeviceToHost));
     return PDF_OK;
   });
 }
 
+// The state is uploaded to staging buffers and checked on the device; only a
+// finite state replaces the handle's (a rejected one leaves it unchanged).
 int pdf_set_state(pdf_handle* h, const double* q, const double* v) {
   if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
+  if (!q && !v) return PDF_OK;
   return guarded(h, [&]() -> int {
-    const size_t n3 = 3 * (size_t)h->dm.N;
-    for (size_t i = 0; i < n3; ++i)
-      if ((q && !std::isfinite(q[i])) || (v && !std::isfinite(v[i])))
-        return fail(h, PDF_NAN_DETECTED, "non-finite value in the state passed to pdf_set_state");
-    CK(cudaStreamSynchronize(h->stream));
+    CK(cudaSetDevice(h->prm.device));
+    cudaStream_t st = h->stream;
+    const size_t n3 = 3 * (size_t)h->dm.N, bytes = n3 * sizeof(double);
+    if (!h->stage) {
+      h->stage = dalloc<double>(2 * n3);
+      h->bad_dev = dalloc<int>(1);
+      CK(cudaHostAlloc(reinterpret_cast<void**>(&h->bad_host), sizeof(int), cudaHostAllocDefault));
+    }
     if (h->copy_stream) CK(cudaStreamSynchronize(h->copy_stream));
-    if (q) CK(cudaMemcpy(h->d.q, q, n3 * sizeof(double), cudaMemcpyHostToDevice));
-    if (v) CK(cudaMemcpy(h->d.v, v, n3 * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemsetAsync(h->bad_dev, 0, sizeof(int), st));
+    if (q) CK(cudaMemcpyAsync(h->stage, q, bytes, cudaMemcpyHostToDevice, st));
+    if (v) CK(cudaMemcpyAsync(h->stage + n3, v, bytes, cudaMemcpyHostToDevice, st));
+    const int64_t n_check = (q && v) ? 2 * (int64_t)n3 : (int64_t)n3;
+    const double* first = q ? h->stage : h->stage + n3;
+    k_check_finite<<<kStrideBlocks, kThreads, 0, st>>>(n_check, first, h->bad_dev);
+    CK(cudaGetLastError());
+    h->launches_outside += 1;
+    CK(cudaMemcpyAsync(h->bad_host, h->bad_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (*h->bad_host) return fail(h, PDF_NAN_DETECTED, "non-finite value in the state passed to pdf_set_state");
+    if (q) CK(cudaMemcpyAsync(h->d.q, h->stage, bytes, cudaMemcpyDeviceToDevice, st));
+    if (v) CK(cudaMemcpyAsync(h->d.v, h->stage + n3, bytes, cudaMemcpyDeviceToDevice, st));
     h->mlp_tag += 2;  // the previous step's contact impulses no longer apply
     return PDF_OK;
   });

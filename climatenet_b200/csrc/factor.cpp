@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <numeric>
 
 #ifdef _OPENMP
@@ -13,6 +14,9 @@
 
 namespace pdfb {
 namespace {
+
+constexpr int kNdMergeLevels = 3;   // see NDBuilder
+constexpr int kBlockedFront = 256;  // diagonal blocks this large use blocked_cholesky
 
 inline double dotn(const double* a, const double* b, int n) {
   double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
@@ -27,16 +31,30 @@ inline double dotn(const double* a, const double* b, int n) {
   return (s0 + s1) + (s2 + s3);
 }
 
+// Nested dissection.  The separators of the top `merge` levels of the
+// dissection tree are not given their own supernodes: they are deferred and
+// ordered last, as one dense root supernode (top()), which removes merge - 1
+// levels from the elimination tree the device sweeps walk level by level.
 struct NDBuilder {
   const Model& m;
   int leaf;
+  int merge;
   std::vector<int> order;           // pivot order being built
   std::vector<int> node_c0, node_n; // node columns
   std::vector<char> side;
+  std::vector<int> deferred;        // separators of depth < merge, deepest first
 
-  NDBuilder(const Model& mm, int lf) : m(mm), leaf(lf), side(mm.N, 0) { order.reserve(mm.N); }
+  NDBuilder(const Model& mm, int lf, int mg) : m(mm), leaf(lf), merge(mg), side(mm.N, 0) { order.reserve(mm.N); }
 
-  void run(std::vector<int>& ids) {
+  void top() {
+    if (deferred.empty()) return;
+    node_c0.push_back((int)order.size());
+    node_n.push_back((int)deferred.size());
+    order.insert(order.end(), deferred.begin(), deferred.end());
+    deferred.clear();
+  }
+
+  void run(std::vector<int>& ids, int depth = 0) {
     if ((int)ids.size() <= leaf) {
       if (!ids.empty()) {
         node_c0.push_back((int)order.size());
@@ -72,16 +90,59 @@ struct NDBuilder {
     for (int v : s1) side[v] = 0;
     s2.clear();
     s2.shrink_to_fit();
-    run(s1);
-    run(s2r);
+    run(s1, depth + 1);
+    run(s2r, depth + 1);
     std::sort(sep.begin(), sep.end());
-    if (!sep.empty()) {
+    if (depth < merge) {
+      deferred.insert(deferred.end(), sep.begin(), sep.end());
+    } else if (!sep.empty()) {
       node_c0.push_back((int)order.size());
       node_n.push_back((int)sep.size());
       order.insert(order.end(), sep.begin(), sep.end());
     }
   }
 };
+
+// Top dissection levels merged into the root supernode (PDF_ND_MERGE
+// overrides it for tuning experiments).
+int nd_merge_levels() {
+  if (const char* e = std::getenv("PDF_ND_MERGE")) {
+    const int v = std::atoi(e);
+    if (v >= 0 && v <= 16) return v;
+  }
+  return kNdMergeLevels;
+}
+
+// In-place Cholesky of the leading ns x ns block of the row-major front F
+// (leading dimension ld, lower triangle), blocked right-looking with the
+// trailing updates spread over the host threads; used for large diagonal
+// blocks (the merged root), where the row-by-row Crout is serial.
+bool blocked_cholesky(double* F, int ns, int ld) {
+  constexpr int B = 64;
+  for (int kb = 0; kb < ns; kb += B) {
+    const int ke = std::min(kb + B, ns);
+    for (int k = kb; k < ke; ++k) {
+      double* Fk = F + (size_t)k * ld;
+      for (int jj = kb; jj < k; ++jj)
+        Fk[jj] = (Fk[jj] - dotn(Fk + kb, F + (size_t)jj * ld + kb, jj - kb)) / F[(size_t)jj * ld + jj];
+      const double d = Fk[k] - dotn(Fk + kb, Fk + kb, k - kb);
+      if (!(d > 0.)) return false;
+      Fk[k] = std::sqrt(d);
+    }
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int i = ke; i < ns; ++i) {
+      double* Fi = F + (size_t)i * ld;
+      for (int jj = kb; jj < ke; ++jj)
+        Fi[jj] = (Fi[jj] - dotn(Fi + kb, F + (size_t)jj * ld + kb, jj - kb)) / F[(size_t)jj * ld + jj];
+    }
+#pragma omp parallel for schedule(dynamic, 8)
+    for (int i = ke; i < ns; ++i) {
+      double* Fi = F + (size_t)i * ld;
+      for (int j = ke; j <= i; ++j) Fi[j] -= dotn(Fi + kb, F + (size_t)j * ld + kb, ke - kb);
+    }
+  }
+  return true;
+}
 
 }  // namespace
 
@@ -90,11 +151,12 @@ bool factorize(const Model& m, double dt, int leaf_size, Factor& f, std::string&
   const int N = m.N;
   f.N = N;
   // ---- ordering and supernode partition -------------------------------
-  NDBuilder nd(m, std::max(8, leaf_size));
+  NDBuilder nd(m, std::max(8, leaf_size), nd_merge_levels());
   {
     std::vector<int> ids(N);
     std::iota(ids.begin(), ids.end(), 0);
     nd.run(ids);
+    nd.top();
   }
   f.perm = nd.order;
   f.iperm.assign(N, 0);
@@ -202,15 +264,23 @@ bool factorize(const Model& m, double dt, int leaf_size, Factor& f, std::string&
       std::vector<double>().swap(U[t]);
     }
     // Crout: L11 rows, then L21 rows (independent), then U = F22 - L21 L21^T
-    for (int k = 0; k < ns; ++k) {
-      double* Fk = &F[(size_t)k * mdim];
-      for (int jj = 0; jj < k; ++jj) Fk[jj] = (Fk[jj] - dotn(Fk, &F[(size_t)jj * mdim], jj)) / F[(size_t)jj * mdim + jj];
-      double d = Fk[k] - dotn(Fk, Fk, k);
-      if (!(d > 0.)) {
+    if (ns >= kBlockedFront && inner_parallel) {
+      if (!blocked_cholesky(F.data(), ns, mdim)) {
         failed = true;
         return;
       }
-      Fk[k] = std::sqrt(d);
+    } else {
+      for (int k = 0; k < ns; ++k) {
+        double* Fk = &F[(size_t)k * mdim];
+        for (int jj = 0; jj < k; ++jj)
+          Fk[jj] = (Fk[jj] - dotn(Fk, &F[(size_t)jj * mdim], jj)) / F[(size_t)jj * mdim + jj];
+        double d = Fk[k] - dotn(Fk, Fk, k);
+        if (!(d > 0.)) {
+          failed = true;
+          return;
+        }
+        Fk[k] = std::sqrt(d);
+      }
     }
 #pragma omp parallel for schedule(dynamic, 8) if (inner_parallel)
     for (int i = ns; i < mdim; ++i) {

@@ -129,6 +129,11 @@ struct pdf_handle {
   cudaEvent_t frame_ready = nullptr;
   cudaStream_t copy_stream = nullptr;
   int frame_guard = -1;
+  // state upload: device staging copies of q, v, the non-finite flag and its
+  // pinned host image
+  double* stage = nullptr;  // 6N: q then v
+  int* bad_dev = nullptr;
+  int* bad_host = nullptr;
   // log reads: device index list and gathered q, v
   int* gather_idx = nullptr;
   double* gather_out = nullptr;

@@ -77,6 +77,7 @@ struct StepOut {
 };
 __global__ void k_finalize(int n3, const double* qk, double* q, StepOut o);
 __global__ void k_gather_vertices(int n, const int* idx, const double* q, const double* v, double* out);
+__global__ void k_check_finite(int64_t n, const double* a, int* bad);
 
 // Templated kernels are launched through host wrappers defined (and
 // instantiated for float and double) next to the kernels, so that every

@@ -426,6 +426,15 @@ __global__ void k_alart_curnier(DContacts c, const double* __restrict__ v, doubl
   }
 }
 
+// Non-finite check of an uploaded state: *bad becomes non-zero if any of the
+// n values is NaN or infinite.
+__global__ void k_check_finite(int64_t n, const double* __restrict__ a, int* bad) {
+  int found = 0;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
+    found |= !isfinite(a[k]);
+  if (__any_sync(0xffffffffu, found) && (threadIdx.x & 31) == 0) atomicOr(bad, 1);
+}
+
 // Positions and velocities of listed vertices: out[0 .. 3n) = q, out[3n .. 6n) = v.
 __global__ void k_gather_vertices(int n, const int* __restrict__ idx, const double* __restrict__ q,
                                   const double* __restrict__ v, double* __restrict__ out) {
