@@ -249,12 +249,12 @@ def timed_steps(sim, steps, barrier, dist, device):
     return max_over_ranks(rep.device_ms, dist), int(s1.kernel_launches - s0.kernel_launches), clk.summary()
 
 
-def e2e_steps(sim, steps, barrier, dist, world):
+def e2e_steps(sim, steps, barrier, dist, world, start):
     """Through the C ABI with host buffers: upload (q, v) from pinned memory,
-    step, read (q, v) back, every step."""
+    step, read (q, v) back, every step, starting from the state `start`."""
     import torch
     from climatenet_b200 import native
-    q0, v0 = sim.state()
+    q0, v0 = start
     # two pinned (q, v) pairs: each step reads back into the pair the next
     # step uploads from
     bufs = [(torch.from_numpy(q0).pin_memory(), torch.from_numpy(v0).pin_memory())]
@@ -328,6 +328,7 @@ def main():
     # ---- the reference's method: FP64, 20 PD iterations per step ---------
     sim_r = make_sim(s, pk, PLAIN_ITERATIONS, "fp64", device=local)
     sim_r.step(args.warmup)
+    start_state = sim_r.state()
     ms_r, launches_r, clk_r = timed_steps(sim_r, K, barrier, dist, local)
     res_r, curve_r, _ = residual_pass(sim_r, K)
     line_extra["fp64_plain_fixed20"] = {"steps_per_s": whole_job_rate(world, K, ms_r), "ms_per_step": ms_r / K,
@@ -360,6 +361,7 @@ def main():
         for name, precision, w in arms:
             sim = make_sim(s, pk, cap, precision, w, device=local, tolerance=tol)
             sim.step(args.warmup)
+            start_state = sim.state()
             ms, launches, clk = timed_steps(sim, K, barrier, dist, local)
             res, _, mean_it = residual_pass(sim, K)
             line_extra[name] = {"steps_per_s": whole_job_rate(world, K, ms), "ms_per_step": ms / K,
@@ -375,7 +377,9 @@ def main():
                                             line_extra["fp64_plain_fixed20"]["steps_per_s"])
 
     value = whole_job_rate(world, K, ms)
-    e2e_value = e2e_steps(sim, max(3, K // 2), barrier, dist, world)
+    # end to end over the same stretch of the run as `value`: from the state
+    # the timed steps started from
+    e2e_value = e2e_steps(sim, K, barrier, dist, world, start_state)
     roof = roofline(sim, prec == "fp32")
     ms_local, bytes_local = sim.time_phase(1, reps=20)
     st = sim.stats()

@@ -146,7 +146,10 @@ class Simulation:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except TypeError:
+            pass  # interpreter shutdown: the module's globals are already gone
 
     def step(self, n=1):
         rep = abi.pdf_step_report()
