@@ -203,9 +203,10 @@ def make_sim(s, pk, iterations, precision, weights=None, device=0, tolerance=0.0
 
 
 def residual_pass(sim, steps):
-    """Over `steps` further steps: mean Alart-Curnier residual after the last
-    iteration (steps with contacts), mean per-iteration curve (fixed iteration
-    counts only) and mean iterations per step."""
+    """Over `steps` steps (a replay of the timed stretch from its start
+    state): mean Alart-Curnier residual after the last iteration (steps with
+    contacts), mean per-iteration curve (fixed iteration counts only) and mean
+    iterations per step."""
     res, curves, its = [], [], []
     for _ in range(steps):
         r = sim.step(1)
@@ -246,7 +247,8 @@ def timed_steps(sim, steps, barrier, dist, device):
         rep = sim.step(steps)
     barrier()
     s1 = sim.stats()
-    return max_over_ranks(rep.device_ms, dist), int(s1.kernel_launches - s0.kernel_launches), clk.summary()
+    return (max_over_ranks(rep.device_ms, dist), int(s1.kernel_launches - s0.kernel_launches), clk.summary(),
+            (s1.iterations - s0.iterations) / steps)
 
 
 def e2e_steps(sim, steps, barrier, dist, world, start):
@@ -329,7 +331,9 @@ def main():
     sim_r = make_sim(s, pk, PLAIN_ITERATIONS, "fp64", device=local)
     sim_r.step(args.warmup)
     start_state = sim_r.state()
-    ms_r, launches_r, clk_r = timed_steps(sim_r, K, barrier, dist, local)
+    ms_r, launches_r, clk_r, _ = timed_steps(sim_r, K, barrier, dist, local)
+    # residuals over the same stretch of the run, replayed from its start
+    sim_r.set_state(*start_state)
     res_r, curve_r, _ = residual_pass(sim_r, K)
     line_extra["fp64_plain_fixed20"] = {"steps_per_s": whole_job_rate(world, K, ms_r), "ms_per_step": ms_r / K,
                                         "pd_iterations": PLAIN_ITERATIONS, "mean_residual": res_r,
@@ -362,10 +366,12 @@ def main():
             sim = make_sim(s, pk, cap, precision, w, device=local, tolerance=tol)
             sim.step(args.warmup)
             start_state = sim.state()
-            ms, launches, clk = timed_steps(sim, K, barrier, dist, local)
+            ms, launches, clk, timed_it = timed_steps(sim, K, barrier, dist, local)
+            sim.set_state(*start_state)
             res, _, mean_it = residual_pass(sim, K)
             line_extra[name] = {"steps_per_s": whole_job_rate(world, K, ms), "ms_per_step": ms / K,
-                                "mean_pd_iterations": mean_it, "mean_residual": res, "tolerance": tol,
+                                "mean_pd_iterations": timed_it, "mean_pd_iterations_replay": mean_it,
+                                "mean_residual": res, "tolerance": tol,
                                 "iteration_cap": cap, "gpu_launches": launches}
             if name != arms[-1][0]:
                 sim.close()
