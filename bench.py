@@ -274,7 +274,13 @@ def e2e_steps(sim, steps, barrier, dist, world, start):
     return whole_job_rate(world, steps, 1e3 * max_over_ranks(time.perf_counter() - t0, dist))
 
 
-def roofline(sim, fp32):
+# DRAM bytes (read + write) of one global solve, forward + backward sweep,
+# from ncu captures of the 500 x 500 cloth (profiles/sweeps_cloth500_fp32.md,
+# profiles/sweeps_cloth500_fp64.md); None for other workloads.
+SOLVE_TRAFFIC_500 = {True: 419.2e6, False: 831.8e6}
+
+
+def roofline(sim, fp32, n=None):
     ms, by = sim.time_phase(0, reps=20)
     pk_ = peaks()
     peak = pk_["hbm_gbs"] if pk_ else 6650.0
@@ -282,7 +288,8 @@ def roofline(sim, fp32):
     achieved = by / (ms * 1e-3) / 1e9
     return {"bound": "hbm", "kernel": "supernodal forward+backward sweeps (one global solve, %s)"
             % ("FP32" if fp32 else "FP64"), "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "ms": ms, "algorithmic_bytes": by,
+            "frac": achieved / peak, "traffic": SOLVE_TRAFFIC_500[fp32] if n == 500 else None,
+            "traffic_unit": "bytes per solve (ncu)", "ms": ms, "algorithmic_bytes": by,
             "peak_source": "MEASURED_PEAKS.json hbm_gbs (measured)" if pk_ else "fallback",
             "factor_elements_stored": st.factor_nnz, "nnz_L": st.factor_nnz_true}
 
@@ -338,7 +345,7 @@ def main():
     line_extra["fp64_plain_fixed20"] = {"steps_per_s": whole_job_rate(world, K, ms_r), "ms_per_step": ms_r / K,
                                         "pd_iterations": PLAIN_ITERATIONS, "mean_residual": res_r,
                                         "residual_curve": curve_r, "gpu_launches": launches_r}
-    line_extra["roofline_fp64"] = roofline(sim_r, False)
+    line_extra["roofline_fp64"] = roofline(sim_r, False, args.n if args.workload == "cloth" else None)
     if args.arm == "fp64":
         sim, ms, launches, clk, iters, res, prec, tol = (sim_r, ms_r, launches_r, clk_r, PLAIN_ITERATIONS, res_r,
                                                         "fp64", 0.0)
@@ -386,7 +393,7 @@ def main():
     # end to end over the same stretch of the run as `value`: from the state
     # the timed steps started from
     e2e_value = e2e_steps(sim, K, barrier, dist, world, start_state)
-    roof = roofline(sim, prec == "fp32")
+    roof = roofline(sim, prec == "fp32", args.n if args.workload == "cloth" else None)
     ms_local, bytes_local = sim.time_phase(1, reps=20)
     st = sim.stats()
     if dist is not None:

@@ -55,6 +55,7 @@ struct __align__(16) WNode {
   int ch[2];
   int pad[2];
 };
+static_assert(sizeof(WNode) == 112, "WNode is read as seven 16-byte vectors");
 
 struct SelfWS {
   int max_nt = 0, max_nv = 0, hit_cap = 0;
@@ -327,12 +328,14 @@ __global__ void __launch_bounds__(kTraverseThreads)
     int sp = 0;
     int node = 0;
     while (node >= 0) {
-      const WNode& nd = nodes[node];
-      const int c0 = __ldg(nd.ch), c1 = __ldg(nd.ch + 1);
-      const bool o0 = box_overlap(x, t, make_double3(__ldg(nd.b), __ldg(nd.b + 1), __ldg(nd.b + 2)),
-                                  make_double3(__ldg(nd.b + 3), __ldg(nd.b + 4), __ldg(nd.b + 5)));
-      const bool o1 = box_overlap(x, t, make_double3(__ldg(nd.b + 6), __ldg(nd.b + 7), __ldg(nd.b + 8)),
-                                  make_double3(__ldg(nd.b + 9), __ldg(nd.b + 10), __ldg(nd.b + 11)));
+      // the 112-byte record in seven 16-byte loads
+      const double2* r = reinterpret_cast<const double2*>(nodes + node);
+      const double2 b01 = __ldg(r), b23 = __ldg(r + 1), b45 = __ldg(r + 2), b67 = __ldg(r + 3),
+                    b89 = __ldg(r + 4), b1011 = __ldg(r + 5);
+      const int4 chv = __ldg(reinterpret_cast<const int4*>(r + 6));
+      const int c0 = chv.x, c1 = chv.y;
+      const bool o0 = box_overlap(x, t, make_double3(b01.x, b01.y, b23.x), make_double3(b23.y, b45.x, b45.y));
+      const bool o1 = box_overlap(x, t, make_double3(b67.x, b67.y, b89.x), make_double3(b89.y, b1011.x, b1011.y));
       if (o0 && c0 < 0) candidate(~c0);
       if (o1 && c1 < 0) candidate(~c1);
       const bool d0 = o0 && c0 >= 0, d1 = o1 && c1 >= 0;
