@@ -1083,6 +1083,9 @@ int pdf_get_state(pdf_handle* h, double* q, double* v) {
 
 // The state is uploaded to staging buffers and checked on the device; only a
 // finite state replaces the handle's (a rejected one leaves it unchanged).
+// Uploading the state the handle already holds (a caller feeding back what it
+// read) changes nothing, so the warm start's memory of the last step's
+// contact impulses is kept; any other state invalidates it.
 int pdf_set_state(pdf_handle* h, const double* q, const double* v) {
   if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
   if (!q && !v) return PDF_OK;
@@ -1092,21 +1095,26 @@ int pdf_set_state(pdf_handle* h, const double* q, const double* v) {
     const size_t n3 = 3 * (size_t)h->dm.N, bytes = n3 * sizeof(double);
     if (!h->stage) {
       h->stage = dalloc<double>(2 * n3);
-      h->bad_dev = dalloc<int>(1);
-      CK(cudaHostAlloc(reinterpret_cast<void**>(&h->bad_host), sizeof(int), cudaHostAllocDefault));
+      h->bad_dev = dalloc<int>(2);
+      CK(cudaHostAlloc(reinterpret_cast<void**>(&h->bad_host), 2 * sizeof(int), cudaHostAllocDefault));
     }
     if (h->copy_stream) CK(cudaStreamSynchronize(h->copy_stream));
-    CK(cudaMemsetAsync(h->bad_dev, 0, sizeof(int), st));
-    if (q) CK(cudaMemcpyAsync(h->stage, q, bytes, cudaMemcpyHostToDevice, st));
-    if (v) CK(cudaMemcpyAsync(h->stage + n3, v, bytes, cudaMemcpyHostToDevice, st));
-    const int64_t n_check = (q && v) ? 2 * (int64_t)n3 : (int64_t)n3;
-    const double* first = q ? h->stage : h->stage + n3;
-    k_check_finite<<<kStrideBlocks, kThreads, 0, st>>>(n_check, first, h->bad_dev);
+    CK(cudaMemsetAsync(h->bad_dev, 0, 2 * sizeof(int), st));
+    if (q) {
+      CK(cudaMemcpyAsync(h->stage, q, bytes, cudaMemcpyHostToDevice, st));
+      k_check_state<<<kStrideBlocks, kThreads, 0, st>>>((int64_t)n3, h->stage, h->d.q, h->bad_dev);
+      h->launches_outside += 1;
+    }
+    if (v) {
+      CK(cudaMemcpyAsync(h->stage + n3, v, bytes, cudaMemcpyHostToDevice, st));
+      k_check_state<<<kStrideBlocks, kThreads, 0, st>>>((int64_t)n3, h->stage + n3, h->d.v, h->bad_dev);
+      h->launches_outside += 1;
+    }
     CK(cudaGetLastError());
-    h->launches_outside += 1;
-    CK(cudaMemcpyAsync(h->bad_host, h->bad_dev, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(h->bad_host, h->bad_dev, 2 * sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    if (*h->bad_host) return fail(h, PDF_NAN_DETECTED, "non-finite value in the state passed to pdf_set_state");
+    if (h->bad_host[0]) return fail(h, PDF_NAN_DETECTED, "non-finite value in the state passed to pdf_set_state");
+    if (!h->bad_host[1]) return PDF_OK;  // the state the handle holds already
     if (q) CK(cudaMemcpyAsync(h->d.q, h->stage, bytes, cudaMemcpyDeviceToDevice, st));
     if (v) CK(cudaMemcpyAsync(h->d.v, h->stage + n3, bytes, cudaMemcpyDeviceToDevice, st));
     h->mlp_tag += 2;  // the previous step's contact impulses no longer apply

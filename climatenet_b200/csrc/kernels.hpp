@@ -77,7 +77,7 @@ struct StepOut {
 };
 __global__ void k_finalize(int n3, const double* qk, double* q, StepOut o);
 __global__ void k_gather_vertices(int n, const int* idx, const double* q, const double* v, double* out);
-__global__ void k_check_finite(int64_t n, const double* a, int* bad);
+__global__ void k_check_state(int64_t n, const double* a, const double* cur, int* flags);
 
 // Templated kernels are launched through host wrappers defined (and
 // instantiated for float and double) next to the kernels, so that every

@@ -426,13 +426,21 @@ __global__ void k_alart_curnier(DContacts c, const double* __restrict__ v, doubl
   }
 }
 
-// Non-finite check of an uploaded state: *bad becomes non-zero if any of the
-// n values is NaN or infinite.
-__global__ void k_check_finite(int64_t n, const double* __restrict__ a, int* bad) {
-  int found = 0;
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x)
-    found |= !isfinite(a[k]);
-  if (__any_sync(0xffffffffu, found) && (threadIdx.x & 31) == 0) atomicOr(bad, 1);
+// Check of an uploaded array against the one it would replace: flags[0]
+// becomes non-zero if any of the n values is NaN or infinite, flags[1] if any
+// differs bitwise from cur.
+__global__ void k_check_state(int64_t n, const double* __restrict__ a, const double* __restrict__ cur, int* flags) {
+  int bad = 0, diff = 0;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    bad |= !isfinite(a[k]);
+    diff |= __double_as_longlong(a[k]) != __double_as_longlong(cur[k]);
+  }
+  bad = __any_sync(0xffffffffu, bad);
+  diff = __any_sync(0xffffffffu, diff);
+  if ((threadIdx.x & 31) == 0) {
+    if (bad) atomicOr(flags, 1);
+    if (diff) atomicOr(flags + 1, 1);
+  }
 }
 
 // Positions and velocities of listed vertices: out[0 .. 3n) = q, out[3n .. 6n) = v.

@@ -232,7 +232,11 @@ int pdf_create(const pdf_scene_desc* scene, const pdf_params* params,
 int pdf_step(pdf_handle* h, int32_t nsteps, pdf_step_report* report);
 
 /* State read-back / overwrite (PhysicScene::getGeneralizedPositions/Speeds,
- * src/physics/PhysicScene.cpp:233-305).  3N doubles each, either may be NULL. */
+ * src/physics/PhysicScene.cpp:233-305).  3N doubles each, either may be NULL.
+ * pdf_set_state checks the uploaded state on the device: a non-finite value
+ * is rejected (PDF_NAN_DETECTED, state unchanged); the state the handle
+ * already holds is a no-op; any other state also drops the learned warm
+ * start's memory of the last step's contact impulses. */
 int pdf_get_state(pdf_handle* h, double* q, double* v);
 int pdf_set_state(pdf_handle* h, const double* q, const double* v);
 

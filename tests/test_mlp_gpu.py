@@ -136,6 +136,34 @@ def test_warm_started_steps_match_oracle():
     assert np.abs(qg - qo).max() / np.abs(qo).max() < 1e-6
 
 
+def test_feeding_back_the_state_keeps_the_impulse_memory():
+    """pdf_set_state with the state the handle already holds changes nothing
+    (a caller that reads the state back and uploads it every step runs the
+    same steps); a different state drops the warm start's impulse memory."""
+    s = _sphere_scene()
+    p = abi.params(time_step=2e-3, iterations=6, warm_start=abi.PDF_WARM_MLP)
+    w = native.mlp_init(seed=9)
+    w[-3] = 1.0
+    a, b, c = (native.Simulation(s, p) for _ in range(3))
+    for g in (a, b, c):
+        g.mlp_set_weights(w)
+        g.step(2)
+    for _ in range(4):
+        a.step(1)
+        b.set_state(*b.state())
+        b.step(1)
+    qa, va = a.state()
+    qb, vb = b.state()
+    assert np.array_equal(qa, qb) and np.array_equal(va, vb)
+    # a changed state (one velocity component nudged) takes the other path
+    q, v = c.state()
+    v[0, 0] += 1e-9
+    c.set_state(q, v)
+    c.step(4)
+    qc, _ = c.state()
+    assert not np.array_equal(qa, qc)
+
+
 def test_contact_capacity_overflow_is_reported():
     s = _sphere_scene()
     g = native.Simulation(s, abi.params(time_step=2e-3, iterations=2, contact_capacity=4))
