@@ -154,14 +154,19 @@ def test_feeding_back_the_state_keeps_the_impulse_memory():
         b.step(1)
     qa, va = a.state()
     qb, vb = b.state()
-    assert np.array_equal(qa, qb) and np.array_equal(va, vb)
-    # a changed state (one velocity component nudged) takes the other path
+    # the sweeps accumulate with atomics, so two handles agree to rounding only
+    scale = np.abs(qa).max()
+    d_ab = np.abs(qa - qb).max() / scale
+    assert d_ab < 1e-11, d_ab
+    # a state that differs in one bit (a denormal added to one velocity) takes
+    # the other path: the first step predicts without the impulse memory
     q, v = c.state()
-    v[0, 0] += 1e-9
+    v[0, 0] += 5e-324
     c.set_state(q, v)
     c.step(4)
     qc, _ = c.state()
-    assert not np.array_equal(qa, qc)
+    d_ac = np.abs(qa - qc).max() / scale
+    assert d_ac > 1e-9 and d_ac > 100 * d_ab, (d_ac, d_ab)
 
 
 def test_contact_capacity_overflow_is_reported():
