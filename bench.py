@@ -160,12 +160,14 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def train_warm_start(args, seed=1):
+def train_warm_start(args, tolerance, candidates=4):
     """Untimed: contacts logged from a cold run with 60 PD iterations (forces
     close to converged) of a sibling of the measured scene (same cloth and
     sphere; friction 0.4 instead of 0.5, rotation reversed, 8 mm instead of
-    5 mm above the sphere), and the network trained on the GPU.  For the batch
-    workload: the batch scene itself."""
+    5 mm above the sphere), `candidates` networks trained on the GPU (seeds
+    1..candidates), and the one needing the fewest PD iterations to reach
+    `tolerance` on the next 10 steps of the sibling scene (not in the training
+    data) kept.  For the batch workload: the batch scene itself."""
     from climatenet_b200 import abi, scenes, warmstart
     if args.workload == "batch":
         s, _, pk = scenes.batch_scene(n_instances=64, seed=4)
@@ -178,11 +180,21 @@ def train_warm_start(args, seed=1):
     pk = dict(pk)
     pk["iterations"] = 60
     t0 = time.time()
-    X, T = warmstart.collect(s, abi.params(**pk), steps=steps, capacity=8_000_000)
+    X, T, end_state = warmstart.collect(s, abi.params(**pk), steps=steps, capacity=8_000_000, return_state=True)
     t1 = time.time()
-    w, info = warmstart.train(X, T, epochs=40, batch=4096, lr=2e-3, seed=seed)
-    info.update(collect_s=t1 - t0, train_s=time.time() - t1,
-                data="%s, %d steps, 60 PD iterations, cold start" % (what, steps))
+    trained = [warmstart.train(X, T, epochs=40, batch=4096, lr=2e-3, seed=seed)
+               for seed in range(1, candidates + 1)]
+    t2 = time.time()
+    pv = dict(pk)
+    pv["precision"] = abi.PDF_FP32_REFINE
+    best, stats = warmstart.select(s, pv, [w for w, _ in trained], tolerance, end_state, steps=10,
+                                   cap=3 * PLAIN_ITERATIONS)
+    w, info = trained[best]
+    info.update(collect_s=t1 - t0, train_s=t2 - t1, select_s=time.time() - t2, chosen_seed=best + 1,
+                candidates=[dict(seed=k + 1, val_loss=trained[k][1]["val_loss"], **stats[k])
+                            for k in range(candidates)],
+                data="%s, %d steps, 60 PD iterations, cold start; selection on its next 10 steps"
+                     % (what, steps))
     return w, info
 
 
@@ -358,7 +370,7 @@ def main():
         arms = [("fp64_plain", "fp64", None), ("fp32_refine", "fp32", None)]
         if args.arm == "same-residual":
             from climatenet_b200 import abi, warmstart
-            weights, tinfo = train_warm_start(args)
+            weights, tinfo = train_warm_start(args, tol)
             line_extra["warm_start_training"] = tinfo
             # the cold-start solver judges the learned warm start on a short
             # stretch of the workload and is the fallback when it does not help

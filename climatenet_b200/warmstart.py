@@ -60,15 +60,44 @@ def fold(w, mu, sigma, nu, tau):
     return pack({"W1": W1, "b1": b1, "W2": p["W2"], "b2": p["b2"], "W3": W3, "b3": b3})
 
 
-def collect(scene, params, steps, capacity=None):
-    """Cold-start run of `steps` steps logging every obstacle contact."""
+def collect(scene, params, steps, capacity=None, return_state=False):
+    """Cold-start run of `steps` steps logging every obstacle contact; with
+    return_state, also the state (q, v) the run ends in."""
     sim = native.Simulation(scene, params)
     sim.mlp_log(capacity or 4_000_000)
     for _ in range(steps):
         sim.step(1)
     X, T = sim.mlp_samples()
+    state = sim.state() if return_state else None
     sim.close()
-    return X, T
+    return (X, T, state) if return_state else (X, T)
+
+
+def select(scene, params, candidates, tolerance, start, steps=10, cap=60):
+    """Picks among trained weight sets on a validation stretch: each candidate
+    drives `steps` iterate-to-tolerance steps from the state `start` (q, v)
+    of `scene`, a stretch its training data did not contain.  Returns (index
+    of the candidate with the fewest mean PD iterations, lower mean residual
+    on ties; per-candidate stats)."""
+    p = dict(params)
+    p.update(iterations=cap, residual_tolerance=tolerance, warm_start=abi.PDF_WARM_MLP)
+    sim = native.Simulation(scene, abi.params(**p))
+    stats = []
+    for w in candidates:
+        sim.mlp_set_weights(w)
+        sim.set_state(*start)  # also drops the impulse memory of the previous candidate
+        its, res = [], []
+        for _ in range(steps):
+            r = sim.step(1)
+            its.append(r.iterations)
+            if r.n_contacts + r.n_self_contacts > 0:
+                res.append(r.residual)
+        stats.append({"mean_pd_iterations": float(np.mean(its)),
+                      "mean_residual": float(np.mean(res)) if res else 0.0})
+    sim.close()
+    best = min(range(len(candidates)),
+               key=lambda k: (stats[k]["mean_pd_iterations"], stats[k]["mean_residual"]))
+    return best, stats
 
 
 def train(X, T, epochs=30, batch=4096, lr=2e-3, seed=0, device=0):
