@@ -203,7 +203,12 @@ def train_warm_start(args, tolerance, candidates=4):
         vsim.close()
     best, stats = warmstart.select(val_scene, pv, [w for w, _ in trained], tolerance, start, steps=10,
                                    cap=3 * PLAIN_ITERATIONS)
+    cold = warmstart.cold_stretch(val_scene, pv, tolerance, start, steps=10, cap=3 * PLAIN_ITERATIONS)
     w, info = trained[best]
+    # a network that does not beat the cold start on the validation stretch
+    # is not offered to the judge
+    info["validation_cold"] = cold
+    info["beats_cold_on_validation"] = stats[best]["mean_pd_iterations"] < cold["mean_pd_iterations"]
     info.update(collect_s=t1 - t0, train_s=t2 - t1, select_s=time.time() - t2, chosen_seed=best + 1,
                 candidates=[dict(seed=k + 1, val_loss=trained[k][1]["val_loss"], **stats[k])
                             for k in range(candidates)],
@@ -392,6 +397,7 @@ def main():
             pj = dict(pk)
             pj["precision"] = abi.PDF_FP32_REFINE
             verdict = warmstart.judge(s, pj, weights, tol, steps=10, warmup=args.warmup, cap=cap)
+            verdict["use"] = bool(verdict["use"] and tinfo["beats_cold_on_validation"])
             line_extra["warm_start_judge"] = verdict
             if not verdict["use"]:
                 weights = None

@@ -100,6 +100,23 @@ def select(scene, params, candidates, tolerance, start, steps=10, cap=60):
     return best, stats
 
 
+def cold_stretch(scene, params, tolerance, start, steps=10, cap=60):
+    """The cold-start solver on the stretch `select` uses: mean PD iterations
+    and mean residual over `steps` iterate-to-tolerance steps from `start`."""
+    p = dict(params)
+    p.update(iterations=cap, residual_tolerance=tolerance, warm_start=abi.PDF_WARM_NONE)
+    sim = native.Simulation(scene, abi.params(**p))
+    sim.set_state(*start)
+    its, res = [], []
+    for _ in range(steps):
+        r = sim.step(1)
+        its.append(r.iterations)
+        if r.n_contacts + r.n_self_contacts > 0:
+            res.append(r.residual)
+    sim.close()
+    return {"mean_pd_iterations": float(np.mean(its)), "mean_residual": float(np.mean(res)) if res else 0.0}
+
+
 def train(X, T, epochs=30, batch=4096, lr=2e-3, seed=0, device=0):
     """Weights (raw features in, raw forces out) and the losses, trained on the GPU.
 
