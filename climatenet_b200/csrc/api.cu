@@ -291,6 +291,22 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   d.vmesh = upload(m.vmesh);
   h->obs.o = d.obstacles;
   h->obs.vmesh = d.vmesh;
+  d.ob_best = dalloc<int>(std::max<size_t>(1, (size_t)h->obs.n * N));
+  h->obs.best = d.ob_best;
+  // mesh obstacles: LBVH over their triangles (a moving mesh's over its
+  // current mesh, refit every step)
+  h->mesh_bvh.assign(h->obs.n, nullptr);
+  h->bvh_since.assign(h->obs.n, 1);
+  for (int k = 0; k < h->obs.n; ++k) {
+    DObstacle& ob = h->host_obs[k];
+    if (ob.type != PDF_OBSTACLE_MESH && ob.type != PDF_OBSTACLE_MOVING_MESH) continue;
+    const int nvo = (int)(ob.type == PDF_OBSTACLE_MOVING_MESH ? h->moving[k].n_vertices
+                                                              : m.obstacle_vertices[k].size() / 3);
+    h->mesh_bvh[k] = mesh_bvh_create(nvo, ob.n_tri);
+    mesh_bvh_build(h->mesh_bvh[k], ob.mv, ob.mt, h->stream);
+    ob.bvh = mesh_bvh_nodes(h->mesh_bvh[k]);
+  }
+  CK(cudaStreamSynchronize(h->stream));
   // state
   d.q = upload(m.q0);
   d.v = upload(m.v0);
@@ -788,6 +804,18 @@ void step_once(pdf_handle* h, bool want_report) {
       launch_moving_mesh_lerp(st, (int)nv3, mc.frames + nv3 * (mc.next - 1), mc.frames + nv3 * mc.next,
                               (mc.clock - t0) / (t1 - t0), mc.cur);
       h->launches_outside += 1;
+      // its hierarchy follows: refit every step, rebuilt every 8
+      const size_t k = &mc - h->moving.data();
+      if (h->mesh_bvh[k]) {
+        if (++h->bvh_since[k] > 8) {
+          mesh_bvh_build(h->mesh_bvh[k], mc.cur, h->host_obs[k].mt, st);
+          h->bvh_since[k] = 1;
+          h->launches_outside += 4;
+        } else {
+          mesh_bvh_refit(h->mesh_bvh[k], mc.cur, h->host_obs[k].mt, st);
+          h->launches_outside += 1;
+        }
+      }
     }
   }
   h->time += dt;
@@ -866,10 +894,11 @@ void free_handle(pdf_handle* h) {
                   d.c.level_order, d.c.slot_of, d.c.n_slots, d.c.slot_vertex, d.c.f, d.c.cf[0], d.c.cf[1],
                   d.c.sf[0], d.c.sf[1], d.c.c_gap, d.c.c_active, h->mlp_w, h->mlp_X, h->mlp_Y, h->rprev,
                   h->rprev_tag, h->log_X, h->log_T, h->log_n, d.iter, d.iter_total, d.blocks_done, d.stamps,
-                  d.c.ac_trace, h->gather_idx, h->gather_out, h->stage, h->bad_dev};
+                  d.c.ac_trace, h->gather_idx, h->gather_out, h->stage, h->bad_dev, d.ob_best};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto p : d.obstacle_v) cudaFree(p);
+  for (auto b : h->mesh_bvh) mesh_bvh_free(b);
   for (auto p : d.obstacle_t) cudaFree(p);
   for (auto& e : h->ev)
     if (e) cudaEventDestroy(e);

@@ -5,10 +5,14 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cub/cub.cuh>
+#include <stdexcept>
+#include <string>
 
 #include "device.cuh"
 #include "geometry.cuh"
 #include "kernels.hpp"
+#include "lbvh.cuh"
 
 namespace pdfb {
 
@@ -45,6 +49,134 @@ __device__ __forceinline__ void box_side(double3 r, const DObstacle& ob, int* ax
   *dist = best;
 }
 
+// Closest kept triangle of a mesh obstacle through its LBVH: the same
+// candidates (closed box test with half-width 1.1 tol), filter and ranking as
+// mesh_obstacle_closest's scan in triangle order, which keeps the first of
+// equal distances: here ties go to the lower triangle index.  Returns the
+// triangle, or -1 when none is within tol.
+__device__ int mesh_obstacle_bvh(double3 x, const double* mv, const int* mt, const WNode* nodes, double tol) {
+  const double t = 1.1 * tol, tol_sq = tol * tol;
+  double best = __longlong_as_double(0x7ff0000000000000LL);  // +inf
+  int bt = -1;
+  int stack[64];
+  int sp = 0;
+  int node = 0;
+  while (node >= 0) {
+    const double2* r = reinterpret_cast<const double2*>(nodes + node);
+    const double2 b01 = __ldg(r), b23 = __ldg(r + 1), b45 = __ldg(r + 2), b67 = __ldg(r + 3), b89 = __ldg(r + 4),
+                  b1011 = __ldg(r + 5);
+    const int4 chv = __ldg(reinterpret_cast<const int4*>(r + 6));
+    const int ch[2] = {chv.x, chv.y};
+    const bool ov[2] = {box_overlap(x, t, make_double3(b01.x, b01.y, b23.x), make_double3(b23.y, b45.x, b45.y)),
+                        box_overlap(x, t, make_double3(b67.x, b67.y, b89.x), make_double3(b89.y, b1011.x, b1011.y))};
+    int next = -1;
+    for (int c = 0; c < 2; ++c) {
+      if (!ov[c]) continue;
+      if (ch[c] < 0) {
+        const int k = ~ch[c];
+        const double3 a = ld3(mv, mt[3 * k]), b = ld3(mv, mt[3 * k + 1]), cc = ld3(mv, mt[3 * k + 2]);
+        double3 cp, w;
+        closest_point(x, a, b, cc, tol, &cp, &w);
+        const double3 dd = cp - x;
+        if (!(dot3(dd, dd) < tol_sq)) continue;
+        const double3 e = tri_point(a, b, cc, w) - x;
+        const double d2 = dot3(e, e);
+        if (d2 < best || (d2 == best && k < bt)) {
+          best = d2;
+          bt = k;
+        }
+      } else if (next < 0) {
+        next = ch[c];
+      } else if (sp < 64) {
+        stack[sp++] = ch[c];
+      } else {
+        return -2;  // deeper than the stack: the caller falls back to the scan
+      }
+    }
+    node = next >= 0 ? next : (sp > 0 ? stack[--sp] : -1);
+  }
+  return best < tol_sq ? bt : -1;
+}
+
+struct MeshBVH {
+  int nv = 0, nt = 0;
+  int *mval = nullptr, *mval_in = nullptr, *left = nullptr, *right = nullptr, *parent = nullptr,
+      *leaf_parent = nullptr, *visits = nullptr;
+  unsigned long long *keys = nullptr, *keys_sorted = nullptr, *bbox = nullptr;
+  double *tlo = nullptr, *thi = nullptr;
+  WNode* nodes = nullptr;
+  void* cub_tmp = nullptr;
+  size_t cub_bytes = 0;
+};
+
+namespace {
+template <typename T>
+T* balloc(size_t n) {
+  T* p = nullptr;
+  const cudaError_t e = cudaMalloc((void**)&p, std::max<size_t>(1, n) * sizeof(T));
+  if (e != cudaSuccess) throw std::runtime_error(std::string("mesh obstacle BVH: ") + cudaGetErrorString(e));
+  return p;
+}
+void bck(cudaError_t e) {
+  if (e != cudaSuccess) throw std::runtime_error(std::string("mesh obstacle BVH: ") + cudaGetErrorString(e));
+}
+}  // namespace
+
+MeshBVH* mesh_bvh_create(int nv, int nt) {
+  MeshBVH* b = new MeshBVH();
+  b->nv = nv;
+  b->nt = nt;
+  b->mval = balloc<int>(nt);
+  b->mval_in = balloc<int>(nt);
+  b->left = balloc<int>(nt);
+  b->right = balloc<int>(nt);
+  b->parent = balloc<int>(nt);
+  b->leaf_parent = balloc<int>(nt);
+  b->visits = balloc<int>(nt);
+  b->keys = balloc<unsigned long long>(nt);
+  b->keys_sorted = balloc<unsigned long long>(nt);
+  b->bbox = balloc<unsigned long long>(6);
+  b->tlo = balloc<double>(3 * (size_t)nt);
+  b->thi = balloc<double>(3 * (size_t)nt);
+  b->nodes = balloc<WNode>(nt);
+  bck(cub::DeviceRadixSort::SortPairs(nullptr, b->cub_bytes, b->keys, b->keys_sorted, b->mval_in, b->mval, nt));
+  b->cub_tmp = balloc<char>(b->cub_bytes);
+  return b;
+}
+
+void mesh_bvh_refit(MeshBVH* b, const double* verts, const int* tris, cudaStream_t st) {
+  const int nt = b->nt, tb = 256;
+  if (nt < 2) return;
+  bck(cudaMemsetAsync(b->visits, 0, sizeof(int) * nt, st));
+  k_refit_wide<<<(nt + tb - 1) / tb, tb, 0, st>>>(nt, b->mval, verts, tris, b->left, b->parent, b->leaf_parent,
+                                                  b->nodes, b->visits);
+}
+
+void mesh_bvh_build(MeshBVH* b, const double* verts, const int* tris, cudaStream_t st) {
+  const int nt = b->nt, nv = b->nv, tb = 256;
+  if (nt < 2) return;
+  const unsigned long long init[6] = {~0ULL, ~0ULL, ~0ULL, 0ULL, 0ULL, 0ULL};
+  bck(cudaMemcpyAsync(b->bbox, init, sizeof(init), cudaMemcpyHostToDevice, st));
+  k_bbox<<<std::min(1024, (nv + tb - 1) / tb), tb, 0, st>>>(nv, verts, b->bbox);
+  k_tri_keys<<<(nt + tb - 1) / tb, tb, 0, st>>>(nt, verts, tris, 0, b->bbox, b->tlo, b->thi, b->keys, b->mval_in);
+  size_t bytes = b->cub_bytes;
+  bck(cub::DeviceRadixSort::SortPairs(b->cub_tmp, bytes, b->keys, b->keys_sorted, b->mval_in, b->mval, nt, 32, 62,
+                                      st));
+  k_build<<<(nt - 1 + tb - 1) / tb, tb, 0, st>>>(nt, b->keys_sorted, b->left, b->right, b->parent, b->leaf_parent);
+  mesh_bvh_refit(b, verts, tris, st);
+}
+
+const void* mesh_bvh_nodes(const MeshBVH* b) { return b->nt >= 2 ? b->nodes : nullptr; }
+
+void mesh_bvh_free(MeshBVH* b) {
+  if (!b) return;
+  void* ptrs[] = {b->mval, b->mval_in, b->left, b->right, b->parent, b->leaf_parent, b->visits, b->keys,
+                  b->keys_sorted, b->bbox, b->tlo, b->thi, b->nodes, b->cub_tmp};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  delete b;
+}
+
 // Per (obstacle, vertex) flag, obstacle-major so that a stable compaction gives
 // the reference's order (obstacles in scene order, vertices ascending:
 // PhysicScene::getCollisionsInfoExceptFor PhysicScene.cpp:115-181 and
@@ -70,9 +202,14 @@ __global__ void k_obstacle_flags(int N, const double* __restrict__ q, DObstacles
     } else if (ob.type == 4) {
       hit = box_inside(x, ob);
     } else {
-      int tri;
-      double3 cp;
-      hit = mesh_obstacle_closest(x, ob.mv, ob.mt, ob.n_tri, ob.tol, &tri, &cp);
+      int tri = -2;
+      if (ob.bvh) tri = mesh_obstacle_bvh(x, ob.mv, ob.mt, static_cast<const WNode*>(ob.bvh), ob.tol);
+      if (tri == -2) {  // no hierarchy (one triangle) or a walk deeper than the stack: scan
+        double3 cp;
+        if (!mesh_obstacle_closest(x, ob.mv, ob.mt, ob.n_tri, ob.tol, &tri, &cp)) tri = -1;
+      }
+      hit = tri >= 0;
+      obs.best[(int64_t)o * N + i] = tri;
     }
     flags[(int64_t)o * N + i] = hit ? 1 : 0;
   }
@@ -148,11 +285,14 @@ __global__ void k_obstacle_materialize(int N, const double* __restrict__ q, DObs
       nrm = make_double3(axis == 0 ? sign : 0., axis == 1 ? sign : 0., axis == 2 ? sign : 0.);
       gap = -dist;
     } else {
-      int tri;
-      double3 cp, w;
-      mesh_obstacle_closest(x, ob.mv, ob.mt, ob.n_tri, ob.tol, &tri, &cp, &w);
+      // the triangle k_obstacle_flags chose; its closest point again (the
+      // contact point is the barycentric point, as in the ranking)
+      const int tri = obs.best[idx[k]];
       const int i0 = ob.mt[3 * tri], i1 = ob.mt[3 * tri + 1], i2 = ob.mt[3 * tri + 2];
       const double3 a = ld3(ob.mv, i0), b = ld3(ob.mv, i1), cc = ld3(ob.mv, i2);
+      double3 cp0, w;
+      closest_point(x, a, b, cc, ob.tol, &cp0, &w);
+      const double3 cp = tri_point(a, b, cc, w);
       nrm = normalized3(cross3(b - a, cc - a));  // Mesh::getTriangleNormal Mesh.cpp:120-126
       gap = dot3(x - cp, nrm);
       if (ob.type == 5 && ob.moving) {

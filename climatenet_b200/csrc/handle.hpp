@@ -28,6 +28,7 @@ struct DeviceBuffers {
   std::vector<int*> obstacle_t;
   DObstacle* obstacles = nullptr;
   int* vmesh = nullptr;
+  int* ob_best = nullptr;  // per (obstacle, vertex): closest mesh-obstacle triangle
   // state
   double *q = nullptr, *v = nullptr, *tn = nullptr, *qk = nullptr, *cstep = nullptr, *bp = nullptr;
   // solve
@@ -103,6 +104,8 @@ struct pdf_handle {
   pdfb::DObstacles obs{};
   std::vector<pdfb::DObstacle> host_obs;
   std::vector<MovingClock> moving;  // one per obstacle (n_frames = 0: not moving)
+  std::vector<pdfb::MeshBVH*> mesh_bvh;  // one per obstacle (null: not a mesh obstacle)
+  std::vector<int> bvh_since;           // moving meshes: steps since the hierarchy was built
   cudaStream_t stream = nullptr;
   cudaEvent_t ev[8] = {};
   cudaGraphExec_t graph = nullptr;

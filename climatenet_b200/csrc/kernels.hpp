@@ -36,12 +36,24 @@ struct DObstacle {
   const double* fnext;
   double frame_dt;
   int moving;
+  const void* bvh;  // mesh obstacles: LBVH node records over mv / mt (null: scan every triangle)
 };
 struct DObstacles {
   int n;
   const DObstacle* o;
   const int* vmesh;  // containing mesh of every vertex
+  int* best;         // per (obstacle, vertex), obstacle-major: closest mesh-obstacle triangle, -1 if none
 };
+
+// LBVH over a mesh obstacle's triangles (lbvh.cuh), kept on the device: built
+// once (static mesh) or rebuilt every few steps and refit every step (moving
+// mesh).  Host-side handle; the node records go to DObstacle::bvh.
+struct MeshBVH;
+MeshBVH* mesh_bvh_create(int nv, int nt);
+void mesh_bvh_build(MeshBVH* b, const double* verts, const int* tris, cudaStream_t st);
+void mesh_bvh_refit(MeshBVH* b, const double* verts, const int* tris, cudaStream_t st);
+const void* mesh_bvh_nodes(const MeshBVH* b);
+void mesh_bvh_free(MeshBVH* b);
 
 __global__ void k_step_init(DModel m, const double* q, double* v, double* tn, double* qk, double* cstep, double gx,
                             double gy, double gz, double dt);

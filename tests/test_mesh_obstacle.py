@@ -1,0 +1,73 @@
+"""Mesh obstacles with many triangles, where the device walks an LBVH over the
+obstacle instead of scanning every triangle: the contact sets, normals and
+states must still equal the oracle's triangle-order scan
+(StaticMesh.cpp:33-56, MovingMesh.cpp:164-249, checkMeshCollision
+geometry_util.cpp:32-92)."""
+import numpy as np
+import pytest
+
+from climatenet_b200 import abi, native, scenes
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+
+
+def uv_sphere(radius, n_lat=24, n_lon=48, center=(0.0, 0.0, 0.0)):
+    """Closed UV sphere, triangles counter-clockwise seen from outside."""
+    verts = [(0.0, 0.0, radius)]
+    for i in range(1, n_lat):
+        th = np.pi * i / n_lat
+        for j in range(n_lon):
+            ph = 2 * np.pi * j / n_lon
+            verts.append((radius * np.sin(th) * np.cos(ph), radius * np.sin(th) * np.sin(ph), radius * np.cos(th)))
+    verts.append((0.0, 0.0, -radius))
+    v = np.array(verts) + np.asarray(center)
+    tris = []
+    ring = lambda i, j: 1 + (i - 1) * n_lon + (j % n_lon)
+    for j in range(n_lon):
+        tris.append((0, ring(1, j), ring(1, j + 1)))
+    for i in range(1, n_lat - 1):
+        for j in range(n_lon):
+            a, b, c, d = ring(i, j), ring(i, j + 1), ring(i + 1, j), ring(i + 1, j + 1)
+            tris.append((a, c, d))
+            tris.append((a, d, b))
+    south = len(verts) - 1
+    for j in range(n_lon):
+        tris.append((south, ring(n_lat - 1, j + 1), ring(n_lat - 1, j)))
+    return v, np.array(tris, dtype=np.int32)
+
+
+def cloth_over_mesh_sphere(moving=False):
+    pos, tri = scenes.grid_mesh(24, 1.0, z=0.003)
+    s = scenes.Scene(friction=((0.3,),))
+    s.add_mesh(pos, tri, area_density=0.1, bending=1e-2, stretching=1e3)
+    v, t = uv_sphere(0.5, center=(0.0, 0.0, -0.5))
+    if moving:
+        frames = np.stack([v + np.array([0.002 * f, 0.0, 0.001 * f]) for f in range(4)])
+        s.add_moving_mesh(frames, t, 4e-3, 0.01)
+    else:
+        s.add_mesh_obstacle(v, t, 0.01)
+    return s, len(t)
+
+
+@pytest.mark.parametrize("moving", [False, True])
+def test_mesh_sphere_obstacle_matches_oracle(moving):
+    s, nt = cloth_over_mesh_sphere(moving)
+    assert nt > 2000
+    p = abi.params(time_step=2e-3, iterations=15)
+    g = native.Simulation(s, p)
+    o = orc.Oracle(s, p)
+    moved = False
+    for _ in range(10):
+        rg = g.step(1)
+        ro = o.step(1)
+        assert rg.n_contacts == ro.n_contacts
+        cg, co = g.contacts(), o.contacts()
+        assert np.array_equal(cg["vertex"], co["vertex"])
+        assert np.array_equal(cg["normal"], co["normal"])
+        assert np.allclose(cg["speed"], co["speed"], rtol=0, atol=1e-12)
+        moved |= bool(np.abs(co["speed"]).max() > 0)
+    assert rg.n_contacts >= 10 and moved == moving
+    qg, vg = g.state()
+    qo, vo = o.state()
+    assert np.abs(qg - qo).max() / np.abs(qo).max() < 1e-6
