@@ -38,7 +38,10 @@ def uv_sphere(radius, n_lat=24, n_lon=48, center=(0.0, 0.0, 0.0)):
 
 
 def cloth_over_mesh_sphere(moving=False):
-    pos, tri = scenes.grid_mesh(24, 1.0, z=0.003)
+    # the grid is shifted off the sphere's meridian planes: a vertex right
+    # above an edge between two facets is at equal distance from both, and
+    # which one wins then hangs on the last bit of its position
+    pos, tri = scenes.grid_mesh(24, 1.0, z=0.003, center=(0.01234, 0.00567))
     s = scenes.Scene(friction=((0.3,),))
     s.add_mesh(pos, tri, area_density=0.1, bending=1e-2, stretching=1e3)
     v, t = uv_sphere(0.5, center=(0.0, 0.0, -0.5))
