@@ -386,7 +386,9 @@ def main():
         # ---- same residual: every arm iterates to tau (the mean residual the
         # reference's method reaches after 20 iterations), cap 60 -----------
         tol = res_r
-        cap = 3 * PLAIN_ITERATIONS
+        # no contact in the stretch (tau = 0): no residual to reach, so the
+        # arms run the reference's 20 iterations
+        cap = 3 * PLAIN_ITERATIONS if tol > 0 else PLAIN_ITERATIONS
         arms = [("fp64_plain", "fp64", None), ("fp32_refine", "fp32", None)]
         if args.arm == "same-residual":
             from climatenet_b200 import abi, warmstart
