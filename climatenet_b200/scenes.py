@@ -208,7 +208,9 @@ def cloth_on_sphere(n=30, side=1.0, z=0.0, layers=1, spacing=0.005, area_density
 
 
 def workload(cfg, n_override=None):
-    """The five benchmark shapes (sizes as named)."""
+    """The benchmark shapes: (scene, step parameters, step count) of the 30 x 30
+    pinned cloth (1), three stacked 128 x 128 layers (2), the 500 x 500 cloth on
+    the rotating sphere (3) and two 256 x 256 layers on a rotating sphere (5)."""
     if cfg == 1:
         n = n_override or 30
         s = cloth_on_sphere(n=n, side=1.0, z=0.0, mu=0.3, sphere_center=(0, 0, -0.5),

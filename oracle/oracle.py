@@ -37,6 +37,10 @@ def lib():
         L.orc_get_self_levels.argtypes = [vp, C.c_void_p, C.c_int32, C.c_void_p, C.c_int32,
                                           C.POINTER(C.c_int32)]
         L.orc_get_residual_history.argtypes = [vp, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]
+        L.orc_trace_alart_curnier.argtypes = [vp, C.c_int32]
+        L.orc_get_residual_applied_history.argtypes = [vp, C.c_void_p, C.c_int32, C.POINTER(C.c_int32)]
+        L.orc_get_alart_curnier_trace.argtypes = [vp, C.c_void_p, C.c_int64, C.POINTER(C.c_int32),
+                                                  C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.orc_get_sizes.argtypes = [vp, C.c_void_p]
         L.orc_projections.argtypes = [vp, C.c_void_p, C.c_void_p]
         L.orc_rhs_base.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -108,6 +112,29 @@ class Oracle:
         qa = None if q is None else np.ascontiguousarray(q, dtype=np.float64)
         va = None if v is None else np.ascontiguousarray(v, dtype=np.float64)
         lib().orc_set_state(self.h, None if qa is None else _ptr(qa), None if va is None else _ptr(va))
+
+    def residual_applied_history(self):
+        """Per iteration of the last step: mean AC norm with the force each
+        contact applied (zero after a take-off)."""
+        n = C.c_int32()
+        lib().orc_get_residual_applied_history(self.h, None, 0, C.byref(n))
+        out = np.zeros(max(1, n.value))
+        lib().orc_get_residual_applied_history(self.h, _ptr(out), n.value, C.byref(n))
+        return out[:n.value]
+
+    def trace_alart_curnier(self, enable=True):
+        lib().orc_trace_alart_curnier(self.h, 1 if enable else 0)
+
+    def alart_curnier_trace(self):
+        """Per-iteration (tangential, |normal|) AC norms of the last step's
+        contacts: array (iterations, contacts + self contacts, 2), and the
+        obstacle-contact count (the layout of the product's trace)."""
+        it, nc, ns = C.c_int32(), C.c_int32(), C.c_int32()
+        lib().orc_get_alart_curnier_trace(self.h, None, 0, C.byref(it), C.byref(nc), C.byref(ns))
+        out = np.zeros((it.value, nc.value + ns.value, 2))
+        lib().orc_get_alart_curnier_trace(self.h, _ptr(out), out.size, C.byref(it), C.byref(nc),
+                                          C.byref(ns))
+        return out, nc.value
 
     def contacts(self):
         n = C.c_int32()

@@ -655,6 +655,12 @@ struct Sim {
   std::vector<double> contact_forces[2], self_forces[2];
   int cur = 0, nxt = 1;
   std::vector<double> residual_hist;
+  /* per-iteration (tangential, |normal|) Alart-Curnier norms of every contact
+   * of the last step, obstacle contacts first (the PRINT_ALART_CURNIER_ERROR
+   * output of SFE:720-752) */
+  bool trace_ac = false;
+  std::vector<double> ac_trace;
+  int trace_nc = 0, trace_ns = 0;
   pdf_step_report last{};
   std::vector<double> tmpx;
 
@@ -662,6 +668,11 @@ struct Sim {
   std::vector<float> mlp_w;
   bool mlp_ready = false;
   std::vector<char> c_active;   /* last projection of the contact was not a take-off */
+  std::vector<char> s_active;   /* same for the self contacts */
+  /* per iteration: mean AC norm with the force each contact actually applied
+   * in that iteration (zero after a take-off) instead of the stale local force
+   * the reference keeps for it */
+  std::vector<double> residual_applied_hist;
   std::vector<double> rprev;    /* world impulse per vertex, end of the tagged step */
   std::vector<int> rprev_tag;
   int mlp_tag = 0;
@@ -1127,6 +1138,11 @@ static void step(Sim& s) {
   if ((int)s.c_active.size() < C) s.c_active.resize(C, 0);
   const double pred_sv = gravity_norm(s) * dt;
   s.residual_hist.clear();
+  s.residual_applied_hist.clear();
+  s.s_active.assign(S, 0);
+  s.ac_trace.clear();
+  s.trace_nc = C;
+  s.trace_ns = S;
   int it = 0;
   double res_mean = 0, res_max = 0, res_n = 0, res_t = 0;
   for (; it < s.prm.local_global_iterations; ++it) {
@@ -1221,6 +1237,7 @@ static void step(Sim& s) {
             V3 fl = btv(B, (1. / mA) * fA - (1. / mB) * fB);
             if (fl.x > 0.) {
               adds[i] = {vid, idB, {0, 0, 0}};
+              s.s_active[sc] = 0;
               continue;
             }
             V3 r = -fl;
@@ -1231,6 +1248,7 @@ static void step(Sim& s) {
             }
             r = ((mA * mB) / (mA + mB)) * r;
             s.s_local_forces[sc] = r;
+            s.s_active[sc] = 1;
             adds[i] = {vid, idB, bv(B, r)};
           }
           for (size_t i = 0; i < lvl.size(); ++i) {
@@ -1272,7 +1290,7 @@ static void step(Sim& s) {
     /* updateIterationData SFE:720-753 -> AC norms SFE:590-652 */
     s.c_ac.assign(C, 0.);
     s.s_ac.assign(S, 0.);
-    double sum = 0, mxv = 0, sn = 0, stt = 0;
+    double sum = 0, mxv = 0, sn = 0, stt = 0, sum_app = 0;
     for (int c = 0; c < C; ++c) {
       const CInfo& ci = s.contacts[c];
       V3 u = btv(s.cbasis[c], ld(s.vnext.data(), ci.vertex) - ci.speed);
@@ -1281,9 +1299,19 @@ static void step(Sim& s) {
       double n3 = std::sqrt(acv[0] * acv[0] + acv[1] * acv[1] + acv[2] * acv[2]);
       s.c_ac[c] = n3;
       sum += n3;
+      {
+        const V3 ra = s.c_active[c] ? s.c_local_forces[c] : V3{0, 0, 0};
+        double an2, at2;
+        auto ap = alart_curnier(u, ra, ci.mu, &an2, &at2);
+        sum_app += std::sqrt(ap[0] * ap[0] + ap[1] * ap[1] + ap[2] * ap[2]);
+      }
       mxv = std::max(mxv, n3);
       sn += an;
       stt += at;
+      if (s.trace_ac) {
+        s.ac_trace.push_back(at);
+        s.ac_trace.push_back(an);
+      }
     }
     for (int c = 0; c < S; ++c) {
       const SelfInfo& si = s.selfc[c];
@@ -1293,9 +1321,19 @@ static void step(Sim& s) {
       double n3 = std::sqrt(acv[0] * acv[0] + acv[1] * acv[1] + acv[2] * acv[2]);
       s.s_ac[c] = n3;
       sum += n3;
+      {
+        const V3 ra = s.s_active[c] ? s.s_local_forces[c] : V3{0, 0, 0};
+        double an2, at2;
+        auto ap = alart_curnier(u, ra, si.mu, &an2, &at2);
+        sum_app += std::sqrt(ap[0] * ap[0] + ap[1] * ap[1] + ap[2] * ap[2]);
+      }
       mxv = std::max(mxv, n3);
       sn += an;
       stt += at;
+      if (s.trace_ac) {
+        s.ac_trace.push_back(at);
+        s.ac_trace.push_back(an);
+      }
     }
     const int nc = C + S;
     res_mean = nc ? sum / nc : 0.;
@@ -1303,6 +1341,7 @@ static void step(Sim& s) {
     res_n = nc ? sn / nc : 0.;
     res_t = nc ? stt / nc : 0.;
     s.residual_hist.push_back(res_mean);
+    s.residual_applied_hist.push_back(nc ? sum_app / nc : 0.);
     if (s.prm.residual_tolerance > 0. && nc > 0 && res_mean <= s.prm.residual_tolerance) {
       ++it;
       break;
@@ -1726,6 +1765,35 @@ int orc_get_residual_history(orc_sim* h, double* out, int32_t cap, int32_t* n) {
   if (n) *n = (int)r.size();
   if (out)
     for (int i = 0; i < (int)r.size() && i < cap; ++i) out[i] = r[i];
+  return PDF_OK;
+}
+
+int orc_get_residual_applied_history(orc_sim* h, double* out, int32_t cap, int32_t* n) {
+  if (!h) return PDF_INVALID_ARG;
+  const auto& r = h->s.residual_applied_hist;
+  if (n) *n = (int)r.size();
+  if (out)
+    for (int i = 0; i < (int)r.size() && i < cap; ++i) out[i] = r[i];
+  return PDF_OK;
+}
+
+int orc_trace_alart_curnier(orc_sim* h, int32_t enable) {
+  if (!h) return PDF_INVALID_ARG;
+  h->s.trace_ac = enable != 0;
+  h->s.ac_trace.clear();
+  return PDF_OK;
+}
+
+int orc_get_alart_curnier_trace(orc_sim* h, double* out, int64_t cap, int32_t* iterations,
+                                int32_t* n_contacts, int32_t* n_self) {
+  if (!h) return PDF_INVALID_ARG;
+  const Sim& s = h->s;
+  const int64_t per = 2 * (int64_t)(s.trace_nc + s.trace_ns);
+  if (iterations) *iterations = per ? (int32_t)((int64_t)s.ac_trace.size() / per) : 0;
+  if (n_contacts) *n_contacts = s.trace_nc;
+  if (n_self) *n_self = s.trace_ns;
+  if (out)
+    for (int64_t i = 0; i < (int64_t)s.ac_trace.size() && i < cap; ++i) out[i] = s.ac_trace[i];
   return PDF_OK;
 }
 

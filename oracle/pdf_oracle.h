@@ -30,6 +30,17 @@ int orc_get_self_contacts(orc_sim* s, pdf_contact* out, int32_t cap, int32_t* n)
 int orc_get_self_levels(orc_sim* s, int32_t* level_ptr, int32_t level_cap,
                         int32_t* order, int32_t order_cap, int32_t* n_levels);
 int orc_get_residual_history(orc_sim* s, double* out, int32_t cap, int32_t* n);
+/* Alart-Curnier trace (SFE:720-752, PRINT_ALART_CURNIER_ERROR): when enabled,
+ * every PD iteration of the next steps records (tangential, |normal|) per
+ * contact, obstacle contacts first; the trace holds the last step only and is
+ * laid out like pdf_get_alart_curnier_trace's. */
+int orc_trace_alart_curnier(orc_sim* s, int32_t enable);
+/* Per iteration of the last step: mean AC norm evaluated with the force each
+ * contact applied in that iteration (zero after a take-off), where the
+ * reference's norm uses the stale local force it keeps for such a contact. */
+int orc_get_residual_applied_history(orc_sim* s, double* out, int32_t cap, int32_t* n);
+int orc_get_alart_curnier_trace(orc_sim* s, double* out, int64_t cap, int32_t* iterations,
+                                int32_t* n_contacts, int32_t* n_self);
 /* Learned warm start, restated from the product (climatenet_b200/csrc/mlp.cu):
  * weights (5,059 floats), the per-contact sample log, and the MLP forward with
  * the tensor cores' bfloat16 rounding emulated. */

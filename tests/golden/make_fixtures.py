@@ -1,7 +1,8 @@
 """Regenerates the committed golden fixtures from the reference checkout.
 
-Run here (where the reference is mounted); the fixtures it writes are small
-JSON files that the tests read on any machine.
+Run where the reference source tree exists, with its root as the only
+argument; the fixtures it writes are small JSON files that the tests read on
+any machine.
 
   analytic_incline.json: the two OBJ meshes of the reference's Figure-5
   known-answer scene (mesh/analytic/cloth.obj and support.obj, coordinates
@@ -15,7 +16,9 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: python tests/golden/make_fixtures.py <reference root>")
+REF = sys.argv[1]
 HERE = os.path.dirname(os.path.abspath(__file__))
 
 
