@@ -306,9 +306,10 @@ def e2e_steps(sim, steps, barrier, dist, world, start):
     return whole_job_rate(world, steps, 1e3 * max_over_ranks(time.perf_counter() - t0, dist))
 
 
-# DRAM bytes (read + write) of one global solve, forward + backward sweep,
-# from ncu captures of the 500 x 500 cloth (profiles/sweeps_cloth500_fp32.md,
-# profiles/sweeps_cloth500_fp64.md); None for other workloads.
+# DRAM bytes (read + write) of one global solve of the 500 x 500 cloth,
+# forward + backward sweep, from ncu's dram__bytes_read.sum +
+# dram__bytes_write.sum (a profiler is needed to count them, so they cannot be
+# measured inside this run); None for other workloads.
 SOLVE_TRAFFIC_500 = {True: 419.2e6, False: 831.8e6}
 
 

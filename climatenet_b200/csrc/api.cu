@@ -1437,6 +1437,9 @@ int pdf_detect_candidates(const double* positions, int32_t n_vertices, const int
   int st = PDF_OK;
   try {
     st = standalone_candidates(positions, n_vertices, triangles, n_triangles, tolerance, pairs, cap, n, device, err);
+  } catch (const std::overflow_error& e) {
+    err = e.what();
+    st = PDF_CAPACITY_EXCEEDED;
   } catch (const std::exception& e) {
     err = e.what();
     st = PDF_CUDA_ERROR;
@@ -1452,6 +1455,9 @@ int pdf_detect_self_collisions(const double* positions, int32_t n_vertices, cons
   int st = PDF_OK;
   try {
     st = standalone_self(positions, n_vertices, triangles, n_triangles, tolerance, out, cap, n, device, err);
+  } catch (const std::overflow_error& e) {
+    err = e.what();
+    st = PDF_CAPACITY_EXCEEDED;
   } catch (const std::exception& e) {
     err = e.what();
     st = PDF_CUDA_ERROR;

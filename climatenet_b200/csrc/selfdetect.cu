@@ -624,7 +624,7 @@ int detect_mesh(SelfWS& w, const double* q, const int* tris_global, int v0, int 
   CKS(cudaMemcpyAsync(&nh, w.n_hits, sizeof(int), cudaMemcpyDeviceToHost, st));
   CKS(cudaMemcpyAsync(&err, w.err, sizeof(int), cudaMemcpyDeviceToHost, st));
   CKS(cudaStreamSynchronize(st));
-  if (err) throw std::runtime_error("BVH traversal stack overflow");
+  if (err) throw std::overflow_error("BVH traversal stack overflow (a vertex's walk needs more than the stack holds)");
   if (nh > 0 && nh <= w.hit_cap) {
     int bits = 64;
     CKS(cub::DeviceRadixSort::SortPairs(w.cub_tmp, bytes, w.hkey, w.hkey2, w.hval, w.hval2, nh, 0, bits, st));
@@ -938,10 +938,6 @@ constexpr size_t kNoAllocScratchBytes = 4 * kTriBytes + 2 * kTriKeyBytes + 7 * k
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Device address of g_noalloc_scratch per device, looked up once per device
-// with that device current (the array's name is only a host-side stand-in).
-static unsigned char* g_noalloc_ptr[64] = {};
-
 __global__ void k_keys_to_pairs(int n, const unsigned long long* __restrict__ keys, int* __restrict__ pairs) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= n) return;
@@ -960,32 +956,28 @@ int noalloc_candidates(const double* positions, int nv, const int* triangles, in
           " triangles (got " + std::to_string(nt) + ")";
     return PDF_CAPACITY_EXCEEDED;
   }
-  int dev = 0;
-  CKS(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) {
-    err = "device ordinal out of range";
-    return PDF_INVALID_ARG;
+  // Set-up, repeated on every call with the caller's device current: the
+  // array's device address on this device (the name is only a host-side
+  // stand-in; cudaGetSymbolAddress allocates nothing) and the check that the
+  // radix sort's workspace fits the reserved block.  Looking the address up on
+  // every call keeps it valid after a cudaDeviceReset and needs no lock when
+  // several host threads call.
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    err = std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e);
+    return PDF_CUDA_ERROR;
   }
-  if (!g_noalloc_ptr[dev]) {
-    // first call on this device: set-up (must not happen during stream capture)
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      err = std::string("cudaGetSymbolAddress(g_noalloc_scratch): ") + cudaGetErrorString(e);
-      return PDF_CUDA_ERROR;
-    }
-    size_t b1 = 0, b2 = 0;
-    CKS(cub::DeviceRadixSort::SortPairs(nullptr, b1, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                        (int*)nullptr, (int*)nullptr, kNoAllocMaxTriangles));
-    CKS(cub::DeviceRadixSort::SortPairs(nullptr, b2, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                        (int*)nullptr, (int*)nullptr, kNoAllocMaxPairs));
-    if (std::max(b1, b2) > kNoAllocSortBytes) {
-      err = "radix-sort workspace larger than the reserved scratch";
-      return PDF_CAPACITY_EXCEEDED;
-    }
-    g_noalloc_ptr[dev] = (unsigned char*)p;
+  size_t b1 = 0, b2 = 0;
+  CKS(cub::DeviceRadixSort::SortPairs(nullptr, b1, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                      (int*)nullptr, (int*)nullptr, kNoAllocMaxTriangles));
+  CKS(cub::DeviceRadixSort::SortPairs(nullptr, b2, (unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                      (int*)nullptr, (int*)nullptr, kNoAllocMaxPairs));
+  if (std::max(b1, b2) > kNoAllocSortBytes) {
+    err = "radix-sort workspace larger than the reserved scratch";
+    return PDF_CAPACITY_EXCEEDED;
   }
-  unsigned char* base = g_noalloc_ptr[dev];
+  unsigned char* base = (unsigned char*)p;
   size_t off = 0;
   auto take = [&](size_t bytes) {
     unsigned char* q = base + off;
@@ -1041,6 +1033,9 @@ extern "C" int pdf_detect_candidates_noalloc(const double* positions, int32_t n_
   try {
     st = pdfb::noalloc_candidates(positions, n_vertices, triangles, n_triangles, tolerance, pairs, cap, n,
                                   (cudaStream_t)cuda_stream, err);
+  } catch (const std::overflow_error& e) {
+    err = e.what();
+    st = PDF_CAPACITY_EXCEEDED;
   } catch (const std::exception& e) {
     err = e.what();
     st = PDF_CUDA_ERROR;

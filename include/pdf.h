@@ -374,11 +374,17 @@ int pdf_detect_self_collisions(const double* positions, int32_t n_vertices,
  *   receives the number of candidate pairs, written sorted by (vertex,
  *   triangle) exactly as pdf_detect_candidates returns them.
  *   Limits: n_triangles <= 65536 and at most 262144 candidate pairs; larger
- *   inputs return PDF_CAPACITY_EXCEEDED without touching pairs.
- *   The first call on a device looks up the array's device address; make that
- *   first call before any stream capture.  All calls share the one array:
- *   calls that overlap on the GPU (other streams, other host threads) race.
- *   The call synchronises cuda_stream (NULL = the legacy default stream). */
+ *   inputs return PDF_CAPACITY_EXCEEDED without touching pairs (when the
+ *   pairs exceed cap or the limit, *n still receives their number).  A vertex
+ *   whose hierarchy walk overflows its stack also gives
+ *   PDF_CAPACITY_EXCEEDED.
+ *   Every call looks up the array's device address on the current device
+ *   (cudaGetSymbolAddress, which allocates nothing), so it stays valid after a
+ *   cudaDeviceReset and from any host thread.  All calls share the one array
+ *   and find it as the previous call left it: calls that overlap on the GPU
+ *   (other streams, other host threads) race.  The call reads the pair count
+ *   back to the host and synchronises cuda_stream (NULL = the legacy default
+ *   stream), so it cannot be recorded into a CUDA graph by stream capture. */
 int pdf_detect_candidates_noalloc(const double* positions, int32_t n_vertices,
                                   const int32_t* triangles, int32_t n_triangles,
                                   double tolerance, int32_t* pairs, int32_t cap,
