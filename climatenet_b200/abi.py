@@ -122,6 +122,9 @@ class pdf_stats(C.Structure):
         ("n_constraint_rows", C.c_int32), ("kernel_launches", C.c_int64),
         ("factor_nnz_true", C.c_int64), ("sweep_chunk", C.c_int32),
         ("sweep_chunk_ms", C.c_double * 3),
+        ("sweep_cut_level", C.c_int32), ("sweep_blocks", C.c_int32),
+        ("sweep_block_elems", C.c_int64), ("sweep_upper_elems", C.c_int64),
+        ("sweep_cut_ms", C.c_double * 8),
     ]
 
 

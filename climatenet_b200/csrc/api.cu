@@ -55,41 +55,82 @@ constexpr int kThreads = 256;
 inline int blocks_for(int64_t n) { return (int)std::max<int64_t>(1, (n + kThreads - 1) / kThreads); }
 constexpr int kStrideBlocks = 592;  // 4 x 148 SMs for grid-stride kernels
 
-// Work items of one sweep are at most 32 x chunk elements; the chunk is
-// chosen per scene by the autotuner in create_impl among these.
-constexpr int kChunk = 64;  // host emulation check (pdf_factor_check)
+// Work items of the upper supernodes are at most 32 x chunk elements and the
+// subtree blocks reach up to the cut level; both are chosen per scene by the
+// autotuner in create_impl among these.
+constexpr int kChunk = 64;
+constexpr int kCutLevel = 4;  // host emulation check (pdf_factor_check)
 constexpr int kRecords = 64;  // step records in flight before the oldest is harvested
 constexpr int kChunkCandidates[3] = {32, 64, 128};
+constexpr int kCutCandidates = 8;  // cut levels 0 .. 7
+// polls of a dependency counter before a sweep gives up (each poll sleeps
+// about 32 ns): far above any legitimate wait
+constexpr int kMaxSpins = 1 << 22;
 
-// Work-item lists of the two sweeps in elimination-tree order (forward:
-// levels bottom-up, backward: top-down), one item per tile and chunk.  The
-// completion counters are cumulative per schedule, so they restart here.
-void build_schedule(pdf_handle* h, int chunk) {
+template <typename T>
+void free_dev(T*& p) {
+  if (p) cudaFree((void*)p);
+  p = nullptr;
+}
+
+void free_plan(DPlan& P) {
+  free_dev(P.fup);
+  free_dev(P.bup);
+  free_dev(P.fblk);
+  free_dev(P.bblk);
+  free_dev(P.fitem);
+  free_dev(P.bitem);
+  free_dev(P.upper_cols);
+}
+
+// Sweep plan (subtree blocks + upper work items, factor.hpp) on the device.
+// The completion counters are cumulative per schedule, so they restart here.
+void build_schedule(pdf_handle* h, int chunk, int cut_level) {
   const Factor& f = h->fac;
-  std::vector<SweepTask> fa, ba;
-  std::vector<SnInfo> sn;
-  build_sweep_tasks(f, chunk, fa, ba, sn);
-  if (h->d.ftasks) cudaFree(h->d.ftasks);
-  if (h->d.btasks) cudaFree(h->d.btasks);
+  SweepPlan& hp = h->d.host_plan;
+  build_sweep_plan(f, chunk, cut_level, hp);
+  DPlan& P = h->d.plan;
+  free_plan(P);
   if (h->d.sn) cudaFree(h->d.sn);
-  h->d.ftasks = upload(fa);
-  h->d.btasks = upload(ba);
-  h->d.nf = (int)fa.size();
-  h->d.nb = (int)ba.size();
-  h->d.sn = upload(sn);
+  h->d.sn = upload(hp.sn);
   if (!h->d.rows) h->d.rows = upload(f.rows);
+  P.fup = upload(hp.fupi);
+  P.bup = upload(hp.bupi);
+  P.nfup = (int)hp.fupi.size();
+  P.nbup = (int)hp.bupi.size();
+  P.sn = h->d.sn;
+  P.rows = h->d.rows;
+  P.fblk = upload(hp.fblk);
+  P.bblk = upload(hp.bblk);
+  P.nblk = (int)hp.fblk.size();
+  P.fitem = upload(hp.fitem);
+  P.bitem = upload(hp.bitem);
+  P.upper_cols = upload(hp.upper_cols);
+  P.n_upper = (int)hp.upper_cols.size();
+  P.perm = h->d.perm;
+  P.max_cols = hp.max_block_cols;
+  if (h->fp32)
+    configure_solve<float>(P);
+  else
+    configure_solve<double>(P);
   h->n_levels = f.n_levels;
+  h->stats.sweep_chunk = chunk;
+  h->stats.sweep_cut_level = cut_level;
+  h->stats.sweep_blocks = P.nblk;
+  h->stats.sweep_block_elems = hp.block_elems;
+  h->stats.sweep_upper_elems = hp.upper_elems;
   // dependency counters start at zero, the solve counter at one
   SweepSync& sy = h->d.sync;
   if (!sy.queue) {
-    sy.queue = dalloc<int>(2);
+    sy.queue = dalloc<int>(4);
     sy.epoch = dalloc<unsigned long long>(1);
     sy.fdone = dalloc<unsigned long long>(f.n_sn);
     sy.fchild = dalloc<unsigned long long>(f.n_sn);
     sy.bdone = dalloc<unsigned long long>(f.n_sn);
     sy.err = dalloc<int>(1);
+    sy.max_spins = kMaxSpins;
   }
-  CK(cudaMemset(sy.queue, 0, 2 * sizeof(int)));
+  CK(cudaMemset(sy.queue, 0, 4 * sizeof(int)));
   const unsigned long long one = 1ULL;
   CK(cudaMemcpy(sy.epoch, &one, sizeof(one), cudaMemcpyHostToDevice));
   CK(cudaMemset(sy.fdone, 0, f.n_sn * sizeof(unsigned long long)));
@@ -315,7 +356,7 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   d.cstep = dalloc<double>(3 * (size_t)N);
   d.bp = dalloc<double>(3 * (size_t)std::max(1, dm.B));
   // solve
-  build_schedule(h, kChunk);
+  build_schedule(h, kChunk, kCutLevel);
   if (h->fp32) {
     d.Wf32 = upload(std::vector<float>(f.Wf.begin(), f.Wf.end()));
     d.Wb32 = upload(std::vector<float>(f.Wb.begin(), f.Wb.end()));
@@ -476,28 +517,37 @@ void launch_local(pdf_handle* h, T* b, int mode) {
                        std::max(h->prm.air_damping, 0.), d.c.slot_of, d.c.f, b, h->prm.time_step, mode);
 }
 
-// Global solve: one persistent forward and one backward sweep, then the
-// write-back of v and q^k (which also clears x, y for the next solve).
+// Global solve: one persistent forward and one backward sweep (which writes
+// back v and q^k of the blocks' columns), then the write-back of the upper
+// columns (which also clears their x, y for the next solve).
 template <typename T>
 void launch_solve(pdf_handle* h, T* b, T* y, T* x, const T* Wf, const T* Wb, int mode) {
   DeviceBuffers& d = h->d;
-  launch_solve_sweeps<T>(h->stream, d.ftasks, d.nf, d.btasks, d.nb, d.sn, d.rows, Wf, Wb, b, y, x, h->dm.N, d.sync);
-  launch_solve_post<T>(h->stream, h->dm.N, d.perm, x, y, d.v, d.qk, d.q, h->prm.time_step, mode, d.sync);
+  launch_solve_sweeps<T>(h->stream, d.plan, Wf, Wb, b, y, x, h->dm.N, d.sync,
+                         WriteBack{d.v, d.qk, d.q, h->prm.time_step, mode});
 }
 
-// Schedule autotuner: times the global solve with each candidate work-item
-// width on this scene's factor (zero right-hand side: the sweeps read the
-// same data and wait on the same dependencies whatever the values) and keeps
-// the fastest.
+template <typename T>
+void launch_solve_with(pdf_handle* h, const SweepSync& sy, T* b, T* y, T* x, const T* Wf, const T* Wb, int mode) {
+  DeviceBuffers& d = h->d;
+  launch_solve_sweeps<T>(h->stream, d.plan, Wf, Wb, b, y, x, h->dm.N, sy,
+                         WriteBack{d.v, d.qk, d.q, h->prm.time_step, mode});
+}
+
+// Schedule autotuner: times the global solve of this scene's factor with
+// each candidate cut level (work-item width 64), then with each work-item
+// width at the best cut level, and keeps the fastest.  The right-hand side is
+// zero (the sweeps read the same data and wait on the same dependencies
+// whatever the values); v and q^k, which the solve writes, are restored.
 void autotune_schedule(pdf_handle* h) {
   DeviceBuffers& d = h->d;
   const int N = h->dm.N;
   cudaStream_t st = h->stream;
-  double best = 1e300;
-  int best_chunk = kChunk;
-  for (int ci = 0; ci < 3; ++ci) {
-    const int chunk = kChunkCandidates[ci];
-    build_schedule(h, chunk);
+  std::vector<double> vsave(3 * (size_t)N), qsave(3 * (size_t)N);
+  CK(cudaMemcpy(vsave.data(), d.v, vsave.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(qsave.data(), d.qk, qsave.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  auto time_plan = [&](int chunk, int cut) {
+    build_schedule(h, chunk, cut);
     double total = 0.;
     for (int r = 0; r < 4; ++r) {
       if (h->fp32) {
@@ -518,21 +568,37 @@ void autotune_schedule(pdf_handle* h) {
       CK(cudaEventElapsedTime(&ms, h->ev[5], h->ev[6]));
       if (r > 0) total += ms;  // first run warms up
     }
-    h->stats.sweep_chunk_ms[ci] = total / 3.;
-    if (total / 3. < best) {
-      best = total / 3.;
+    int derr = 0;
+    CK(cudaMemcpy(&derr, d.sync.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (derr) throw CudaFail("a supernodal sweep gave up waiting for a dependency while tuning");
+    return total / 3.;
+  };
+  double best = 1e300;
+  int best_cut = kCutLevel, best_chunk = kChunk;
+  for (int cut = 0; cut < kCutCandidates; ++cut) {
+    const double ms = time_plan(kChunk, cut);
+    h->stats.sweep_cut_ms[cut] = ms;
+    if (ms < best) {
+      best = ms;
+      best_cut = cut;
+    }
+  }
+  for (int ci = 0; ci < 3; ++ci) {
+    const int chunk = kChunkCandidates[ci];
+    const double ms = chunk == kChunk ? h->stats.sweep_cut_ms[best_cut] : time_plan(chunk, best_cut);
+    h->stats.sweep_chunk_ms[ci] = ms;
+    if (ms < best) {
+      best = ms;
       best_chunk = chunk;
     }
   }
-  build_schedule(h, best_chunk);
-  h->stats.sweep_chunk = best_chunk;
+  build_schedule(h, best_chunk, best_cut);
   if (h->fp32)
     launch_solve_prep<float>(st, N, d.x32, d.y32, d.sync);
   else
     launch_solve_prep<double>(st, N, d.x64, d.y64, d.sync);
-  int derr = 0;
-  CK(cudaMemcpy(&derr, d.sync.err, sizeof(int), cudaMemcpyDeviceToHost));
-  if (derr) throw CudaFail("a supernodal sweep gave up waiting for a dependency while tuning");
+  CK(cudaMemcpy(d.v, vsave.data(), vsave.size() * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d.qk, qsave.data(), qsave.size() * sizeof(double), cudaMemcpyHostToDevice));
   CK(cudaStreamSynchronize(st));
 }
 
@@ -884,8 +950,7 @@ void free_handle(pdf_handle* h) {
   void* ptrs[] = {d.mass, d.ring_kappa, d.ring_bend, d.self_bend, d.ring_ptr, d.ring_idx, d.bend_of, d.bend_ptr,
                   d.bend_idx, d.bend_coef, d.bend_w, d.bend_rest, d.pin_term, d.ata_ptr, d.ata_col, d.ata_val,
                   d.perm, d.iperm, d.vmat, d.friction, d.tris, d.obstacles, d.vmesh, d.q, d.v, d.tn, d.qk,
-                  d.cstep, d.bp, d.ftasks,
-                  d.btasks, d.sn, d.rows, d.Wf64, d.Wb64, d.Wf32, d.Wb32, d.sync.queue, d.sync.epoch,
+                  d.cstep, d.bp, d.sn, d.rows, d.Wf64, d.Wb64, d.Wf32, d.Wb32, d.sync.queue, d.sync.epoch,
                   d.sync.fdone, d.sync.fchild, d.sync.bdone, d.sync.err, d.b64, d.y64, d.x64, d.b32, d.y32,
                   d.x32, d.flags, d.sel_idx, d.cub_tmp, d.newf, d.ac_hist, d.c.n_contacts, d.c.c_vertex,
                   d.c.c_normal, d.c.c_speed, d.c.c_mu, d.c.c_basis, d.c.c_force, d.c.c_ac, d.c.c_slot, d.c.n_self,
@@ -897,6 +962,7 @@ void free_handle(pdf_handle* h) {
                   d.c.ac_trace, h->gather_idx, h->gather_out, h->stage, h->bad_dev, d.ob_best};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  free_plan(d.plan);
   for (auto p : d.obstacle_v) cudaFree(p);
   for (auto b : h->mesh_bvh) mesh_bvh_free(b);
   for (auto p : d.obstacle_t) cudaFree(p);
@@ -1027,6 +1093,14 @@ int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms_out, d
       for (size_t b = 0; b + 1 < h->model.bend_ptr.size(); ++b)
         bsum += (h->model.bend_ptr[b + 1] - h->model.bend_ptr[b]) * 12. + 8.;
       bytes = 4. * 24. * N + E * 16. + bsum;
+    } else if (phase == 3) {
+      // obstacle tests: positions read, one flag byte per (obstacle, vertex);
+      // self collision (when on): positions and triangles read (24 N + 12 T),
+      // the 112-byte node records written by the refit and read once by the
+      // traversal, and the triangle boxes (48 T) written and read
+      const double T = (double)h->model.tris.size() / 3.;
+      bytes = (double)h->obs.n * (24. * N + N);
+      if (h->prm.self_collision) bytes += 24. * N + 12. * T + 2. * 112. * std::max(0., T - 1.) + 2. * 48. * T;
     }
     // phase 0 works on a saved right-hand side restored between repetitions
     double* save64 = nullptr;
@@ -1414,6 +1488,36 @@ int pdf_get_residual_history(pdf_handle* h, double* out, int32_t cap, int32_t* n
 
 void pdf_destroy(pdf_handle* h) { free_handle(h); }
 
+int pdf_check_wait_timeout(pdf_handle* h, int32_t max_spins) {
+  if (!h || max_spins <= 0) return fail(h, PDF_INVALID_ARG, "invalid wait-timeout check");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    DeviceBuffers& d = h->d;
+    const int N = h->dm.N;
+    cudaStream_t st = h->stream;
+    build_schedule(h, h->stats.sweep_chunk > 0 ? h->stats.sweep_chunk : kChunk, 0);
+    if (d.plan.nfup == 0) return fail(h, PDF_INVALID_ARG, "the scene's sweep schedule has no dependency wait");
+    // targets one solve ahead: the counters stop one solve short of them
+    const unsigned long long ahead = 2ULL;
+    CK(cudaMemcpy(d.sync.epoch, &ahead, sizeof(ahead), cudaMemcpyHostToDevice));
+    SweepSync sy = d.sync;
+    sy.max_spins = max_spins;
+    if (h->fp32) {
+      launch_solve_prep<float>(st, N, d.x32, d.y32, sy);
+      launch_solve_with<float>(h, sy, d.b32, d.y32, d.x32, d.Wf32, d.Wb32, 1);
+    } else {
+      launch_solve_prep<double>(st, N, d.x64, d.y64, sy);
+      launch_solve_with<double>(h, sy, d.b64, d.y64, d.x64, d.Wf64, d.Wb64, 0);
+    }
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(st));
+    int derr = 0;
+    CK(cudaMemcpy(&derr, d.sync.err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (!(derr & 1)) return fail(h, PDF_INVALID_ARG, "no dependency wait gave up");
+    return fail(h, PDF_DEVICE_TIMEOUT, "a supernodal sweep gave up waiting for a dependency (wait-timeout check)");
+  });
+}
+
 int pdf_factor_check(const pdf_scene_desc* scene, const pdf_params* params, const double* b, double* x) {
   if (!scene || !params || !b || !x) return fail(nullptr, PDF_INVALID_ARG, "null argument");
   try {
@@ -1423,7 +1527,27 @@ int pdf_factor_check(const pdf_scene_desc* scene, const pdf_params* params, cons
     std::string err;
     if (!factorize(m, params->time_step, 40, f, err)) return fail(nullptr, PDF_NOT_SPD, err);
     std::vector<double> bv(b, b + 3 * (size_t)m.N), xv;
-    if (!emulate_sweeps(f, kChunk, bv, xv, err)) return fail(nullptr, PDF_INVALID_ARG, err);
+    // every schedule the autotuner can choose: cut levels 0 .. 7, chunks
+    // 32 / 64 / 128; all must solve the system alike
+    std::vector<double> x0;
+    double scale = 0.;
+    for (int cut = 0; cut < kCutCandidates; ++cut)
+      for (int chunk : kChunkCandidates) {
+        SweepPlan plan;
+        build_sweep_plan(f, chunk, cut, plan);
+        if (!emulate_sweeps(f, plan, bv, xv, err)) return fail(nullptr, PDF_INVALID_ARG, err);
+        if (x0.empty()) {
+          x0 = xv;
+          for (double t : x0) scale = std::max(scale, std::fabs(t));
+          continue;
+        }
+        for (size_t k = 0; k < xv.size(); ++k)
+          if (!(std::fabs(xv[k] - x0[k]) <= 1e-10 * scale))
+            return fail(nullptr, PDF_INVALID_ARG,
+                        "sweep schedules disagree (cut level " + std::to_string(cut) + ", chunk " +
+                            std::to_string(chunk) + ")");
+      }
+    xv = x0;
     std::copy(xv.begin(), xv.end(), x);
   } catch (const std::exception& e) {
     return fail(nullptr, PDF_INVALID_ARG, e.what());

@@ -465,12 +465,126 @@ void build_sweep_tasks(const Factor& f, int chunk, std::vector<SweepTask>& fa, s
   for (const auto& t : ba) sn[t.sn].ntb++;
 }
 
-bool emulate_sweeps(const Factor& f, int chunk, const std::vector<double>& bin, std::vector<double>& xout,
-                    std::string& err) {
-  const int64_t n = f.N;
+void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan) {
+  const int S = f.n_sn;
+  plan = SweepPlan{};
+  plan.cut_level = cut_level;
+  plan.chunk = chunk;
+  // subtree extents: supernodes are numbered in column order and every
+  // parent comes after its children, so one ascending pass accumulates them
+  std::vector<int> lo(S), cnt(S, 0);
+  for (int s = 0; s < S; ++s) lo[s] = f.sn_c0[s];
+  for (int s = 0; s < S; ++s) {
+    cnt[s] += f.sn_ns[s];
+    const int p = f.sn_parent[s];
+    if (p >= 0) {
+      lo[p] = std::min(lo[p], lo[s]);
+      cnt[p] += cnt[s];
+    }
+  }
+  auto eligible = [&](int s) {
+    return f.sn_level[s] <= cut_level && f.sn_level[s] < kMaxBlockLevels && cnt[s] <= kMaxBlockCols &&
+           f.sn_c0[s] + f.sn_ns[s] - lo[s] == cnt[s];
+  };
+  std::vector<int> blk(S, -1);
+  std::vector<int> roots;
+  // descending: a root's block id is set before its descendants are visited
+  for (int s = S - 1; s >= 0; --s) {
+    const int p = f.sn_parent[s];
+    if (p >= 0 && blk[p] >= 0) {
+      blk[s] = blk[p];
+    } else if (eligible(s)) {
+      blk[s] = (int)roots.size();
+      roots.push_back(s);
+    }
+  }
+  const int nb = (int)roots.size();
+  std::vector<std::vector<int>> members(nb);
+  for (int s = 0; s < S; ++s)
+    if (blk[s] >= 0) members[blk[s]].push_back(s);
+  // stored elements of a supernode's tiles (either copy has the same count)
+  auto sn_elems = [&](int s) {
+    return f.ftile_off[f.sn_ftile0[s + 1]] - f.ftile_off[f.sn_ftile0[s]];
+  };
+  // largest blocks first (their CTAs start early, the small ones fill in)
+  std::vector<int64_t> cost(nb, 0);
+  for (int b = 0; b < nb; ++b)
+    for (int s : members[b]) cost[b] += sn_elems(s);
+  std::vector<int> order(nb);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  for (int b : order) {
+    const int r = roots[b];
+    SweepBlock fb{}, bb{};
+    fb.c0 = bb.c0 = lo[r];
+    fb.c1 = bb.c1 = f.sn_c0[r] + f.sn_ns[r];
+    fb.parent = bb.parent = f.sn_parent[r];
+    fb.nlev = bb.nlev = f.sn_level[r] + 1;
+    plan.max_block_cols = std::max(plan.max_block_cols, fb.c1 - fb.c0);
+    plan.block_elems += cost[b];
+    std::vector<std::vector<int>> by_lev(fb.nlev);
+    for (int s : members[b]) by_lev[f.sn_level[s]].push_back(s);
+    fb.item0 = (int)plan.fitem.size();
+    for (int L = 0; L < fb.nlev; ++L) {
+      fb.lev[L] = (int)plan.fitem.size() - fb.item0;
+      for (int s : by_lev[L])
+        for (int64_t t = f.sn_ftile0[s]; t < f.sn_ftile0[s + 1]; ++t)
+          plan.fitem.push_back({f.ftile_off[t], f.sn_c0[s] - fb.c0, f.sn_ns[s], f.sn_nr[s],
+                                (int)(t - f.sn_ftile0[s]), (int)f.sn_roff[s], 0});
+    }
+    fb.lev[fb.nlev] = (int)plan.fitem.size() - fb.item0;
+    bb.item0 = (int)plan.bitem.size();
+    for (int k = 0; k < bb.nlev; ++k) {
+      const int L = bb.nlev - 1 - k;
+      bb.lev[k] = (int)plan.bitem.size() - bb.item0;
+      for (int s : by_lev[L])
+        for (int64_t t = f.sn_btile0[s]; t < f.sn_btile0[s + 1]; ++t)
+          plan.bitem.push_back({f.btile_off[t], f.sn_c0[s] - bb.c0, f.sn_ns[s], f.sn_nr[s],
+                                (int)(t - f.sn_btile0[s]), (int)f.sn_roff[s], 0});
+    }
+    bb.lev[bb.nlev] = (int)plan.bitem.size() - bb.item0;
+    plan.fblk.push_back(fb);
+    plan.bblk.push_back(bb);
+  }
+  // upper supernodes: the per-warp work items and their dependency records
   std::vector<SweepTask> fa, ba;
-  std::vector<SnInfo> sn;
-  build_sweep_tasks(f, chunk, fa, ba, sn);
+  build_sweep_tasks(f, chunk, fa, ba, plan.sn);
+  for (const SweepTask& t : fa)
+    if (blk[t.sn] < 0) plan.fup.push_back(t);
+  for (const SweepTask& t : ba)
+    if (blk[t.sn] < 0) plan.bup.push_back(t);
+  for (int s = 0; s < S; ++s) {
+    plan.sn[s].ntf = plan.sn[s].ntb = 0;
+    if (blk[s] >= 0) continue;
+    plan.upper_elems += sn_elems(s);
+    for (int c = f.sn_c0[s]; c < f.sn_c0[s] + f.sn_ns[s]; ++c) plan.upper_cols.push_back(c);
+  }
+  for (const SweepTask& t : plan.fup) plan.sn[t.sn].ntf++;
+  for (const SweepTask& t : plan.bup) plan.sn[t.sn].ntb++;
+  auto upper = [&](const SweepTask& t, bool fwd) {
+    const SnInfo& q = plan.sn[t.sn];
+    UpperItem u{};
+    u.off = t.off;
+    u.sn = t.sn;
+    u.tile = t.tile;
+    u.a0 = t.a0;
+    u.a1 = t.a1;
+    u.c0 = q.c0;
+    u.ns = q.ns;
+    u.nr = q.nr;
+    u.roff = (int)q.roff;
+    u.parent = q.parent;
+    u.wait = fwd ? q.nchild : (q.parent >= 0 ? plan.sn[q.parent].ntb : 0);
+    u.ntf = q.ntf;
+    return u;
+  };
+  for (const SweepTask& t : plan.fup) plan.fupi.push_back(upper(t, true));
+  for (const SweepTask& t : plan.bup) plan.bupi.push_back(upper(t, false));
+}
+
+bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<double>& bin,
+                    std::vector<double>& xout, std::string& err) {
+  const int64_t n = f.N;
   std::vector<double> b(3 * n), y(3 * n, 0.), x(3 * n, 0.);
   for (int64_t k = 0; k < n; ++k)
     for (int c = 0; c < 3; ++c) b[k + c * n] = bin[3 * (size_t)f.perm[k] + c];
@@ -482,8 +596,51 @@ bool emulate_sweeps(const Factor& f, int chunk, const std::vector<double>& bin, 
     return true;
   };
   const int64_t nWf = (int64_t)f.Wf.size(), nWb = (int64_t)f.Wb.size(), nrows = (int64_t)f.rows.size();
-  for (const SweepTask& tk : fa) {
-    const SnInfo& s = sn[tk.sn];
+  const int64_t nfi = (int64_t)plan.fitem.size(), nbi = (int64_t)plan.bitem.size();
+  // forward, blocks: the block's slice of b in "shared memory"
+  for (const SweepBlock& B : plan.fblk) {
+    const int nc = B.c1 - B.c0;
+    if (nc <= 0 || nc > plan.max_block_cols || B.nlev > kMaxBlockLevels) {
+      err = "bad block extent";
+      return false;
+    }
+    if (!chk(B.c0, n, "block columns") || !chk(B.c1 - 1, n, "block columns")) return false;
+    std::vector<double> sb(3 * (size_t)nc);
+    for (int k = 0; k < nc; ++k)
+      for (int c = 0; c < 3; ++c) sb[k + c * nc] = b[B.c0 + k + c * n];
+    for (int L = 0; L < B.nlev; ++L)
+      for (int it = B.item0 + B.lev[L]; it < B.item0 + B.lev[L + 1]; ++it) {
+        if (!chk(it, nfi, "forward block items")) return false;
+        const BlockItem& I = plan.fitem[it];
+        const int m = std::min(kTile, I.ns + I.nr - kTile * I.tile), w = std::min(I.ns, kTile * I.tile + kTile);
+        for (int l = 0; l < m; ++l) {
+          double acc[3] = {0, 0, 0};
+          for (int j = 0; j < w; ++j) {
+            const int64_t wi = I.off + (int64_t)j * m + l;
+            if (!chk(wi, nWf, "forward block tile") || !chk(I.c0l + j, nc, "forward block vector")) return false;
+            for (int c = 0; c < 3; ++c) acc[c] += f.Wf[wi] * sb[I.c0l + j + c * nc];
+          }
+          const int row = kTile * I.tile + l;
+          if (row < I.ns) {
+            if (!chk(I.c0l + row, nc, "forward block y")) return false;
+            for (int c = 0; c < 3; ++c) y[B.c0 + I.c0l + row + c * n] = acc[c];
+          } else {
+            if (!chk(I.roff + row - I.ns, nrows, "forward block rows")) return false;
+            const int64_t r = f.rows[I.roff + row - I.ns];
+            if (!chk(r, n, "forward block scatter")) return false;
+            if (r < B.c1) {
+              if (!chk(r - B.c0, nc, "forward block shared scatter")) return false;
+              for (int c = 0; c < 3; ++c) sb[r - B.c0 + c * nc] -= acc[c];
+            } else {
+              for (int c = 0; c < 3; ++c) b[r + c * n] -= acc[c];
+            }
+          }
+        }
+      }
+  }
+  // forward, upper work items (the records the device reads)
+  for (const UpperItem& tk : plan.fupi) {
+    const UpperItem& s = tk;
     const int mrows = std::min(kTile, s.ns + s.nr - tk.tile * kTile);
     for (int l = 0; l < mrows; ++l) {
       const int row = tk.tile * kTile + l;
@@ -503,8 +660,9 @@ bool emulate_sweeps(const Factor& f, int chunk, const std::vector<double>& bin, 
       }
     }
   }
-  for (const SweepTask& tk : ba) {
-    const SnInfo& s = sn[tk.sn];
+  // backward, upper work items
+  for (const UpperItem& tk : plan.bupi) {
+    const UpperItem& s = tk;
     const int j0t = tk.tile * kTile, nd = s.ns - j0t;
     const int mc = std::min(kTile, nd);
     for (int l = 0; l < mc; ++l) {
@@ -528,6 +686,43 @@ bool emulate_sweeps(const Factor& f, int chunk, const std::vector<double>& bin, 
       if (col < s.ns)
         for (int c = 0; c < 3; ++c) x[s.c0 + col + c * n] += acc[c];
     }
+  }
+  // backward, blocks: x of the block's columns in "shared memory"
+  for (const SweepBlock& B : plan.bblk) {
+    const int nc = B.c1 - B.c0;
+    std::vector<double> sx(3 * (size_t)nc, 0.);
+    for (int L = 0; L < B.nlev; ++L)
+      for (int it = B.item0 + B.lev[L]; it < B.item0 + B.lev[L + 1]; ++it) {
+        if (!chk(it, nbi, "backward block items")) return false;
+        const BlockItem& I = plan.bitem[it];
+        const int j0t = kTile * I.tile, nd = I.ns - j0t, mc = std::min(kTile, nd), h = nd + I.nr;
+        for (int l = 0; l < mc; ++l) {
+          double acc[3] = {0, 0, 0};
+          for (int i = 0; i < h; ++i) {
+            const int64_t wi = I.off + (int64_t)i * mc + l;
+            if (!chk(wi, nWb, "backward block tile")) return false;
+            double v[3];
+            if (i < nd) {
+              if (!chk(I.c0l + j0t + i, nc, "backward block y")) return false;
+              for (int c = 0; c < 3; ++c) v[c] = y[B.c0 + I.c0l + j0t + i + c * n];
+            } else {
+              if (!chk(I.roff + i - nd, nrows, "backward block rows")) return false;
+              const int64_t r = f.rows[I.roff + i - nd];
+              if (!chk(r, n, "backward block gather")) return false;
+              if (r < B.c1) {
+                if (!chk(r - B.c0, nc, "backward block shared gather")) return false;
+                for (int c = 0; c < 3; ++c) v[c] = -sx[r - B.c0 + c * nc];
+              } else {
+                for (int c = 0; c < 3; ++c) v[c] = -x[r + c * n];
+              }
+            }
+            for (int c = 0; c < 3; ++c) acc[c] += f.Wb[wi] * v[c];
+          }
+          for (int c = 0; c < 3; ++c) sx[I.c0l + j0t + l + c * nc] = acc[c];
+        }
+      }
+    for (int k = 0; k < nc; ++k)
+      for (int c = 0; c < 3; ++c) x[B.c0 + k + c * n] = sx[k + c * nc];
   }
   xout.assign(3 * n, 0.);
   for (int64_t k = 0; k < n; ++k)

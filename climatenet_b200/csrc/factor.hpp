@@ -84,11 +84,70 @@ struct SnInfo {
 void build_sweep_tasks(const Factor& f, int chunk, std::vector<SweepTask>& fwd, std::vector<SweepTask>& bwd,
                        std::vector<SnInfo>& sn);
 
-// Host emulation of the two device sweeps on the tiled layout (same work
-// items, same index arithmetic, every index bounds-checked): solves
-// (M + dt^2 A^T A) x = b for three right-hand sides given vertex-major (3N),
-// result vertex-major.  Returns false with err on an out-of-range index.
-bool emulate_sweeps(const Factor& f, int chunk, const std::vector<double>& b, std::vector<double>& x,
+// ---- subtree blocks ------------------------------------------------------
+// The lower part of the elimination tree is cut into subtrees that one CTA
+// solves alone: the subtree's columns are contiguous in the pivot order, so
+// its slice of the vector lives in shared memory, the levels inside it are
+// separated by CTA barriers, and only rows of supernodes above the subtree
+// (its ancestors) are updated in global memory.  Supernodes that are in no
+// block ("upper" supernodes) keep the dependency-driven per-warp work items.
+constexpr int kMaxBlockLevels = 16;
+constexpr int kMaxBlockCols = 2048;
+
+struct SweepBlock {
+  int c0, c1;    // columns [c0, c1) of the subtree
+  int parent;    // supernode above the subtree root, -1 if none
+  int nlev;      // levels inside the block
+  int item0;     // first item of the block in the item array
+  int lev[kMaxBlockLevels + 1];  // item offsets (from item0) per level, in sweep order
+};
+// One tile of a supernode inside a block: forward, rows [32 tile, 32 tile + m)
+// of W_s over its w = min(ns, 32 tile + 32) columns; backward, columns
+// [32 tile, 32 tile + mc) over its ns - 32 tile + nr rows.
+struct BlockItem {
+  int64_t off;   // tile offset in the forward (backward) tiled copy
+  int c0l;       // first column of the supernode, relative to the block
+  int ns, nr;
+  int tile;
+  int roff;      // offset of the supernode's row set in Factor::rows
+  int pad;
+};
+
+// An upper work item as the device reads it: the SweepTask with the fields
+// of its supernode it needs and its dependency targets per solve, so that one
+// 64-byte load replaces the task load and the dependent supernode load.
+struct alignas(16) UpperItem {
+  int64_t off;     // tile offset in the tiled copy
+  int sn, tile, a0, a1;
+  int c0, ns, nr, roff;
+  int parent;      // parent supernode, -1 if none
+  int wait;        // forward: children of sn; backward: work items of the parent
+  int ntf;         // forward: work items of sn (its last one signals the parent)
+  int pad[3];
+};
+static_assert(sizeof(UpperItem) == 64, "UpperItem is one 64-byte record");
+
+struct SweepPlan {
+  int cut_level = 0, chunk = 0;
+  std::vector<SweepTask> fup, bup;     // upper work items, forward / backward
+  std::vector<SnInfo> sn;              // dependency record (upper supernodes)
+  std::vector<SweepBlock> fblk, bblk;  // blocks, item offsets in forward / backward order
+  std::vector<BlockItem> fitem, bitem;
+  std::vector<UpperItem> fupi, bupi;   // the upper items as the device reads them
+  std::vector<int> upper_cols;         // pivot positions of the upper supernodes' columns
+  int max_block_cols = 0;
+  int64_t block_elems = 0, upper_elems = 0;  // stored W elements per sweep copy
+};
+
+// Blocks are the largest subtrees whose root is at most cut_level and whose
+// columns are contiguous and at most kMaxBlockCols; the rest is upper.
+void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan);
+
+// Host emulation of the two device sweeps of a plan on the tiled layout (same
+// blocks and work items, same index arithmetic, every index bounds-checked):
+// solves (M + dt^2 A^T A) x = b for three right-hand sides given vertex-major
+// (3N), result vertex-major.  Returns false with err on an out-of-range index.
+bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<double>& b, std::vector<double>& x,
                     std::string& err);
 
 // W column offset inside a supernode: column j starts at colstart(j).

@@ -32,8 +32,8 @@ struct DeviceBuffers {
   // state
   double *q = nullptr, *v = nullptr, *tn = nullptr, *qk = nullptr, *cstep = nullptr, *bp = nullptr;
   // solve
-  SweepTask *ftasks = nullptr, *btasks = nullptr;
-  int nf = 0, nb = 0;  // work items per sweep
+  DPlan plan{};       // device copy of the sweep plan (blocks, upper items)
+  SweepPlan host_plan;
   SnInfo* sn = nullptr;
   int* rows = nullptr;
   double *Wf64 = nullptr, *Wb64 = nullptr;  // tiled factor copies (forward / backward)

@@ -8,7 +8,8 @@
 
 namespace pdfb {
 
-// Work queues (2 ints), solve counter and cumulative completion counters.
+// Work queues (4 ints: forward / backward upper items, forward / backward
+// blocks), solve counter and cumulative completion counters.
 struct SweepSync {
   int* queue;
   unsigned long long* epoch;
@@ -16,7 +17,37 @@ struct SweepSync {
   unsigned long long* fchild;  // per supernode: children whose forward finished
   unsigned long long* bdone;   // per supernode: backward work items finished
   int* err;                    // set when a dependency wait gives up
+  int max_spins;               // polls of a dependency counter before giving up
   DTrace trace;                // iteration clock (forward sweep row)
+};
+
+// Device view of a SweepPlan (factor.hpp) and its launch shape.
+struct DPlan {
+  const UpperItem* fup;
+  const UpperItem* bup;
+  int nfup, nbup;
+  const SnInfo* sn;
+  const int* rows;
+  const SweepBlock* fblk;
+  const SweepBlock* bblk;
+  int nblk;
+  const BlockItem* fitem;
+  const BlockItem* bitem;
+  const int* upper_cols;
+  int n_upper;
+  const int* perm;  // pivot position -> vertex
+  int max_cols;     // widest block (shared-memory slice, 3 planes)
+  int smem, grid_f, grid_b;
+};
+
+// Write-back of the solution: v[perm] = x (mode 0) or v[perm] += x (mode 1,
+// FP32 correction), q^k = q_n + dt v.
+struct WriteBack {
+  double* v;
+  double* qk;
+  const double* q;
+  double dt;
+  int mode;
 };
 
 // Analytic and mesh obstacles (device array, refreshed every step for the
@@ -108,14 +139,15 @@ template <typename T>
 void launch_friction_self(dim3 grid, dim3 block, cudaStream_t st, DModel m, DContacts c, T* b, double* newf,
                           const int* iter);
 // Solve vectors b, y, x are three planes of n values (x, y, z components) in
-// pivot order.  y and x must be zero before a solve (k_solve_post / prep).
+// pivot order.  y and x of the upper supernodes must be zero before a solve
+// (the previous solve's write-back, or launch_solve_prep).  One solve is the
+// forward sweep, the backward sweep (with the blocks' write-back) and the
+// write-back of the upper columns.
 template <typename T>
-void launch_solve_sweeps(cudaStream_t st, const SweepTask* ftasks, int nf, const SweepTask* btasks, int nb,
-                         const SnInfo* sn, const int* rows, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
-                         SweepSync sy);
+void configure_solve(DPlan& P);  // shared memory and persistent grids
 template <typename T>
-void launch_solve_post(cudaStream_t st, int n, const int* perm, T* x, T* y, double* v, double* qk, const double* q,
-                       double dt, int mode, SweepSync sy);
+void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
+                         SweepSync sy, WriteBack wb);
 template <typename T>
 void launch_solve_prep(cudaStream_t st, int n, T* x, T* y, SweepSync sy);
 

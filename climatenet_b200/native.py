@@ -54,6 +54,7 @@ def lib():
     L.pdf_export_stats.argtypes = [vp, C.c_char_p]
     L.pdf_get_residual_history.argtypes = [vp, vp, i32, C.POINTER(i32)]
     L.pdf_time_phase.argtypes = [vp, i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.pdf_check_wait_timeout.argtypes = [vp, i32]
     L.pdf_factor_check.argtypes = [C.POINTER(abi.pdf_scene_desc), C.POINTER(abi.pdf_params), vp, vp]
     L.pdf_detect_candidates_noalloc.argtypes = [vp, i32, vp, i32, C.c_double, vp, i32, C.POINTER(i32), vp]
     L.pdf_destroy.argtypes = [vp]

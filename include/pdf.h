@@ -182,6 +182,12 @@ typedef struct pdf_stats {
   int64_t factor_nnz_true;          /* structural nnz(L) without padding        */
   int32_t sweep_chunk;              /* work-item width chosen by the autotuner  */
   double sweep_chunk_ms[3];         /* solve time measured for 32, 64, 128      */
+  /* subtree blocks of the solve schedule chosen by the autotuner: the
+   * elimination-tree level up to which subtrees are solved by one CTA each,
+   * the number of blocks, and the factor elements in blocks / above them */
+  int32_t sweep_cut_level, sweep_blocks;
+  int64_t sweep_block_elems, sweep_upper_elems;
+  double sweep_cut_ms[8];           /* solve time measured for cut levels 0-7   */
 } pdf_stats;
 
 /* One contact, as the reference's CollisionInfo / SelfCollisionInfo plus
@@ -321,15 +327,28 @@ int pdf_get_residual_history(pdf_handle* h, double* out, int32_t cap,
  * sweeps), 1 = local step (projections + right-hand side), 2 = contact
  * projection, 3 = detection (obstacles and self-collision).  The state is not
  * advanced in a meaningful way; call it before or after a measured run.
- * *bytes receives the algorithmic bytes one repetition must move. */
+ * *bytes receives the algorithmic bytes one repetition must move (phases 0,
+ * 1 and 3; 0 for phase 2). */
 int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms,
                    double* bytes);
 
+/* Check of the bounded device waits (no counterpart in the reference): runs
+ * one global solve whose dependency targets lie one solve ahead of the
+ * completion counters, on a schedule whose blocks are only the leaves, so
+ * that no wait of the supernodal sweeps can be satisfied, with each wait
+ * limited to max_spins polls (about 32 ns of sleep each).  Every wait gives
+ * up, the sweeps return, and the call returns PDF_DEVICE_TIMEOUT (or
+ * PDF_INVALID_ARG when the scene's schedule has nothing to wait for).  The
+ * GPU context stays usable; the handle does not: destroy it. */
+int pdf_check_wait_timeout(pdf_handle* h, int32_t max_spins);
+
 /* Host-only consistency check of the factorisation and of the device sweep
  * layout (no GPU needed): builds the global-step matrix of the scene, factors
- * it, and runs a sequential emulation of the two device sweeps (same work
- * items, same tiled layout, every index bounds-checked) to solve
- * (M + dt^2 A^T A) x = b for three right-hand sides (3N, vertex-major). */
+ * it, and runs a sequential emulation of the two device sweeps (same subtree
+ * blocks and work items, same tiled layout, every index bounds-checked) to
+ * solve (M + dt^2 A^T A) x = b for three right-hand sides (3N,
+ * vertex-major), for every schedule the autotuner can choose; they must
+ * agree to 1e-10 relative (else PDF_INVALID_ARG). */
 int pdf_factor_check(const pdf_scene_desc* scene, const pdf_params* params,
                      const double* b, double* x);
 
