@@ -10,6 +10,7 @@
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
 #include <fstream>
+#include <sstream>
 #include <ios>
 #include <limits>
 #include <ostream>
@@ -1350,37 +1351,57 @@ void write_stats_section(std::ostream& of, const char* name, const std::vector<T
 
 extern "C" {
 
+// The stats file's text (SimulationFrictionEstimation::exportStats SFE:756-771
+// around SimulationBase::exportStats SimulationBase.cpp:474-494).
+void write_stats(pdf_handle* h, std::ostream& of) {
+  CK(cudaSetDevice(h->prm.device));
+  CK(cudaStreamSynchronize(h->stream));
+  harvest_all(h);
+  const StatSamples& sm = h->samples;
+  const bool self = h->prm.self_collision != 0;
+  write_stats_section(of, "LHS computation time (µs)", std::vector<double>{1e3 * h->lhs_ms});
+  write_stats_section(of, "Cholesky computation time (µs)", std::vector<double>{1e3 * h->stats.factor_ms});
+  write_stats_section(of, "Iteration time (µs)", sm.iteration);
+  write_stats_section(of, "Collision detection time (µs)", sm.detection);
+  if (self) {
+    write_stats_section(of, "Number of collisions", sm.collisions);
+    write_stats_section(of, "Self collision detection time (µs)", sm.self_detection);
+  }
+  write_stats_section(of, "Number of self collisions", sm.self_collisions);
+  write_stats_section(of, "Solver time (µs)", sm.solver);
+  write_stats_section(of, "Full RHS computation time (µs)", sm.rhs);
+  write_stats_section(of, "Step time (µs)", sm.step);
+  write_stats_section(of, "RHS base computation time (µs)", sm.rhs_base);
+  write_stats_section(of, "RHS friction overhead (µs)", sm.friction);
+  if (self) {
+    write_stats_section(of, "Self collision time (µs)", sm.self_friction);
+    write_stats_section(of, "Self collision ordering time (µs)", sm.ordering);
+  }
+}
+
 int pdf_export_stats(pdf_handle* h, const char* path) {
   if (!h || !path) return fail(h, PDF_INVALID_ARG, "null argument");
   std::ofstream of(path);
   if (!of) return fail(h, PDF_IO_ERROR, std::string("cannot open ") + path);
   return guarded(h, [&]() -> int {
-    CK(cudaSetDevice(h->prm.device));
-    CK(cudaStreamSynchronize(h->stream));
-    harvest_all(h);
-    const StatSamples& sm = h->samples;
-    const bool self = h->prm.self_collision != 0;
-    // SimulationFrictionEstimation::exportStats (SFE:756-771) around
-    // SimulationBase::exportStats (SimulationBase.cpp:474-494)
-    write_stats_section(of, "LHS computation time (µs)", std::vector<double>{1e3 * h->lhs_ms});
-    write_stats_section(of, "Cholesky computation time (µs)", std::vector<double>{1e3 * h->stats.factor_ms});
-    write_stats_section(of, "Iteration time (µs)", sm.iteration);
-    write_stats_section(of, "Collision detection time (µs)", sm.detection);
-    if (self) {
-      write_stats_section(of, "Number of collisions", sm.collisions);
-      write_stats_section(of, "Self collision detection time (µs)", sm.self_detection);
-    }
-    write_stats_section(of, "Number of self collisions", sm.self_collisions);
-    write_stats_section(of, "Solver time (µs)", sm.solver);
-    write_stats_section(of, "Full RHS computation time (µs)", sm.rhs);
-    write_stats_section(of, "Step time (µs)", sm.step);
-    write_stats_section(of, "RHS base computation time (µs)", sm.rhs_base);
-    write_stats_section(of, "RHS friction overhead (µs)", sm.friction);
-    if (self) {
-      write_stats_section(of, "Self collision time (µs)", sm.self_friction);
-      write_stats_section(of, "Self collision ordering time (µs)", sm.ordering);
-    }
+    write_stats(h, of);
     if (!of) return fail(h, PDF_IO_ERROR, std::string("cannot write ") + path);
+    return PDF_OK;
+  });
+}
+
+int pdf_export_stats_text(pdf_handle* h, char* buf, int64_t cap, int64_t* len) {
+  if (!h || !len || (cap > 0 && !buf)) return fail(h, PDF_INVALID_ARG, "null argument");
+  return guarded(h, [&]() -> int {
+    std::ostringstream os;
+    write_stats(h, os);
+    const std::string t = os.str();
+    *len = (int64_t)t.size();
+    if (cap > 0) {
+      const int64_t n = std::min<int64_t>(cap - 1, (int64_t)t.size());
+      std::memcpy(buf, t.data(), (size_t)n);
+      buf[n] = '\0';
+    }
     return PDF_OK;
   });
 }

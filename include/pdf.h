@@ -234,7 +234,16 @@ int pdf_create(const pdf_scene_desc* scene, const pdf_params* params,
                pdf_handle** out);
 
 /* Replaces SimulationBase::step() (src/physics/SimulationBase.cpp:103-173),
- * called nsteps times.  report may be NULL. */
+ * called nsteps times.  report may be NULL.
+ * Fixed per-vertex limits of self-collision detection (the reference's
+ * vectors have none): at most 32 candidate triangles per vertex before the
+ * closest-point filter, and at most 16 pairing partners per vertex; beyond
+ * them, or beyond the contact buffers, the call returns
+ * PDF_CAPACITY_EXCEEDED.  The steps are enqueued together and the error is
+ * read after the last one, so from the first step that overflowed on, the
+ * state (and every later step of the call) was computed with truncated
+ * contacts: after PDF_CAPACITY_EXCEEDED restore a state saved before the
+ * call (pdf_set_state) or recreate the handle. */
 int pdf_step(pdf_handle* h, int32_t nsteps, pdf_step_report* report);
 
 /* State read-back / overwrite (PhysicScene::getGeneralizedPositions/Speeds,
@@ -271,6 +280,11 @@ int pdf_get_self_levels(pdf_handle* h, int32_t* level_ptr, int32_t level_cap,
  * iteration's kernels, since the iterations run inside a CUDA graph. */
 int pdf_get_stats(pdf_handle* h, pdf_stats* out);
 int pdf_export_stats(pdf_handle* h, const char* path);
+/* The same text into a caller buffer: *len receives its length (without the
+ * terminating NUL); at most cap - 1 characters and a NUL are written (cap 0:
+ * query the length).  Lets a caller append the sections to a stream it
+ * already holds, as SimulationBase::exportStats(std::ofstream&) does. */
+int pdf_export_stats_text(pdf_handle* h, char* buf, int64_t cap, int64_t* len);
 
 /* ---- frame output and per-step logs (src/main.cpp:86-114) -------------- */
 /* Enqueues a copy of the current positions (3N doubles) into the handle's
