@@ -254,23 +254,54 @@ def instance_scene(inst):
     return s
 
 
-def batch_scene(n_instances=64, seed=4, spacing=3.0):
+def batch_scene(n_instances=64, seed=4, spacing=3.0, subset=None):
     """All instances of the batch as ONE scene: instance k is mesh k (material
     k) translated by a grid offset, with its own sphere restricted to mesh k
     (material n_instances + k, friction table entry [k][n_instances + k] =
     mu_k).  The global matrix is block diagonal, so one factorisation and one
-    set of launches per PD iteration step every instance together."""
+    set of launches per PD iteration step every instance together.
+    `subset` (instance indices) builds the scene of those instances only, each
+    at the offset it has in the whole batch (one rank's shard)."""
     insts = batch_instances(n_instances, seed)
-    m = len(insts)
+    keep = list(range(len(insts))) if subset is None else sorted(subset)
+    m = len(keep)
     fr = np.zeros((2 * m, 2 * m))
-    for k, it in enumerate(insts):
-        fr[k, m + k] = it["mu"]
+    for j, k in enumerate(keep):
+        fr[j, m + j] = insts[k]["mu"]
     s = Scene(friction=fr)
-    side = int(np.ceil(np.sqrt(m)))
-    for k, it in enumerate(insts):
+    side = int(np.ceil(np.sqrt(len(insts))))
+    for j, k in enumerate(keep):
+        it = insts[k]
         ox, oy = spacing * (k % side), spacing * (k // side)
         p, t = grid_mesh(it["n"], 1.0, z=it["h"], center=(ox, oy))
-        s.add_mesh(p, t, area_density=0.1, bending=1e-2, stretching=1e3, material=k)
+        s.add_mesh(p, t, area_density=0.1, bending=1e-2, stretching=1e3, material=j)
         s.obstacles.append(dict(type=abi.PDF_OBSTACLE_SPHERE, center=(ox, oy, -it["R"]), radius=it["R"],
-                                material=m + k, mesh=k))
-    return s, insts, dict(time_step=2.5e-3, iterations=20)
+                                material=m + j, mesh=j))
+    return s, [insts[k] for k in keep], dict(time_step=2.5e-3, iterations=20)
+
+
+def instance_cost(inst):
+    """Estimated per-iteration work of one n x n instance: nnz(A) of its
+    springs and bending rows plus nnz(L) of a nested-dissection factor of
+    the grid (31/4 N log2 N, George's bound for 2D grids)."""
+    n = inst["n"]
+    N = n * n
+    E = 2 * n * (n - 1) + (n - 1) ** 2
+    B = max(0, n - 2) ** 2
+    return 2 * E + 7 * B + 7.75 * N * np.log2(N)
+
+
+def shard_instances(insts, world):
+    """Instances of a batch onto `world` ranks: greedy bin packing by
+    estimated cost (largest first, each onto the least-loaded rank, ties to
+    the lower rank).  Returns per rank the sorted instance indices.  The
+    instances are independent, so the ranks step their shards without any
+    collective."""
+    order = sorted(range(len(insts)), key=lambda k: (-instance_cost(insts[k]), k))
+    load = [0.0] * world
+    shards = [[] for _ in range(world)]
+    for k in order:
+        r = min(range(world), key=lambda j: (load[j], j))
+        shards[r].append(k)
+        load[r] += instance_cost(insts[k])
+    return [sorted(sh) for sh in shards]

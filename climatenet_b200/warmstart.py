@@ -131,7 +131,7 @@ def train(X, T, epochs=30, batch=4096, lr=2e-3, seed=0, device=0):
     return fold(w, mu, sigma, nu, tau), dict(train_loss=tl, val_loss=vl, samples=len(X))
 
 
-def judge(scene, params, weights, tolerance, steps=10, warmup=3, cap=60):
+def judge(scene, params, weights, tolerance, steps=10, warmup=3, cap=60, start=None):
     """The cold-start solver as judge of the learned warm start.
 
     Runs the scene twice from the same state in iterate-to-tolerance mode
@@ -139,7 +139,8 @@ def judge(scene, params, weights, tolerance, steps=10, warmup=3, cap=60):
     iterations): cold, and with the warm start.  Returns a dict with the mean
     iterations and residuals of both runs and `use`: whether the warm start
     needed fewer iterations (ties go to the cold start, the fallback).
-    `params` are abi.params keyword arguments."""
+    `params` are abi.params keyword arguments; `start` (q, v), when given, is
+    the state both runs restart from after their `warmup` steps."""
     out = {}
     for name, w in (("cold", None), ("warm", weights)):
         p = dict(params)
@@ -149,6 +150,8 @@ def judge(scene, params, weights, tolerance, steps=10, warmup=3, cap=60):
         if w is not None:
             sim.mlp_set_weights(w)
         sim.step(warmup)
+        if start is not None:
+            sim.set_state(*start)
         its, res = [], []
         for _ in range(steps):
             r = sim.step(1)
