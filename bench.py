@@ -18,6 +18,12 @@ seeded.  Arms, all on the same workload:
                        workload first and replaces it when it does not save
                        iterations.
 
+Every arm measures the same stretch of the run: steps 11 .. 10+K, from the
+state after 10 steps of the reference's method from the scene's initial
+state (independent of --warmup: each arm's warm-up steps start from that
+state and the arm returns to it before the timed steps).  Residuals,
+iteration counts and the end-of-stretch position error against the
+reference's method come from a replay of the same steps.
 Iterate-to-tolerance runs as a conditional CUDA-graph loop on the device.
 value = the learned arm's whole-job steps/s, timed on the device (CUDA events
 on the simulation's stream, max over ranks); every arm's steps/s, iterations
@@ -51,6 +57,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "steps/s at 250k-vertex cloth: plain FP64 vs FP32+refine+learned, same residual"
 PLAIN_ITERATIONS = 20
+# steps of the reference's method from the scene's initial state before the
+# measured stretch (the stretch is the same for every arm and every --warmup)
+PREROLL = 10
 
 
 def peaks():
@@ -106,10 +115,16 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-def workload(args):
+def workload(args, rank=0, world=1):
+    """The measured scene.  The batch shards by instance across ranks (cost-
+    based bin packing, each rank steps the block-diagonal scene of its shard,
+    no collective in the step loop); the single cloth runs as replicas."""
     from climatenet_b200 import scenes
     if args.workload == "batch":
-        s, _, pk = scenes.batch_scene(n_instances=64, seed=4)
+        subset = None
+        if world > 1:
+            subset = scenes.shard_instances(scenes.batch_instances(64, seed=4), world)[rank]
+        s, _, pk = scenes.batch_scene(n_instances=64, seed=4, subset=subset)
     else:
         s, pk, _ = scenes.workload(3, n_override=args.n)
     return s, dict(pk)
@@ -123,8 +138,11 @@ def workload_name(args):
             "self-collision tol 2 mm, dt=2e-3" % (args.n, args.n, args.n * args.n))
 
 
-def cpu_baseline(args, steps):
-    """The FP64 CPU oracle (restatement of the reference loop, OpenMP) on the host cores."""
+def cpu_baseline(args, steps, start=None):
+    """The FP64 CPU oracle (restatement of the reference loop, OpenMP) on the
+    host cores: `steps` steps of the reference's method from the state
+    `start` (after one warm-up step from it), or from the scene's initial
+    state."""
     from climatenet_b200 import abi
     from oracle.oracle import Oracle
     s, pk = workload(args)
@@ -132,31 +150,58 @@ def cpu_baseline(args, steps):
     t0 = time.time()
     o = Oracle(s, abi.params(**pk))
     setup = time.time() - t0
+    if start is not None:
+        o.set_state(*start)
     o.step(1)  # warm-up
+    if start is not None:
+        o.set_state(*start)
     t0 = time.time()
     for _ in range(steps):
         o.step(1)
     dt = time.time() - t0
     cores = os.cpu_count()
     return {"value": steps / dt, "unit": "steps/s", "cores": cores, "kind": "port",
-            "sample": "%d steps of the same workload (%d PD iterations, FP64) after 1 warm-up step "
+            "sample": "%d steps of the same workload (%d PD iterations, FP64) %s, after 1 warm-up step "
                       "(set-up %.1f s untimed), OMP_NUM_THREADS=%s"
-                      % (steps, PLAIN_ITERATIONS, setup, os.environ.get("OMP_NUM_THREADS", cores))}
+                      % (steps, PLAIN_ITERATIONS, "from the measured stretch's start state" if start is not None
+                         else "from the initial state", setup, os.environ.get("OMP_NUM_THREADS", cores))}
 
 
 def run_reference(args, rank, world):
+    """The reference arm: the FP64 CPU oracle with the reference's method over
+    the stretch the GPU arms measure (PREROLL steps from the initial state,
+    untimed, then the timed steps), on all host cores; rank 0 only."""
     if rank != 0:
         return
-    steps = max(1, min(args.steps, 3))
-    cb = cpu_baseline(args, steps)
-    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "steps/s", "n_gpus": world,
-            "steps": steps, "warmup": 1, "ms_per_step": 1e3 / cb["value"], "higher_is_better": True,
+    from climatenet_b200 import abi
+    from oracle.oracle import Oracle
+    steps = max(1, min(args.steps, 30))
+    s, pk = workload(args)
+    pk["iterations"] = PLAIN_ITERATIONS
+    t0 = time.time()
+    o = Oracle(s, abi.params(**pk))
+    o.step(PREROLL)
+    start = o.state()
+    o.step(1)  # warm-up
+    o.set_state(*start)
+    setup = time.time() - t0
+    t0 = time.time()
+    for _ in range(steps):
+        o.step(1)
+    value = steps / (time.time() - t0)
+    cores = os.cpu_count()
+    cb = {"kind": "port", "cores": cores, "value": value, "unit": "steps/s",
+          "sample": "steps %d-%d of the run (the stretch the GPU arms time), %d PD iterations, FP64; "
+                    "%d steps before it and 1 warm-up step untimed (%.1f s), OMP_NUM_THREADS=%s"
+                    % (PREROLL + 1, PREROLL + steps, PLAIN_ITERATIONS, PREROLL, setup,
+                       os.environ.get("OMP_NUM_THREADS", cores))}
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world,
+            "steps": steps, "warmup": 1, "ms_per_step": 1e3 / value, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": workload_name(args), "pd_iterations": PLAIN_ITERATIONS,
-                       "parallelism": "replicas"},
-            "cpu_baseline": {k: cb[k] for k in ("kind", "cores", "sample")} | {"value": cb["value"],
-                                                                                "unit": "steps/s"},
-            "e2e": {"value": cb["value"], "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                       "stretch": "steps %d-%d" % (PREROLL + 1, PREROLL + steps), "parallelism": "replicas"},
+            "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": "steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -310,7 +355,7 @@ def e2e_steps(sim, steps, barrier, dist, world, start):
 # forward + backward sweep, from ncu's dram__bytes_read.sum +
 # dram__bytes_write.sum (a profiler is needed to count them, so they cannot be
 # measured inside this run); None for other workloads.
-SOLVE_TRAFFIC_500 = {True: 419.2e6, False: 831.8e6}
+SOLVE_TRAFFIC_500 = {True: None, False: None}
 
 
 def roofline(sim, fp32, n=None):
@@ -327,6 +372,72 @@ def roofline(sim, fp32, n=None):
             "factor_elements_stored": st.factor_nnz, "nnz_L": st.factor_nnz_true}
 
 
+def stretch_start(s, pk, device):
+    """The state every arm's measured stretch starts from: PREROLL steps of
+    the reference's method (FP64, 20 PD iterations) from the scene's initial
+    state.  Fixed, whatever --warmup is."""
+    sim = make_sim(s, pk, PLAIN_ITERATIONS, "fp64", device=device)
+    sim.step(PREROLL)
+    st = sim.state()
+    sim.close()
+    return st
+
+
+def run_arm(sim, K, warmup, start, barrier, dist, units, device):
+    """Warm-up steps (untimed), back to `start`, K timed steps; then a replay
+    of the same K steps from `start` for the residuals, iteration counts and
+    the end-of-stretch positions."""
+    sim.step(warmup)
+    sim.set_state(*start)
+    ms, launches, clk, timed_it = timed_steps(sim, K, barrier, dist, device)
+    sim.set_state(*start)
+    res, curve, mean_it = residual_pass(sim, K)
+    q_end, _ = sim.state()
+    rec = {"steps_per_s": whole_job_rate(units, K, ms), "ms_per_step": ms / K, "mean_pd_iterations": timed_it,
+           "mean_pd_iterations_replay": mean_it, "mean_residual": res, "gpu_launches": launches}
+    return rec, ms, launches, clk, curve, q_end
+
+
+def rel_position_error(q, q_ref):
+    return float(np.abs(q - q_ref).max() / max(np.abs(q_ref).max(), 1e-300))
+
+
+def per_kernel_roofline(sim, fp32, pk_):
+    """Device time (CUDA events, 20 repetitions in isolation) and algorithmic
+    bytes of each phase of a step, against the measured HBM copy bandwidth."""
+    peak = pk_["hbm_gbs"] if pk_ else 6650.0
+    out = []
+    for phase, name in ((0, "global solve: supernodal forward + backward sweeps (%s)" % ("FP32" if fp32 else "FP64")),
+                        (1, "local step: bending projections + vertex right-hand side (FP64)"),
+                        (3, "detection: obstacles + self-collision LBVH refit and traversal")):
+        ms, by = sim.time_phase(phase, reps=20)
+        gbs = by / (ms * 1e-3) / 1e9 if ms > 0 else 0.0
+        out.append({"kernel": name, "ms": ms, "algorithmic_bytes": by, "achieved_gbs": gbs, "frac": gbs / peak})
+    return out
+
+
+def batch_measurement(args, barrier, dist, rank, world, device):
+    """The 64-instance batch (cloths of n ~ U{20..150}, seed 4, one
+    block-diagonal scene per rank; with several ranks each steps its shard),
+    FP32 + refinement, the reference's 20 PD iterations, over the same kind of
+    fixed stretch as the main workload."""
+    from types import SimpleNamespace
+    a = SimpleNamespace(**dict(vars(args), workload="batch"))
+    t0 = time.time()
+    s, pk = workload(a, rank, world)
+    sim = make_sim(s, pk, PLAIN_ITERATIONS, "fp32", device=device)
+    setup_s = time.time() - t0
+    start = stretch_start(s, pk, device)
+    rec, ms, launches, clk, _, _ = run_arm(sim, args.steps, args.warmup, start, barrier, dist, 1, device)
+    st = sim.stats()
+    sim.close()
+    rec.update(instances=64, vertices=s.n_vertices, pd_iterations=PLAIN_ITERATIONS, precision="fp32",
+               setup_s=setup_s, clocks=clk,
+               sweep_schedule={"cut_level": st.sweep_cut_level, "blocks": st.sweep_blocks, "chunk": st.sweep_chunk},
+               parallelism=("instance shards (cost-based bin packing, no collective)" if world > 1 else "single"))
+    return rec
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -338,6 +449,7 @@ def main():
     ap.add_argument("--arm", default="same-residual", choices=["same-residual", "fp64", "fp32"])
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the 64-instance batch measurement")
     args = ap.parse_args()
     args.warmup = max(3, args.warmup)
 
@@ -361,23 +473,23 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    s, pk = workload(args)
+    s, pk = workload(args, rank, world)
     N = s.n_vertices
     K = args.steps
+    # steps of the whole job per timed step: every replica of the cloth is a
+    # job step; the batch's shards together make one step of the batch
+    units = 1 if args.workload == "batch" else world
     line_extra = {}
     weights = None
+    pk_ = peaks()
+    start = stretch_start(s, pk, local)
 
     # ---- the reference's method: FP64, 20 PD iterations per step ---------
     sim_r = make_sim(s, pk, PLAIN_ITERATIONS, "fp64", device=local)
-    sim_r.step(args.warmup)
-    start_state = sim_r.state()
-    ms_r, launches_r, clk_r, _ = timed_steps(sim_r, K, barrier, dist, local)
-    # residuals over the same stretch of the run, replayed from its start
-    sim_r.set_state(*start_state)
-    res_r, curve_r, _ = residual_pass(sim_r, K)
-    line_extra["fp64_plain_fixed20"] = {"steps_per_s": whole_job_rate(world, K, ms_r), "ms_per_step": ms_r / K,
-                                        "pd_iterations": PLAIN_ITERATIONS, "mean_residual": res_r,
-                                        "residual_curve": curve_r, "gpu_launches": launches_r}
+    rec_r, ms_r, launches_r, clk_r, curve_r, q_ref = run_arm(sim_r, K, args.warmup, start, barrier, dist, units, local)
+    res_r = rec_r["mean_residual"]
+    rec_r.update(pd_iterations=PLAIN_ITERATIONS, residual_curve=curve_r)
+    line_extra["fp64_plain_fixed20"] = rec_r
     line_extra["roofline_fp64"] = roofline(sim_r, False, args.n if args.workload == "cloth" else None)
     if args.arm == "fp64":
         sim, ms, launches, clk, iters, res, prec, tol = (sim_r, ms_r, launches_r, clk_r, PLAIN_ITERATIONS, res_r,
@@ -385,7 +497,8 @@ def main():
     else:
         sim_r.close()
         # ---- same residual: every arm iterates to tau (the mean residual the
-        # reference's method reaches after 20 iterations), cap 60 -----------
+        # reference's method reaches after 20 iterations over the same
+        # stretch), cap 60 -----------------------------------------------
         tol = res_r
         # no contact in the stretch (tau = 0): no residual to reach, so the
         # arms run the reference's 20 iterations
@@ -399,7 +512,7 @@ def main():
             # stretch of the workload and is the fallback when it does not help
             pj = dict(pk)
             pj["precision"] = abi.PDF_FP32_REFINE
-            verdict = warmstart.judge(s, pj, weights, tol, steps=10, warmup=args.warmup, cap=cap)
+            verdict = warmstart.judge(s, pj, weights, tol, steps=10, warmup=args.warmup, cap=cap, start=start)
             verdict["use"] = bool(verdict["use"] and tinfo["beats_cold_on_validation"])
             line_extra["warm_start_judge"] = verdict
             if not verdict["use"]:
@@ -407,15 +520,11 @@ def main():
             arms.append(("learned", "fp32", weights))
         for name, precision, w in arms:
             sim = make_sim(s, pk, cap, precision, w, device=local, tolerance=tol)
-            sim.step(args.warmup)
-            start_state = sim.state()
-            ms, launches, clk, timed_it = timed_steps(sim, K, barrier, dist, local)
-            sim.set_state(*start_state)
-            res, _, mean_it = residual_pass(sim, K)
-            line_extra[name] = {"steps_per_s": whole_job_rate(world, K, ms), "ms_per_step": ms / K,
-                                "mean_pd_iterations": timed_it, "mean_pd_iterations_replay": mean_it,
-                                "mean_residual": res, "tolerance": tol,
-                                "iteration_cap": cap, "gpu_launches": launches}
+            rec, ms, launches, clk, _, q_end = run_arm(sim, K, args.warmup, start, barrier, dist, units, local)
+            rec.update(tolerance=tol, iteration_cap=cap,
+                       position_error_vs_fixed20=rel_position_error(q_end, q_ref))
+            line_extra[name] = rec
+            res = rec["mean_residual"]
             if name != arms[-1][0]:
                 sim.close()
         prec, iters = "fp32", cap
@@ -425,43 +534,53 @@ def main():
         line_extra["speedup_vs_fixed20"] = (line_extra[head]["steps_per_s"] /
                                             line_extra["fp64_plain_fixed20"]["steps_per_s"])
 
-    value = whole_job_rate(world, K, ms)
+    value = whole_job_rate(units, K, ms)
     # end to end over the same stretch of the run as `value`: from the state
     # the timed steps started from
-    e2e_value = e2e_steps(sim, K, barrier, dist, world, start_state)
+    e2e_value = e2e_steps(sim, K, barrier, dist, units, start)
     roof = roofline(sim, prec == "fp32", args.n if args.workload == "cloth" else None)
-    ms_local, bytes_local = sim.time_phase(1, reps=20)
+    roof["per_kernel"] = per_kernel_roofline(sim, prec == "fp32", pk_)
     st = sim.stats()
+    batch = None
+    if args.workload == "cloth" and not args.no_batch:
+        batch = batch_measurement(args, barrier, dist, rank, world, local)
     if dist is not None:
         dist.barrier()
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "steps/s", "n_gpus": world, "steps": K,
             "warmup": args.warmup, "ms_per_step": ms / K, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None,
+            "scaling": "strong" if args.workload == "batch" else "weak", "vs_baseline": None,
             "dtype": "f64" if prec == "fp64" else "f32 solves + f64 residual / state",
             "data": "synthetic",
             "config": {"workload": workload_name(args), "vertices": N, "arm": args.arm,
+                       "stretch": "steps %d-%d of the run: %d steps of the reference's method from the initial "
+                                  "state, then the timed steps (independent of --warmup)"
+                                  % (PREROLL + 1, PREROLL + K, PREROLL),
                        "pd_iterations": iters, "precision": prec, "residual_tolerance": tol,
                        "warm_start": ("mlp" if weights is not None else
                                       ("none (the cold-start judge rejected the learned warm start)"
                                        if "warm_start_judge" in line_extra else "none")),
-                       "parallelism": "replicas" if world > 1 else "single",
+                       "parallelism": ("instance shards (cost-based bin packing, no collective)"
+                                       if args.workload == "batch" else "replicas") if world > 1 else "single",
                        "l2": "inputs larger than L2: factor panels %.0f MB per sweep copy"
                              % (st.factor_nnz * (4 if prec == "fp32" else 8) / 1e6),
                        "nnz_L": st.factor_nnz_true, "supernodes": st.n_supernodes, "etree_levels": st.n_levels,
+                       "sweep_schedule": {"cut_level": st.sweep_cut_level, "blocks": st.sweep_blocks,
+                                          "chunk": st.sweep_chunk, "block_elements": st.sweep_block_elems,
+                                          "upper_elements": st.sweep_upper_elems},
                        "mean_residual": res},
             "roofline": roof,
-            "local_step": {"ms": ms_local, "algorithmic_bytes": bytes_local,
-                           "achieved_gbs": bytes_local / (ms_local * 1e-3) / 1e9},
             "e2e": {"value": e2e_value, "unit": "steps/s", "h2d_bytes_per_step": 2 * 24 * N,
                     "d2h_bytes_per_step": 2 * 24 * N},
             "gpu_launches": launches,
             "clocks": clk,
         }
         line.update(line_extra)
+        if batch is not None:
+            line["batch"] = batch
         if not args.no_cpu and world == 1:
-            line["cpu_baseline"] = cpu_baseline(args, args.cpu_steps)
+            line["cpu_baseline"] = cpu_baseline(args, args.cpu_steps, start)
         print(json.dumps(line), flush=True)
     sim.close()
     if dist is not None:

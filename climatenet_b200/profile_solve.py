@@ -1,10 +1,21 @@
-"""Runs the global solve of the 500 x 500 cloth workload in isolation, for
-profiling: one full step (so that the right-hand side is realistic), then
-`reps` back-to-back forward + backward supernodal sweeps.
+"""Runs parts of the 500 x 500 cloth workload for profiling.
+
+Default: one full step (so that the right-hand side is realistic), then
+`reps` back-to-back repetitions of one phase in isolation (0 = global solve:
+forward + backward supernodal sweeps and the write-back, 1 = local step,
+2 = contact projection, 3 = detection).  With --steps K: K full steps of the
+step loop instead (for a launch list of whole steps).  With --mlp-samples M:
+one forward and one gradient launch of the warm-start MLP on M seeded random
+samples instead (for the tensor-pipe counters of k_mlp_forward / k_mlp_grad).
 
   python -m climatenet_b200.profile_solve [--n 500] [--reps 3] [--precision fp64|fp32]
+                                          [--phase 0] [--steps 0] [--iterations 20]
+                                          [--mlp-samples 0]
 """
 import argparse
+import time
+
+import numpy as np
 
 from . import abi, native, scenes
 
@@ -15,12 +26,35 @@ def main():
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--phase", type=int, default=0)
+    ap.add_argument("--steps", type=int, default=0)
+    ap.add_argument("--iterations", type=int, default=20)
+    ap.add_argument("--mlp-samples", type=int, default=0)
     args = ap.parse_args()
+    if args.mlp_samples > 0:
+        rng = np.random.default_rng(0)
+        X = rng.standard_normal((args.mlp_samples, 10)).astype(np.float32)
+        T = rng.standard_normal((args.mlp_samples, 3)).astype(np.float32)
+        w = native.mlp_init(1)
+        t0 = time.time()
+        native.mlp_forward(w, X)
+        native.mlp_gradient(w, X, T)
+        print("MLP forward + gradient on %d samples: %.3f s wall (host copies included)"
+              % (args.mlp_samples, time.time() - t0))
+        return
     s, pk, _ = scenes.workload(3, n_override=args.n)
+    pk["iterations"] = args.iterations
     if args.precision == "fp32":
         pk["precision"] = abi.PDF_FP32_REFINE
     sim = native.Simulation(s, abi.params(**pk))
+    st = sim.stats()
+    print("schedule: cut level %d, %d blocks, chunk %d; solve ms per cut level %s"
+          % (st.sweep_cut_level, st.sweep_blocks, st.sweep_chunk, [round(x, 4) for x in st.sweep_cut_ms]))
     sim.step(1)
+    if args.steps > 0:
+        r = sim.step(args.steps)
+        print("%d steps: %.3f ms per step on the device, %d PD iterations in the last step"
+              % (args.steps, r.device_ms / args.steps, r.iterations))
+        return
     ms, by = sim.time_phase(args.phase, args.reps)
     print("phase %d: %.4f ms per repetition, %.1f MB algorithmic, %.1f GB/s"
           % (args.phase, ms, by / 1e6, by / (ms * 1e-3) / 1e9 if ms > 0 else 0.0))
