@@ -82,6 +82,8 @@ void free_plan(DPlan& P) {
   free_dev(P.fitem);
   free_dev(P.bitem);
   free_dev(P.upper_cols);
+  free_dev(P.rows_loc);
+  free_dev(P.bidx);
 }
 
 // Sweep plan (subtree blocks + upper work items, factor.hpp) on the device.
@@ -109,11 +111,12 @@ void build_schedule(pdf_handle* h, int chunk, int cut_level) {
   P.upper_cols = upload(hp.upper_cols);
   P.n_upper = (int)hp.upper_cols.size();
   P.perm = h->d.perm;
+  P.rows_loc = upload(hp.rows_loc);
+  P.bidx = upload(hp.bidx.empty() ? std::vector<int>(kSlab, 0) : hp.bidx);
   P.max_cols = hp.max_block_cols;
-  if (h->fp32)
-    configure_solve<float>(P);
-  else
-    configure_solve<double>(P);
+  P.max_ext = hp.max_block_ext;
+  const bool fits = h->fp32 ? configure_solve<float>(P) : configure_solve<double>(P);
+  if (!fits) throw CudaFail("the sweep's block kernels do not fit the device's shared memory");
   h->n_levels = f.n_levels;
   h->stats.sweep_chunk = chunk;
   h->stats.sweep_cut_level = cut_level;

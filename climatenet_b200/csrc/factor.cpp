@@ -353,17 +353,17 @@ bool factorize(const Model& m, double dt, int leaf_size, Factor& f, std::string&
       for (int64_t t = 0; t < ft0[s + 1] - ft0[s]; ++t) {
         const int64_t w = std::min(ns, kTile * t + kTile);
         const int64_t m = std::min<int64_t>(kTile, ns + nr - kTile * t);
-        f.ftile_off[ft0[s] + t + 1] = f.ftile_off[ft0[s] + t] + m * w;
+        f.ftile_off[ft0[s] + t + 1] = f.ftile_off[ft0[s] + t] + pad_tile(m * w);
       }
       for (int64_t t = 0; t < f.sn_btile0[s + 1] - f.sn_btile0[s]; ++t) {
         const int64_t hgt = ns - kTile * t + nr;
         const int64_t mc = std::min<int64_t>(kTile, ns - kTile * t);
-        f.btile_off[f.sn_btile0[s] + t + 1] = f.btile_off[f.sn_btile0[s] + t] + mc * hgt;
+        f.btile_off[f.sn_btile0[s] + t + 1] = f.btile_off[f.sn_btile0[s] + t] + pad_tile(mc * hgt);
       }
     }
     f.sn_ftile0 = ft0;
-    f.Wf.assign(f.ftile_off[nft], 0.);
-    f.Wb.assign(f.btile_off[nbt], 0.);
+    f.Wf.assign(f.ftile_off[nft] + kTilePad, 0.);
+    f.Wb.assign(f.btile_off[nbt] + kTilePad, 0.);
     f.tiled_w = std::max(f.ftile_off[nft], f.btile_off[nbt]);
 #pragma omp parallel for schedule(dynamic, 4)
     for (int s = 0; s < S; ++s) {
@@ -484,7 +484,7 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
   }
   auto eligible = [&](int s) {
     return f.sn_level[s] <= cut_level && f.sn_level[s] < kMaxBlockLevels && cnt[s] <= kMaxBlockCols &&
-           f.sn_c0[s] + f.sn_ns[s] - lo[s] == cnt[s];
+           f.sn_nr[s] <= kMaxBlockExt && f.sn_c0[s] + f.sn_ns[s] - lo[s] == cnt[s];
   };
   std::vector<int> blk(S, -1);
   std::vector<int> roots;
@@ -499,6 +499,7 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
     }
   }
   const int nb = (int)roots.size();
+  plan.rows_loc.assign(f.rows.size(), -1);
   std::vector<std::vector<int>> members(nb);
   for (int s = 0; s < S; ++s)
     if (blk[s] >= 0) members[blk[s]].push_back(s);
@@ -520,7 +521,19 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
     fb.c1 = bb.c1 = f.sn_c0[r] + f.sn_ns[r];
     fb.parent = bb.parent = f.sn_parent[r];
     fb.nlev = bb.nlev = f.sn_level[r] + 1;
+    fb.ext0 = bb.ext0 = (int)f.sn_roff[r];
+    fb.next = bb.next = f.sn_nr[r];
     plan.max_block_cols = std::max(plan.max_block_cols, fb.c1 - fb.c0);
+    plan.max_block_ext = std::max(plan.max_block_ext, fb.next);
+    // where each row of each member lives in the block's shared vector
+    const int nc = fb.c1 - fb.c0;
+    const int* rr = f.rows.data() + f.sn_roff[r];
+    for (int s : members[b])
+      for (int k = 0; k < f.sn_nr[s]; ++k) {
+        const int row = f.rows[f.sn_roff[s] + k];
+        plan.rows_loc[f.sn_roff[s] + k] =
+            row < fb.c1 ? row - fb.c0 : nc + (int)(std::lower_bound(rr, rr + fb.next, row) - rr);
+      }
     plan.block_elems += cost[b];
     std::vector<std::vector<int>> by_lev(fb.nlev);
     for (int s : members[b]) by_lev[f.sn_level[s]].push_back(s);
@@ -538,9 +551,15 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
       const int L = bb.nlev - 1 - k;
       bb.lev[k] = (int)plan.bitem.size() - bb.item0;
       for (int s : by_lev[L])
-        for (int64_t t = f.sn_btile0[s]; t < f.sn_btile0[s + 1]; ++t)
-          plan.bitem.push_back({f.btile_off[t], f.sn_c0[s] - bb.c0, f.sn_ns[s], f.sn_nr[s],
-                                (int)(t - f.sn_btile0[s]), (int)f.sn_roff[s], 0});
+        for (int64_t t = f.sn_btile0[s]; t < f.sn_btile0[s + 1]; ++t) {
+          const int tl = (int)(t - f.sn_btile0[s]);
+          const int c0l = f.sn_c0[s] - bb.c0, j0t = kTile * tl, nd = f.sn_ns[s] - j0t, h = nd + f.sn_nr[s];
+          plan.bitem.push_back({f.btile_off[t], c0l, f.sn_ns[s], f.sn_nr[s], tl, (int)f.sn_roff[s],
+                                (int)plan.bidx.size()});
+          for (int i = 0; i < h; ++i)
+            plan.bidx.push_back(i < nd ? -1 - (c0l + j0t + i) : plan.rows_loc[f.sn_roff[s] + i - nd]);
+          while (plan.bidx.size() % kSlab) plan.bidx.push_back(0);
+        }
     }
     bb.lev[bb.nlev] = (int)plan.bitem.size() - bb.item0;
     plan.fblk.push_back(fb);
@@ -561,6 +580,11 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
   }
   for (const SweepTask& t : plan.fup) plan.sn[t.sn].ntf++;
   for (const SweepTask& t : plan.bup) plan.sn[t.sn].ntb++;
+  // the blocks finish in an earlier launch than the upper items: an upper
+  // supernode waits only for its upper children
+  std::vector<int> upper_children(S, 0);
+  for (int s = 0; s < S; ++s)
+    if (blk[s] < 0 && f.sn_parent[s] >= 0) upper_children[f.sn_parent[s]]++;
   auto upper = [&](const SweepTask& t, bool fwd) {
     const SnInfo& q = plan.sn[t.sn];
     UpperItem u{};
@@ -574,7 +598,7 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
     u.nr = q.nr;
     u.roff = (int)q.roff;
     u.parent = q.parent;
-    u.wait = fwd ? q.nchild : (q.parent >= 0 ? plan.sn[q.parent].ntb : 0);
+    u.wait = fwd ? upper_children[t.sn] : (q.parent >= 0 ? plan.sn[q.parent].ntb : 0);
     u.ntf = q.ntf;
     return u;
   };
@@ -597,46 +621,56 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
   };
   const int64_t nWf = (int64_t)f.Wf.size(), nWb = (int64_t)f.Wb.size(), nrows = (int64_t)f.rows.size();
   const int64_t nfi = (int64_t)plan.fitem.size(), nbi = (int64_t)plan.bitem.size();
-  // forward, blocks: the block's slice of b in "shared memory"
+  // forward, blocks: the block's slice of b and its ext rows in "shared memory"
+  const int64_t nloc = (int64_t)plan.rows_loc.size();
   for (const SweepBlock& B : plan.fblk) {
-    const int nc = B.c1 - B.c0;
-    if (nc <= 0 || nc > plan.max_block_cols || B.nlev > kMaxBlockLevels) {
+    const int nc = B.c1 - B.c0, ld = nc + B.next;
+    if (nc <= 0 || nc > plan.max_block_cols || B.next > plan.max_block_ext || B.nlev > kMaxBlockLevels) {
       err = "bad block extent";
       return false;
     }
     if (!chk(B.c0, n, "block columns") || !chk(B.c1 - 1, n, "block columns")) return false;
-    std::vector<double> sb(3 * (size_t)nc);
+    std::vector<double> sv(3 * (size_t)ld, 0.);
     for (int k = 0; k < nc; ++k)
-      for (int c = 0; c < 3; ++c) sb[k + c * nc] = b[B.c0 + k + c * n];
+      for (int c = 0; c < 3; ++c) sv[k + c * ld] = b[B.c0 + k + c * n];
     for (int L = 0; L < B.nlev; ++L)
       for (int it = B.item0 + B.lev[L]; it < B.item0 + B.lev[L + 1]; ++it) {
         if (!chk(it, nfi, "forward block items")) return false;
         const BlockItem& I = plan.fitem[it];
         const int m = std::min(kTile, I.ns + I.nr - kTile * I.tile), w = std::min(I.ns, kTile * I.tile + kTile);
+        if ((I.off % kTilePad) != 0) {
+          err = "forward tile not aligned";
+          return false;
+        }
         for (int l = 0; l < m; ++l) {
           double acc[3] = {0, 0, 0};
           for (int j = 0; j < w; ++j) {
             const int64_t wi = I.off + (int64_t)j * m + l;
             if (!chk(wi, nWf, "forward block tile") || !chk(I.c0l + j, nc, "forward block vector")) return false;
-            for (int c = 0; c < 3; ++c) acc[c] += f.Wf[wi] * sb[I.c0l + j + c * nc];
+            for (int c = 0; c < 3; ++c) acc[c] += f.Wf[wi] * sv[I.c0l + j + c * ld];
           }
           const int row = kTile * I.tile + l;
           if (row < I.ns) {
             if (!chk(I.c0l + row, nc, "forward block y")) return false;
             for (int c = 0; c < 3; ++c) y[B.c0 + I.c0l + row + c * n] = acc[c];
           } else {
-            if (!chk(I.roff + row - I.ns, nrows, "forward block rows")) return false;
-            const int64_t r = f.rows[I.roff + row - I.ns];
-            if (!chk(r, n, "forward block scatter")) return false;
-            if (r < B.c1) {
-              if (!chk(r - B.c0, nc, "forward block shared scatter")) return false;
-              for (int c = 0; c < 3; ++c) sb[r - B.c0 + c * nc] -= acc[c];
-            } else {
-              for (int c = 0; c < 3; ++c) b[r + c * n] -= acc[c];
-            }
+            if (!chk(I.roff + row - I.ns, nloc, "forward block rows")) return false;
+            const int loc = plan.rows_loc[I.roff + row - I.ns];
+            if (!chk(loc, ld, "forward block shared scatter")) return false;
+            for (int c = 0; c < 3; ++c) sv[loc + c * ld] -= acc[c];
           }
         }
       }
+    // the ext rows' accumulated updates go to b once
+    for (int e = 0; e < B.next; ++e) {
+      if (!chk(B.ext0 + e, nrows, "forward block ext rows")) return false;
+      const int64_t r = f.rows[B.ext0 + e];
+      if (!chk(r, n, "forward block ext scatter") || r < B.c1) {
+        if (err.empty()) err = "ext row inside its block";
+        return false;
+      }
+      for (int c = 0; c < 3; ++c) b[r + c * n] += sv[nc + e + c * ld];
+    }
   }
   // forward, upper work items (the records the device reads)
   for (const UpperItem& tk : plan.fupi) {
@@ -687,42 +721,50 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
         for (int c = 0; c < 3; ++c) x[s.c0 + col + c * n] += acc[c];
     }
   }
-  // backward, blocks: x of the block's columns in "shared memory"
+  // backward, blocks: x of the block's columns and ext rows, and y of its
+  // columns, in "shared memory"
+  const int64_t nbidx = (int64_t)plan.bidx.size();
   for (const SweepBlock& B : plan.bblk) {
-    const int nc = B.c1 - B.c0;
-    std::vector<double> sx(3 * (size_t)nc, 0.);
+    const int nc = B.c1 - B.c0, ld = nc + B.next;
+    std::vector<double> sx(3 * (size_t)ld, 0.), ys(3 * (size_t)nc, 0.);
+    for (int e = 0; e < B.next; ++e) {
+      if (!chk(B.ext0 + e, nrows, "backward block ext rows")) return false;
+      const int64_t r = f.rows[B.ext0 + e];
+      if (!chk(r, n, "backward block ext gather")) return false;
+      for (int c = 0; c < 3; ++c) sx[nc + e + c * ld] = x[r + c * n];
+    }
+    for (int k = 0; k < nc; ++k)
+      for (int c = 0; c < 3; ++c) ys[k + c * nc] = y[B.c0 + k + c * n];
     for (int L = 0; L < B.nlev; ++L)
       for (int it = B.item0 + B.lev[L]; it < B.item0 + B.lev[L + 1]; ++it) {
         if (!chk(it, nbi, "backward block items")) return false;
         const BlockItem& I = plan.bitem[it];
         const int j0t = kTile * I.tile, nd = I.ns - j0t, mc = std::min(kTile, nd), h = nd + I.nr;
+        if ((I.off % kTilePad) != 0 || (I.idx0 % kSlab) != 0) {
+          err = "backward tile or index list not aligned";
+          return false;
+        }
         for (int l = 0; l < mc; ++l) {
           double acc[3] = {0, 0, 0};
           for (int i = 0; i < h; ++i) {
             const int64_t wi = I.off + (int64_t)i * mc + l;
-            if (!chk(wi, nWb, "backward block tile")) return false;
+            if (!chk(wi, nWb, "backward block tile") || !chk(I.idx0 + i, nbidx, "backward block index")) return false;
+            const int idx = plan.bidx[I.idx0 + i];
             double v[3];
-            if (i < nd) {
-              if (!chk(I.c0l + j0t + i, nc, "backward block y")) return false;
-              for (int c = 0; c < 3; ++c) v[c] = y[B.c0 + I.c0l + j0t + i + c * n];
+            if (idx < 0) {
+              if (!chk(-1 - idx, nc, "backward block y")) return false;
+              for (int c = 0; c < 3; ++c) v[c] = ys[-1 - idx + c * nc];
             } else {
-              if (!chk(I.roff + i - nd, nrows, "backward block rows")) return false;
-              const int64_t r = f.rows[I.roff + i - nd];
-              if (!chk(r, n, "backward block gather")) return false;
-              if (r < B.c1) {
-                if (!chk(r - B.c0, nc, "backward block shared gather")) return false;
-                for (int c = 0; c < 3; ++c) v[c] = -sx[r - B.c0 + c * nc];
-              } else {
-                for (int c = 0; c < 3; ++c) v[c] = -x[r + c * n];
-              }
+              if (!chk(idx, ld, "backward block shared gather")) return false;
+              for (int c = 0; c < 3; ++c) v[c] = -sx[idx + c * ld];
             }
             for (int c = 0; c < 3; ++c) acc[c] += f.Wb[wi] * v[c];
           }
-          for (int c = 0; c < 3; ++c) sx[I.c0l + j0t + l + c * nc] = acc[c];
+          for (int c = 0; c < 3; ++c) sx[I.c0l + j0t + l + c * ld] = acc[c];
         }
       }
     for (int k = 0; k < nc; ++k)
-      for (int c = 0; c < 3; ++c) x[B.c0 + k + c * n] = sx[k + c * nc];
+      for (int c = 0; c < 3; ++c) x[B.c0 + k + c * n] = sx[k + c * ld];
   }
   xout.assign(3 * n, 0.);
   for (int64_t k = 0; k < n; ++k)

@@ -29,7 +29,8 @@
 //                        (h_t = ns - 32t + nr); element (local row i, col
 //                        32t+l) at off + mc i + l.
 //    Only the last tile of a supernode is narrower than 32; no rows or lanes
-//    of zeros are stored.
+//    of zeros are stored (each tile is padded to a multiple of kTilePad
+//    elements).
 #pragma once
 #include <cstdint>
 #include <string>
@@ -40,6 +41,12 @@
 namespace pdfb {
 
 constexpr int kTile = 32;
+// Every tile of the tiled copies starts on a multiple of kTilePad elements
+// (16 bytes in FP32 and FP64), the alignment bulk asynchronous copies need;
+// the arrays end with kTilePad elements of zeros, so that a copy rounded up
+// to 16 bytes stays inside them.
+constexpr int kTilePad = 4;
+inline int64_t pad_tile(int64_t elems) { return (elems + kTilePad - 1) / kTilePad * kTilePad; }
 
 struct Factor {
   int N = 0;
@@ -88,29 +95,37 @@ void build_sweep_tasks(const Factor& f, int chunk, std::vector<SweepTask>& fwd, 
 // The lower part of the elimination tree is cut into subtrees that one CTA
 // solves alone: the subtree's columns are contiguous in the pivot order, so
 // its slice of the vector lives in shared memory, the levels inside it are
-// separated by CTA barriers, and only rows of supernodes above the subtree
-// (its ancestors) are updated in global memory.  Supernodes that are in no
+// separated by CTA barriers, and the factor streams in through bulk
+// asynchronous copies.  The rows a subtree touches outside itself are exactly
+// its root's row set R_root (a child's rows beyond its parent's columns are
+// rows of the parent), so they live in shared memory too ("ext" rows): the
+// forward sweep accumulates their updates there and adds them to b once per
+// block, the backward sweep loads their x once per block.  Supernodes in no
 // block ("upper" supernodes) keep the dependency-driven per-warp work items.
 constexpr int kMaxBlockLevels = 16;
-constexpr int kMaxBlockCols = 2048;
+constexpr int kMaxBlockCols = 1536;
+constexpr int kMaxBlockExt = 1024;
+constexpr int kSlab = 16;  // columns (forward) / rows (backward) per bulk copy
 
 struct SweepBlock {
   int c0, c1;    // columns [c0, c1) of the subtree
   int parent;    // supernode above the subtree root, -1 if none
   int nlev;      // levels inside the block
   int item0;     // first item of the block in the item array
+  int ext0;      // its ext rows are Factor::rows[ext0, ext0 + next) (R of the root)
+  int next;
   int lev[kMaxBlockLevels + 1];  // item offsets (from item0) per level, in sweep order
 };
 // One tile of a supernode inside a block: forward, rows [32 tile, 32 tile + m)
 // of W_s over its w = min(ns, 32 tile + 32) columns; backward, columns
-// [32 tile, 32 tile + mc) over its ns - 32 tile + nr rows.
+// [32 tile, 32 tile + mc) over its h = ns - 32 tile + nr rows.
 struct BlockItem {
   int64_t off;   // tile offset in the forward (backward) tiled copy
   int c0l;       // first column of the supernode, relative to the block
   int ns, nr;
   int tile;
-  int roff;      // offset of the supernode's row set in Factor::rows
-  int pad;
+  int roff;      // offset of the supernode's row set in Factor::rows (and rows_loc)
+  int idx0;      // backward: offset of the tile's row-index list in bidx (multiple of 4)
 };
 
 // An upper work item as the device reads it: the SweepTask with the fields
@@ -135,12 +150,20 @@ struct SweepPlan {
   std::vector<BlockItem> fitem, bitem;
   std::vector<UpperItem> fupi, bupi;   // the upper items as the device reads them
   std::vector<int> upper_cols;         // pivot positions of the upper supernodes' columns
-  int max_block_cols = 0;
+  // per entry of Factor::rows of a block supernode: the row's place in the
+  // block's shared vector (column - c0 inside the block, nc + ext index outside)
+  std::vector<int> rows_loc;
+  // backward tiles of blocks: per row of the tile, padded to kSlab rows, where
+  // its vector entry is: >= 0 the shared vector (x), < 0 the shared y slice
+  // (entry -1 - k is column k of the block)
+  std::vector<int> bidx;
+  int max_block_cols = 0, max_block_ext = 0;
   int64_t block_elems = 0, upper_elems = 0;  // stored W elements per sweep copy
 };
 
 // Blocks are the largest subtrees whose root is at most cut_level and whose
-// columns are contiguous and at most kMaxBlockCols; the rest is upper.
+// columns are contiguous, at most kMaxBlockCols, with at most kMaxBlockExt
+// rows outside; the rest is upper.
 void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan);
 
 // Host emulation of the two device sweeps of a plan on the tiled layout (same

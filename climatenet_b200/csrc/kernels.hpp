@@ -35,9 +35,13 @@ struct DPlan {
   const BlockItem* bitem;
   const int* upper_cols;
   int n_upper;
-  const int* perm;  // pivot position -> vertex
-  int max_cols;     // widest block (shared-memory slice, 3 planes)
-  int smem, grid_f, grid_b;
+  const int* perm;      // pivot position -> vertex
+  const int* rows_loc;  // block supernodes: place of each row in the block's shared vector
+  const int* bidx;      // backward block tiles: per-row vector index lists
+  int max_cols;         // widest block (shared-memory slice, 3 planes)
+  int max_ext;          // most rows outside a block
+  int smem_f, smem_b;   // dynamic shared memory of the forward / backward block kernels
+  int grid_bf, grid_bb, grid_uf, grid_ub;
 };
 
 // Write-back of the solution: v[perm] = x (mode 0) or v[perm] += x (mode 1,
@@ -144,7 +148,7 @@ void launch_friction_self(dim3 grid, dim3 block, cudaStream_t st, DModel m, DCon
 // forward sweep, the backward sweep (with the blocks' write-back) and the
 // write-back of the upper columns.
 template <typename T>
-void configure_solve(DPlan& P);  // shared memory and persistent grids
+bool configure_solve(DPlan& P);  // shared memory and grids; false if a block kernel does not fit
 template <typename T>
 void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
                          SweepSync sy, WriteBack wb);

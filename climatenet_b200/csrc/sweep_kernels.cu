@@ -6,29 +6,33 @@
 // W_s = [D^-1 ; L_R D^-1] (see factor.hpp) in 32-lane tiles:
 //   forward : y_s = D^-1 b_s ; b_R -= (L_R D^-1) b_s
 //   backward: x_s = W_s^T [y_s ; -x_R]
-// A sweep is ONE persistent launch with two kinds of work (factor.hpp,
-// SweepPlan):
-//  * subtree blocks — the lower levels of the elimination tree, cut into
-//    subtrees with contiguous columns.  One CTA solves a block alone: the
-//    block's slice of the vector sits in shared memory, its levels are
-//    separated by CTA barriers, each tile of each supernode is one warp's
-//    item, and only rows of the block's ancestors are updated in global
-//    memory.  No dependency counter is touched inside a block.
-//  * upper work items — the supernodes above the blocks, split into 32-row
-//    (forward) / 32-column (backward) tiles times column / row chunks, taken
-//    by warps from a queue in elimination-tree order; a warp waits (bounded
-//    spin) only for the supernodes its item depends on: forward, all children
-//    complete (block roots signal once per block); backward, the parent
-//    complete.  Partial sums land in y / b_R / x with atomics.
-// The forward launch runs the blocks first (they depend on nothing), then the
-// upper items; the backward launch runs the upper items first, then the
-// blocks, whose write-back of v and q^k is fused in.  Every element of W is
-// read once per sweep with coalesced 32-lane loads that stream past the
-// caches (__ldcs); vectors other CTAs update during the sweep are read
-// through L2 (ld.global.cg).  Completion counters are cumulative over solves:
-// supernode s has finished solve number e when its counter reaches
-// e * (its work items).  A wait that exceeds SweepSync::max_spins sets the
-// error flag and gives up instead of hanging.
+// One solve is five launches (factor.hpp, SweepPlan):
+//  1. k_block_forward — the lower levels of the elimination tree, cut into
+//     subtrees with contiguous columns ("blocks"), one CTA per block: the
+//     block's slice of b and its rows outside the block ("ext" rows, the row
+//     set of the block's root) sit in shared memory, the block's levels are
+//     separated by CTA barriers, each tile of each supernode is one warp's
+//     item, and the factor streams in through bulk asynchronous copies
+//     (cp.async.bulk, global -> shared, completion on an mbarrier) into a ring
+//     of stages per warp, kept several slabs ahead of the warp's arithmetic
+//     (across level barriers too: the factor does not depend on the data).
+//     The ext rows' updates are added to b with one atomic each per block.
+//  2. k_upper_forward — the supernodes above the blocks, split into 32-row
+//     tiles x column chunks, taken by warps from a queue in elimination-tree
+//     order; a warp waits (bounded spin) only until the supernode's upper
+//     children are complete (the blocks finished in launch 1).  Partial sums
+//     land in y / b_R with atomics.
+//  3. k_upper_backward — the same supernodes top-down in 32-column tiles x row
+//     chunks; an item waits until its parent is complete; sums land in x.
+//  4. k_block_backward — the blocks top-down: their y slice and the final x
+//     of their ext rows are loaded into shared memory, the factor and, per
+//     slab, the row-index list of the tile stream in as in launch 1, and x of
+//     the block's columns is written back into v and q^k directly.
+//  5. k_solve_post — the write-back of the upper supernodes' columns.
+// Completion counters are cumulative over solves: supernode s has finished
+// solve number e when its counter reaches e * (its work items).  Every wait
+// (counter or mbarrier) gives up after SweepSync::max_spins polls, sets the
+// error flag and returns instead of hanging.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,6 +44,14 @@ namespace pdfb {
 
 constexpr int kTicketBatch = 2;
 constexpr int kSweepThreads = 256;
+
+// Bulk-copy stages per warp: one slab (32 rows x kSlab columns, or kSlab rows
+// x 32 columns) each, 12 KB per warp in both precisions.
+template <typename T>
+struct Stages {
+  static constexpr int R = sizeof(T) == 8 ? 3 : 6;
+  static constexpr int kElems = kTile * kSlab;
+};
 
 __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long* p) {
   return *reinterpret_cast<const volatile unsigned long long*>(p);
@@ -71,6 +83,47 @@ __device__ __forceinline__ bool wait_counter(const unsigned long long* ctr, unsi
   return true;
 }
 
+// ---- mbarrier and bulk-copy primitives (PTX, sm_90+; no multicast)
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// orders this thread's (and, after __syncwarp, the warp's) generic-proxy
+// reads of a stage before the bulk copy that overwrites it
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// global -> shared bulk copy of `bytes` (multiple of 16, both addresses
+// 16-byte aligned), completing `bytes` transactions on `bar`
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int max_spins) {
+  for (int k = 0; k < max_spins; ++k)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+// every lane waits (each needs the barrier's acquire to see the copied data);
+// the outcome is made uniform across the warp
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* bar, uint32_t parity, int max_spins) {
+  return __all_sync(0xffffffffu, mbar_wait(bar, parity, max_spins)) != 0;
+}
+__device__ __forceinline__ uint32_t round16(uint32_t bytes) { return (bytes + 15u) & ~15u; }
+
 // Issues the (up to) 32 loads of one 32-wide slab of a tile: lane l reads
 // element (l, u) at p[stride u]; absent columns (u >= m) and lanes outside the
 // tile (act false) read as zero.
@@ -78,140 +131,6 @@ template <typename T>
 __device__ __forceinline__ void load_tile(T (&w)[32], const T* p, int m, int stride = kTile, bool act = true) {
 #pragma unroll
   for (int u = 0; u < 32; ++u) w[u] = (act && u < m) ? ldw(p + u * stride) : T(0);
-}
-
-// ---------------------------------------------------------------- blocks
-
-// Slab width of the block tiles: 16 columns (forward) / rows (backward), so
-// that a slab of W and the vector entries it multiplies fit the register
-// budget of two resident CTAs per SM (32-wide slabs took 206-220 registers).
-constexpr int kSlab = 16;
-
-template <typename T>
-__device__ __forceinline__ void load_slab(T (&w)[kSlab], const T* p, int m, int stride, bool act) {
-#pragma unroll
-  for (int u = 0; u < kSlab; ++u) w[u] = (act && u < m) ? ldw(p + u * stride) : T(0);
-}
-
-// Forward tile of a block: rows [32 tile, 32 tile + m) of W_s times the
-// block's slice sv of b; y_s rows are written (each by exactly one lane), the
-// R rows are subtracted from the slice (ancestors inside the block, shared
-// atomics) or from b (ancestors above the block, global atomics).
-template <typename T>
-__device__ __forceinline__ void block_fwd_item(const BlockItem& I, int c0b, int c1b, int nc, T* sv, const T* W,
-                                               T* b, T* y, const int* rows, int n, int lane) {
-  const int m = min(kTile, I.ns + I.nr - kTile * I.tile);
-  const int w = min(I.ns, kTile * I.tile + kTile);
-  const bool act = lane < m;
-  const T* wp = W + I.off + lane;
-  const T* vx = sv + I.c0l;
-  const T* vy = vx + nc;
-  const T* vz = vy + nc;
-  T ax = 0, ay = 0, az = 0;
-#pragma unroll 1
-  for (int j0 = 0; j0 < w; j0 += kSlab) {
-    const int cnt = min(kSlab, w - j0);
-    T wv[kSlab];
-    load_slab(wv, wp + (int64_t)j0 * m, cnt, m, act);
-    if (cnt == kSlab) {
-#pragma unroll
-      for (int u = 0; u < kSlab; ++u) {
-        ax += wv[u] * vx[j0 + u];
-        ay += wv[u] * vy[j0 + u];
-        az += wv[u] * vz[j0 + u];
-      }
-    } else {
-#pragma unroll
-      for (int u = 0; u < kSlab; ++u)
-        if (u < cnt) {
-          ax += wv[u] * vx[j0 + u];
-          ay += wv[u] * vy[j0 + u];
-          az += wv[u] * vz[j0 + u];
-        }
-    }
-  }
-  const int row = kTile * I.tile + lane;
-  if (row < I.ns) {
-    const int64_t o = (int64_t)c0b + I.c0l + row;
-    y[o] = ax;
-    y[o + n] = ay;
-    y[o + 2 * (int64_t)n] = az;
-  } else if (row < I.ns + I.nr) {
-    const int r = rows[I.roff + row - I.ns];
-    if (r < c1b) {
-      T* s = sv + (r - c0b);
-      atomicAdd(s, -ax);
-      atomicAdd(s + nc, -ay);
-      atomicAdd(s + 2 * nc, -az);
-    } else {
-      atomicAdd(b + r, -ax);
-      atomicAdd(b + r + n, -ay);
-      atomicAdd(b + r + 2 * (int64_t)n, -az);
-    }
-  }
-}
-
-// Backward tile of a block: columns [32 tile, 32 tile + mc) of W_s (lane =
-// column) over its rows: y_s from the forward sweep, then -x_R from the slice
-// sx (ancestors inside the block, already final) or from x (ancestors above
-// the block, final once the block's parent is).  The vector entries of a slab
-// are staged in the warp's shared buffer stage[3][kSlab] and read back as
-// broadcasts (fewer live registers than shuffled values).
-template <typename T>
-__device__ __forceinline__ void block_bwd_item(const BlockItem& I, int c0b, int c1b, int nc, T* sx, const T* W,
-                                               const T* y, const T* x, const int* rows, int n, int lane,
-                                               T* stage) {
-  const int j0t = kTile * I.tile, nd = I.ns - j0t, mc = min(kTile, nd), h = nd + I.nr;
-  const bool act = lane < mc;
-  const T* wp = W + I.off + lane;
-  T ax = 0, ay = 0, az = 0;
-#pragma unroll 1
-  for (int i0 = 0; i0 < h; i0 += kSlab) {
-    const int cnt = min(kSlab, h - i0);
-    T wv[kSlab];
-    load_slab(wv, wp + (int64_t)i0 * mc, cnt, mc, act);
-    const int il = i0 + lane;
-    T vx = 0, vy = 0, vz = 0;
-    if (lane < cnt) {
-      if (il < nd) {
-        const int64_t o = (int64_t)c0b + I.c0l + j0t + il;
-        vx = y[o];
-        vy = y[o + n];
-        vz = y[o + 2 * (int64_t)n];
-      } else {
-        const int r = rows[I.roff + il - nd];
-        if (r < c1b) {
-          const T* s = sx + (r - c0b);
-          vx = -s[0];
-          vy = -s[nc];
-          vz = -s[2 * nc];
-        } else {
-          vx = -ldcg(x + r);
-          vy = -ldcg(x + r + n);
-          vz = -ldcg(x + r + 2 * (int64_t)n);
-        }
-      }
-    }
-    __syncwarp();  // the previous slab's reads of stage are done
-    if (lane < kSlab) {
-      stage[lane] = vx;
-      stage[kSlab + lane] = vy;
-      stage[2 * kSlab + lane] = vz;
-    }
-    __syncwarp();
-#pragma unroll
-    for (int u = 0; u < kSlab; ++u) {
-      ax += wv[u] * stage[u];
-      ay += wv[u] * stage[kSlab + u];
-      az += wv[u] * stage[2 * kSlab + u];
-    }
-  }
-  if (act) {
-    T* s = sx + I.c0l + j0t + lane;
-    s[0] = ax;
-    s[nc] = ay;
-    s[2 * nc] = az;
-  }
 }
 
 // CTA-wide ticket: thread 0 draws, everyone reads it after the barrier.
@@ -222,48 +141,370 @@ __device__ __forceinline__ int cta_ticket(int* queue, int* slot) {
   return *slot;
 }
 
-// ---------------------------------------------------------------- sweeps
+// ---------------------------------------------------------------- blocks
+
+// Walks one warp's slabs of a block in the order the warp consumes them: the
+// items of level L taken round-robin by warp (item0 + lev[L] + warp, + nw,
+// ...), the slabs of an item in order.  Every lane holds the same cursor.
+struct SlabCursor {
+  int L, it, j0, len;  // len: the current item's columns (forward) / rows (backward)
+  __device__ __forceinline__ bool done(int nlev) const { return L >= nlev; }
+};
+
+template <bool kFwd>
+__device__ __forceinline__ int item_extent(const BlockItem& I) {
+  return kFwd ? min(I.ns, kTile * I.tile + kTile) : I.ns - kTile * I.tile + I.nr;
+}
+
+template <bool kFwd>
+__device__ __forceinline__ void cursor_settle(SlabCursor& c, const SweepBlock& B, const BlockItem* items, int warp,
+                                              int nw) {
+  while (c.L < B.nlev && c.it >= B.item0 + B.lev[c.L + 1]) {
+    ++c.L;
+    if (c.L < B.nlev) c.it = B.item0 + B.lev[c.L] + warp;
+  }
+  if (c.L < B.nlev) c.len = item_extent<kFwd>(items[c.it]);
+}
+
+template <bool kFwd>
+__device__ __forceinline__ void cursor_start(SlabCursor& c, const SweepBlock& B, const BlockItem* items, int warp,
+                                             int nw) {
+  c.L = 0;
+  c.it = B.item0 + B.lev[0] + warp;
+  c.j0 = 0;
+  cursor_settle<kFwd>(c, B, items, warp, nw);
+}
+
+template <bool kFwd>
+__device__ __forceinline__ void cursor_next(SlabCursor& c, const SweepBlock& B, const BlockItem* items, int warp,
+                                            int nw) {
+  c.j0 += kSlab;
+  if (c.j0 >= c.len) {
+    c.j0 = 0;
+    c.it += nw;
+    cursor_settle<kFwd>(c, B, items, warp, nw);
+  }
+}
+
+// lane 0: the bulk copy of the slab at cursor c into stage `st`
+template <typename T, bool kFwd>
+__device__ __forceinline__ void issue_slab(const SlabCursor& c, const BlockItem* items, const T* W, const int* bidx,
+                                           T* stage, int* istage, uint64_t* bar) {
+  const BlockItem I = items[c.it];
+  const int cnt = min(kSlab, c.len - c.j0);
+  // forward: rows of the tile m, the slab = columns j0.. (column-major, m per
+  // column); backward: columns of the tile mc, the slab = rows j0.. (mc per row)
+  const int width = kFwd ? min(kTile, I.ns + I.nr - kTile * I.tile) : min(kTile, I.ns - kTile * I.tile);
+  const uint32_t wbytes = round16((uint32_t)(width * cnt) * (uint32_t)sizeof(T));
+  const uint32_t ibytes = kFwd ? 0u : (uint32_t)(kSlab * sizeof(int));
+  mbar_expect_tx(bar, wbytes + ibytes);
+  bulk_g2s(stage, W + I.off + (int64_t)width * c.j0, wbytes, bar);
+  if (!kFwd) bulk_g2s(istage, bidx + I.idx0 + c.j0, ibytes, bar);
+}
+
+// Shared-memory layout of the block kernels (the same computation on the
+// host in configure_solve): rings | index rings (backward) | mbarriers |
+// vector (3 planes of nc + next) | y slice (backward, 3 planes of nc) |
+// per-warp staging of 3 x kSlab vector entries (backward).
+template <typename T>
+struct BlockSmem {
+  T* ring;
+  int* iring;
+  uint64_t* bar;
+  T* sv;
+  T* ys;
+  T* vstage;
+};
+
+template <typename T, bool kFwd>
+__device__ __forceinline__ BlockSmem<T> block_smem(unsigned char* base, int nw, int warp, int max_ld, int max_cols) {
+  constexpr int R = Stages<T>::R, KE = Stages<T>::kElems;
+  BlockSmem<T> s;
+  size_t off = 0;
+  s.ring = reinterpret_cast<T*>(base) + (size_t)warp * R * KE;
+  off += (size_t)nw * R * KE * sizeof(T);
+  s.iring = reinterpret_cast<int*>(base + off) + (size_t)warp * R * kSlab;
+  if (!kFwd) off += (size_t)nw * R * kSlab * sizeof(int);
+  s.bar = reinterpret_cast<uint64_t*>(base + off) + warp * R;
+  off += (size_t)nw * R * sizeof(uint64_t);
+  s.sv = reinterpret_cast<T*>(base + off);
+  off += 3 * (size_t)max_ld * sizeof(T);
+  s.ys = reinterpret_cast<T*>(base + off);
+  if (!kFwd) off += 3 * (size_t)max_cols * sizeof(T);
+  s.vstage = reinterpret_cast<T*>(base + off) + (size_t)warp * 3 * kSlab;
+  return s;
+}
+
+template <typename T, bool kFwd>
+size_t block_smem_bytes(int nw, int max_ld, int max_cols) {
+  constexpr int R = Stages<T>::R, KE = Stages<T>::kElems;
+  size_t b = (size_t)nw * R * KE * sizeof(T) + (size_t)nw * R * sizeof(uint64_t) + 3 * (size_t)max_ld * sizeof(T);
+  if (!kFwd) b += (size_t)nw * R * kSlab * sizeof(int) + 3 * (size_t)max_cols * sizeof(T) + (size_t)nw * 3 * kSlab * sizeof(T);
+  return b;
+}
+
+// After an mbarrier wait gave up: wait (bounded) for every copy this warp
+// still has in flight, so that none lands after the CTA exits.
+__device__ __forceinline__ void drain_stages(uint64_t* bar, uint32_t pending, uint32_t par, int R, int max_spins) {
+  for (int k = 0; k < R; ++k)
+    if (pending & (1u << k)) mbar_wait(bar + k, (par >> k) & 1u, max_spins);
+}
 
 template <typename T>
-__global__ void __launch_bounds__(kSweepThreads) k_sweep_forward(DPlan P, const T* __restrict__ W, T* b, T* y, int n,
-                                                                 SweepSync sy) {
+__global__ void __launch_bounds__(kSweepThreads, 1) k_block_forward(DPlan P, const T* __restrict__ W, T* b, T* y,
+                                                                    int n, SweepSync sy) {
   trace_stamp(sy.trace, DTrace::kSolve);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int R = Stages<T>::R, KE = Stages<T>::kElems;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int s_ticket;
-  T* sv = reinterpret_cast<T*>(smem_raw);
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const unsigned long long ep = ld_volatile_u64(sy.epoch);
-  // ---- subtree blocks
+  const BlockSmem<T> sm = block_smem<T, true>(smem_raw, nw, warp, P.max_cols + P.max_ext, P.max_cols);
+  if (lane == 0)
+    for (int k = 0; k < R; ++k) mbar_init(sm.bar + k, 1);
+  fence_mbar_init();
+  __syncwarp();
+  uint32_t par = 0, pending = 0;  // per stage: wait parity, fill in flight
+  int prod = 0, cons = 0;         // slabs issued / consumed by this warp
+  bool failed = false;
   for (;;) {
     const int bi = cta_ticket(sy.queue + 2, &s_ticket);
     if (bi >= P.nblk) break;
     const SweepBlock& B = P.fblk[bi];
-    const int c0b = B.c0, c1b = B.c1, nc = c1b - c0b, item0 = B.item0, nlev = B.nlev;
+    const int c0b = B.c0, nc = B.c1 - B.c0, ld = nc + B.next;
+    T* sv = sm.sv;
     for (int k = threadIdx.x; k < nc; k += blockDim.x) {
       sv[k] = b[c0b + k];
-      sv[nc + k] = b[(int64_t)n + c0b + k];
-      sv[2 * nc + k] = b[2 * (int64_t)n + c0b + k];
+      sv[ld + k] = b[(int64_t)n + c0b + k];
+      sv[2 * ld + k] = b[2 * (int64_t)n + c0b + k];
+    }
+    for (int e = threadIdx.x; e < B.next; e += blockDim.x) sv[nc + e] = sv[ld + nc + e] = sv[2 * ld + nc + e] = T(0);
+    SlabCursor pc;
+    cursor_start<true>(pc, B, P.fitem, warp, nw);
+    for (int k = 0; k < R && !pc.done(B.nlev) && !failed; ++k) {
+      const int st = prod % R;
+      if (lane == 0) issue_slab<T, true>(pc, P.fitem, W, P.bidx, sm.ring + st * KE, nullptr, sm.bar + st);
+      pending |= 1u << st;
+      ++prod;
+      cursor_next<true>(pc, B, P.fitem, warp, nw);
     }
     __syncthreads();
-    for (int L = 0; L < nlev; ++L) {
-      const int i1 = item0 + B.lev[L + 1];
+    for (int L = 0; L < B.nlev; ++L) {
+      const int i1 = B.item0 + B.lev[L + 1];
 #pragma unroll 1
-      for (int it = item0 + B.lev[L] + warp; it < i1; it += nw)
-        block_fwd_item<T>(P.fitem[it], c0b, c1b, nc, sv, W, b, y, P.rows, n, lane);
+      for (int it = B.item0 + B.lev[L] + warp; it < i1; it += nw) {
+        const BlockItem I = P.fitem[it];
+        const int m = min(kTile, I.ns + I.nr - kTile * I.tile);
+        const int w = min(I.ns, kTile * I.tile + kTile);
+        const int row = kTile * I.tile + lane;
+        const int loc = (row >= I.ns && row < I.ns + I.nr) ? P.rows_loc[I.roff + row - I.ns] : -1;
+        const T* vx = sv + I.c0l;
+        T ax = 0, ay = 0, az = 0;
+#pragma unroll 1
+        for (int j0 = 0; j0 < w; j0 += kSlab) {
+          const int st = cons % R;
+          if (!failed && !mbar_wait_warp(sm.bar + st, (par >> st) & 1u, sy.max_spins)) {
+            failed = true;
+            if (lane == 0) atomicOr(sy.err, 1);
+          }
+          if (!(pending & (1u << st)) || failed) {
+            // nothing valid in this stage
+          } else {
+            const T* sp = sm.ring + st * KE;
+            const int cnt = min(kSlab, w - j0);
+            if (lane < m) {
+#pragma unroll
+              for (int u = 0; u < kSlab; ++u)
+                if (u < cnt) {
+                  const T wv = sp[m * u + lane];
+                  ax += wv * vx[j0 + u];
+                  ay += wv * vx[ld + j0 + u];
+                  az += wv * vx[2 * ld + j0 + u];
+                }
+            }
+          }
+          if (!failed) {
+            par ^= 1u << st;
+            pending &= ~(1u << st);
+          }
+          __syncwarp();
+          ++cons;
+          if (!pc.done(B.nlev) && !failed) {
+            if (lane == 0) {
+              fence_proxy_async();
+              issue_slab<T, true>(pc, P.fitem, W, P.bidx, sm.ring + st * KE, nullptr, sm.bar + st);
+            }
+            pending |= 1u << st;
+            ++prod;
+            cursor_next<true>(pc, B, P.fitem, warp, nw);
+          }
+        }
+        if (row < I.ns) {
+          const int64_t o = (int64_t)c0b + I.c0l + row;
+          y[o] = ax;
+          y[o + n] = ay;
+          y[o + 2 * (int64_t)n] = az;
+        } else if (loc >= 0) {
+          atomicAdd(sv + loc, -ax);
+          atomicAdd(sv + ld + loc, -ay);
+          atomicAdd(sv + 2 * ld + loc, -az);
+        }
+      }
       __syncthreads();
     }
-    if (B.parent >= 0) {
-      // the block's global updates of its ancestors' rows happen before the
-      // parent sees the block complete
-      __threadfence();
-      __syncthreads();
-      if (threadIdx.x == 0) atomicAdd(sy.fchild + B.parent, 1ULL);
+    // the ext rows' updates, once per block
+    for (int e = threadIdx.x; e < B.next; e += blockDim.x) {
+      const int64_t r = P.rows[B.ext0 + e];
+      atomicAdd(b + r, sv[nc + e]);
+      atomicAdd(b + r + n, sv[ld + nc + e]);
+      atomicAdd(b + r + 2 * (int64_t)n, sv[2 * ld + nc + e]);
     }
   }
-  // ---- upper work items.  Tickets are taken kTicketBatch at a time and
-  // processed in order, the next batch drawn while the current one runs:
-  // every item with a smaller ticket is held by a running warp (and every
-  // block by a running CTA), so the waits below always end.
+  if (failed) drain_stages(sm.bar, pending, par, R, sy.max_spins);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSweepThreads, 1) k_block_backward(DPlan P, const T* __restrict__ W,
+                                                                     const T* __restrict__ y, const T* x, int n,
+                                                                     SweepSync sy, WriteBack wb) {
+  constexpr int R = Stages<T>::R, KE = Stages<T>::kElems;
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  __shared__ int s_ticket;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const BlockSmem<T> sm = block_smem<T, false>(smem_raw, nw, warp, P.max_cols + P.max_ext, P.max_cols);
+  if (lane == 0)
+    for (int k = 0; k < R; ++k) mbar_init(sm.bar + k, 1);
+  fence_mbar_init();
+  __syncwarp();
+  uint32_t par = 0, pending = 0;
+  int prod = 0, cons = 0;
+  bool failed = false;
+  for (;;) {
+    const int bi = cta_ticket(sy.queue + 3, &s_ticket);
+    if (bi >= P.nblk) break;
+    const SweepBlock& B = P.bblk[bi];
+    const int c0b = B.c0, nc = B.c1 - B.c0, ld = nc + B.next;
+    T* sv = sm.sv;
+    T* ys = sm.ys;
+    // the y slice, and the final x of the ext rows (the upper supernodes
+    // finished in the previous launch)
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+      ys[k] = y[c0b + k];
+      ys[nc + k] = y[(int64_t)n + c0b + k];
+      ys[2 * nc + k] = y[2 * (int64_t)n + c0b + k];
+    }
+    for (int e = threadIdx.x; e < B.next; e += blockDim.x) {
+      const int64_t r = P.rows[B.ext0 + e];
+      sv[nc + e] = x[r];
+      sv[ld + nc + e] = x[r + n];
+      sv[2 * ld + nc + e] = x[r + 2 * (int64_t)n];
+    }
+    SlabCursor pc;
+    cursor_start<false>(pc, B, P.bitem, warp, nw);
+    for (int k = 0; k < R && !pc.done(B.nlev) && !failed; ++k) {
+      const int st = prod % R;
+      if (lane == 0)
+        issue_slab<T, false>(pc, P.bitem, W, P.bidx, sm.ring + st * KE, sm.iring + st * kSlab, sm.bar + st);
+      pending |= 1u << st;
+      ++prod;
+      cursor_next<false>(pc, B, P.bitem, warp, nw);
+    }
+    __syncthreads();
+    for (int L = 0; L < B.nlev; ++L) {
+      const int i1 = B.item0 + B.lev[L + 1];
+#pragma unroll 1
+      for (int it = B.item0 + B.lev[L] + warp; it < i1; it += nw) {
+        const BlockItem I = P.bitem[it];
+        const int j0t = kTile * I.tile, nd = I.ns - j0t, mc = min(kTile, nd), h = nd + I.nr;
+        T ax = 0, ay = 0, az = 0;
+#pragma unroll 1
+        for (int i0 = 0; i0 < h; i0 += kSlab) {
+          const int st = cons % R;
+          if (!failed && !mbar_wait_warp(sm.bar + st, (par >> st) & 1u, sy.max_spins)) {
+            failed = true;
+            if (lane == 0) atomicOr(sy.err, 1);
+          }
+          const int cnt = min(kSlab, h - i0);
+          const bool valid = (pending & (1u << st)) && !failed;
+          if (lane < kSlab) {
+            T vx = 0, vy = 0, vz = 0;
+            if (valid && lane < cnt) {
+              const int idx = sm.iring[st * kSlab + lane];
+              if (idx < 0) {
+                const int k = -1 - idx;
+                vx = ys[k];
+                vy = ys[nc + k];
+                vz = ys[2 * nc + k];
+              } else {
+                vx = -sv[idx];
+                vy = -sv[ld + idx];
+                vz = -sv[2 * ld + idx];
+              }
+            }
+            sm.vstage[lane] = vx;
+            sm.vstage[kSlab + lane] = vy;
+            sm.vstage[2 * kSlab + lane] = vz;
+          }
+          __syncwarp();
+          if (valid && lane < mc) {
+            const T* sp = sm.ring + st * KE;
+#pragma unroll
+            for (int u = 0; u < kSlab; ++u)
+              if (u < cnt) {
+                const T wv = sp[mc * u + lane];
+                ax += wv * sm.vstage[u];
+                ay += wv * sm.vstage[kSlab + u];
+                az += wv * sm.vstage[2 * kSlab + u];
+              }
+          }
+          if (!failed) {
+            par ^= 1u << st;
+            pending &= ~(1u << st);
+          }
+          __syncwarp();
+          ++cons;
+          if (!pc.done(B.nlev) && !failed) {
+            if (lane == 0) {
+              fence_proxy_async();
+              issue_slab<T, false>(pc, P.bitem, W, P.bidx, sm.ring + st * KE, sm.iring + st * kSlab, sm.bar + st);
+            }
+            pending |= 1u << st;
+            ++prod;
+            cursor_next<false>(pc, B, P.bitem, warp, nw);
+          }
+        }
+        if (lane < mc) {
+          T* s = sv + I.c0l + j0t + lane;
+          s[0] = ax;
+          s[ld] = ay;
+          s[2 * ld] = az;
+        }
+      }
+      __syncthreads();
+    }
+    if (!failed)
+      for (int k = threadIdx.x; k < nc; k += blockDim.x) {
+        const int64_t vtx = P.perm[c0b + k];
+        for (int c = 0; c < 3; ++c) {
+          double val = (double)sv[k + c * ld];
+          if (wb.mode == 1) val += wb.v[3 * vtx + c];
+          wb.v[3 * vtx + c] = val;
+          wb.qk[3 * vtx + c] = wb.q[3 * vtx + c] + wb.dt * val;
+        }
+      }
+  }
+  if (failed) drain_stages(sm.bar, pending, par, R, sy.max_spins);
+}
+
+// ---------------------------------------------------------- upper items
+
+// Tickets are taken kTicketBatch at a time and processed in order, the next
+// batch drawn while the current one runs: every item with a smaller ticket is
+// held by a running warp, so the waits below always end.
+template <typename T>
+__global__ void __launch_bounds__(kSweepThreads) k_upper_forward(DPlan P, const T* __restrict__ W, T* b, T* y, int n,
+                                                                 SweepSync sy) {
+  const int lane = threadIdx.x & 31;
+  const unsigned long long ep = ld_volatile_u64(sy.epoch);
   int t = 0, tend = 0, next = 0;
   if (lane == 0) next = atomicAdd(sy.queue + 0, kTicketBatch);
   for (;; ++t) {
@@ -332,26 +573,20 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_forward(DPlan P, const 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kSweepThreads) k_sweep_backward(DPlan P, const T* __restrict__ W,
-                                                                  const T* __restrict__ y, T* x, int n,
-                                                                  SweepSync sy, WriteBack wb) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  __shared__ int s_ticket, s_ok;
-  __shared__ T s_stage[kSweepThreads / 32][3 * kSlab];
-  T* sx = reinterpret_cast<T*>(smem_raw);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+__global__ void __launch_bounds__(kSweepThreads) k_upper_backward(DPlan P, const T* __restrict__ W,
+                                                                  const T* __restrict__ y, T* x, int n, SweepSync sy) {
+  const int lane = threadIdx.x & 31;
   const unsigned long long ep = ld_volatile_u64(sy.epoch);
-  // ---- upper work items (top-down); tickets as in the forward sweep
   int t = 0, tend = 0, next = 0;
   if (lane == 0) next = atomicAdd(sy.queue + 1, kTicketBatch);
   for (;; ++t) {
     if (t >= tend) {
       t = __shfl_sync(0xffffffffu, next, 0);
       tend = t + kTicketBatch;
-      if (t >= P.nbup) break;
+      if (t >= P.nbup) return;
       if (lane == 0) next = atomicAdd(sy.queue + 1, kTicketBatch);
     }
-    if (t >= P.nbup) break;
+    if (t >= P.nbup) return;
     const UpperItem tk = P.bup[t];
     const int mcols = min(kTile, tk.ns - tk.tile * kTile);
     const T* wbase = W + tk.off + lane;
@@ -401,34 +636,6 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_backward(DPlan P, const
     __syncwarp();
     if (lane == 0) atomicAdd(sy.bdone + tk.sn, 1ULL);
   }
-  // ---- subtree blocks (top-down inside each), write-back of v and q^k
-  for (;;) {
-    const int bi = cta_ticket(sy.queue + 3, &s_ticket);
-    if (bi >= P.nblk) break;
-    const SweepBlock& B = P.bblk[bi];
-    const int c0b = B.c0, c1b = B.c1, nc = c1b - c0b, item0 = B.item0, nlev = B.nlev;
-    if (threadIdx.x == 0)
-      s_ok = B.parent < 0 ||
-             wait_counter(sy.bdone + B.parent, ep * (unsigned long long)P.sn[B.parent].ntb, sy.err, sy.max_spins);
-    __syncthreads();
-    if (!s_ok) continue;  // uniform: the error flag is set, the state is left as it was
-    for (int L = 0; L < nlev; ++L) {
-      const int i1 = item0 + B.lev[L + 1];
-#pragma unroll 1
-      for (int it = item0 + B.lev[L] + warp; it < i1; it += nw)
-        block_bwd_item<T>(P.bitem[it], c0b, c1b, nc, sx, W, y, x, P.rows, n, lane, s_stage[warp]);
-      __syncthreads();
-    }
-    for (int k = threadIdx.x; k < nc; k += blockDim.x) {
-      const int64_t vtx = P.perm[c0b + k];
-      for (int c = 0; c < 3; ++c) {
-        double val = (double)sx[k + c * nc];
-        if (wb.mode == 1) val += wb.v[3 * vtx + c];
-        wb.v[3 * vtx + c] = val;
-        wb.qk[3 * vtx + c] = wb.q[3 * vtx + c] + wb.dt * val;
-      }
-    }
-  }
 }
 
 // After the backward sweep, for the upper supernodes' columns: v[perm] = x
@@ -466,30 +673,42 @@ __global__ void k_solve_prep(int n, T* x, T* y, SweepSync sy) {
 }
 
 // Persistent grid: as many CTAs as can be resident at once with this dynamic
-// shared memory.
+// shared memory (0 when the kernel does not fit).
 template <typename K>
 int resident_ctas(K kernel, size_t smem) {
-  int dev = 0, sms = 148, per_sm = 1;
+  int dev = 0, sms = 148, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kSweepThreads, smem);
-  return std::max(1, per_sm) * sms;
+  return per_sm * sms;
 }
 
 template <typename T>
-void configure_solve(DPlan& P) {
-  const size_t smem = 3 * (size_t)std::max(1, P.max_cols) * sizeof(T);
-  P.smem = (int)smem;
-  P.grid_f = resident_ctas(k_sweep_forward<T>, smem);
-  P.grid_b = resident_ctas(k_sweep_backward<T>, smem);
+bool configure_solve(DPlan& P) {
+  const int nw = kSweepThreads / 32;
+  const int max_ld = std::max(1, P.max_cols + P.max_ext);
+  P.smem_f = (int)block_smem_bytes<T, true>(nw, max_ld, std::max(1, P.max_cols));
+  P.smem_b = (int)block_smem_bytes<T, false>(nw, max_ld, std::max(1, P.max_cols));
+  const int rf = resident_ctas(k_block_forward<T>, P.smem_f);
+  const int rb = resident_ctas(k_block_backward<T>, P.smem_b);
+  P.grid_bf = std::max(1, std::min(rf, std::max(1, P.nblk)));
+  P.grid_bb = std::max(1, std::min(rb, std::max(1, P.nblk)));
+  P.grid_uf = std::max(1, resident_ctas(k_upper_forward<T>, 0));
+  P.grid_ub = std::max(1, resident_ctas(k_upper_backward<T>, 0));
+  return rf > 0 && rb > 0;
 }
 
 template <typename T>
 void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
                          SweepSync sy, WriteBack wb) {
-  k_sweep_forward<T><<<P.grid_f, kSweepThreads, P.smem, st>>>(P, Wf, b, y, n, sy);
-  k_sweep_backward<T><<<P.grid_b, kSweepThreads, P.smem, st>>>(P, Wb, y, x, n, sy, wb);
+  k_block_forward<T><<<P.grid_bf, kSweepThreads, P.smem_f, st>>>(P, Wf, b, y, n, sy);
+  k_upper_forward<T><<<P.grid_uf, kSweepThreads, 0, st>>>(P, Wf, b, y, n, sy);
+  k_upper_backward<T><<<P.grid_ub, kSweepThreads, 0, st>>>(P, Wb, y, x, n, sy);
+  k_block_backward<T><<<P.grid_bb, kSweepThreads, P.smem_b, st>>>(P, Wb, y, x, n, sy, wb);
   k_solve_post<T><<<std::max(1, std::min(148 * 4, (P.n_upper + 255) / 256)), 256, 0, st>>>(P, x, y, n, wb, sy);
 }
 template <typename T>
@@ -497,8 +716,8 @@ void launch_solve_prep(cudaStream_t st, int n, T* x, T* y, SweepSync sy) {
   k_solve_prep<T><<<std::min(148 * 4, (3 * n + 255) / 256), 256, 0, st>>>(n, x, y, sy);
 }
 
-template void configure_solve<double>(DPlan&);
-template void configure_solve<float>(DPlan&);
+template bool configure_solve<double>(DPlan&);
+template bool configure_solve<float>(DPlan&);
 template void launch_solve_sweeps<double>(cudaStream_t, const DPlan&, const double*, const double*, double*, double*,
                                           double*, int, SweepSync, WriteBack);
 template void launch_solve_sweeps<float>(cudaStream_t, const DPlan&, const float*, const float*, float*, float*,

@@ -9,7 +9,7 @@ from climatenet_b200 import abi, native, scenes
 from oracle.oracle import Oracle
 
 
-@pytest.mark.parametrize("n,layers", [(12, 1), (30, 1), (40, 3), (90, 1)])
+@pytest.mark.parametrize("n,layers", [(12, 1), (30, 1), (40, 3), (90, 1), (160, 1)])
 def test_tiled_solve_matches_oracle(n, layers):
     s = scenes.cloth_on_sphere(n=n, layers=layers, pins=(layers == 1))
     p = abi.params(time_step=2e-3, iterations=5)
