@@ -518,11 +518,19 @@ def main():
             if not verdict["use"]:
                 weights = None
             arms.append(("learned", "fp32", weights))
+        q_fp64 = None
         for name, precision, w in arms:
             sim = make_sim(s, pk, cap, precision, w, device=local, tolerance=tol)
             rec, ms, launches, clk, _, q_end = run_arm(sim, K, args.warmup, start, barrier, dist, units, local)
+            # end-of-stretch positions against the reference's method (20
+            # iterations: a different stopping point) and, for the FP32 arms,
+            # against the FP64 arm at the same residual
             rec.update(tolerance=tol, iteration_cap=cap,
                        position_error_vs_fixed20=rel_position_error(q_end, q_ref))
+            if name == "fp64_plain":
+                q_fp64 = q_end
+            else:
+                rec["position_error_vs_fp64_same_residual"] = rel_position_error(q_end, q_fp64)
             line_extra[name] = rec
             res = rec["mean_residual"]
             if name != arms[-1][0]:
