@@ -237,6 +237,8 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   d.bend_w = upload(m.bend_w);
   d.bend_rest = upload(m.bend_rest);
   d.pin_term = m.has_pins ? upload(m.pin_term) : nullptr;
+  d.spring_k = upload(m.spring_k);
+  d.pin_w = m.has_pins ? upload(m.pin_w) : nullptr;
   d.ata_ptr = upload(m.ata_ptr);
   d.ata_col = upload(m.ata_col);
   d.ata_val = upload(m.ata_val);
@@ -263,6 +265,8 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   dm.bend_w = d.bend_w;
   dm.bend_rest = d.bend_rest;
   dm.pin_term = d.pin_term;
+  dm.spring_k = d.spring_k;
+  dm.pin_w = d.pin_w;
   dm.ata_ptr = d.ata_ptr;
   dm.ata_col = d.ata_col;
   dm.ata_val = d.ata_val;
@@ -356,6 +360,7 @@ void create_impl(pdf_handle* h, const pdf_scene_desc* sc, const pdf_params* p) {
   d.q = upload(m.q0);
   d.v = upload(m.v0);
   d.tn = dalloc<double>(3 * (size_t)N);
+  h->dm.tn = d.tn;
   d.qk = upload(m.q0);
   d.cstep = dalloc<double>(3 * (size_t)N);
   d.bp = dalloc<double>(3 * (size_t)std::max(1, dm.B));
@@ -516,7 +521,7 @@ void launch_local(pdf_handle* h, T* b, int mode) {
   DeviceBuffers& d = h->d;
   const DModel& dm = h->dm;
   cudaStream_t st = h->stream;
-  if (dm.B > 0) k_bend_proj<<<blocks_for(dm.B), kThreads, 0, st>>>(dm, d.qk, d.bp);
+  if (dm.B > 0) k_bend_proj<<<blocks_for(dm.B), kThreads, 0, st>>>(dm, d.qk, d.bp, mode);
   launch_vertex_rhs<T>(blocks_for(dm.N), kThreads, st, dm, d.qk, d.v, d.cstep, d.bp,
                        std::max(h->prm.air_damping, 0.), d.c.slot_of, d.c.f, b, h->prm.time_step, mode);
 }
@@ -951,7 +956,7 @@ void free_handle(pdf_handle* h) {
   if (h->graph) cudaGraphExecDestroy(h->graph);
   self_detect_free(h);
   DeviceBuffers& d = h->d;
-  void* ptrs[] = {d.mass, d.ring_kappa, d.ring_bend, d.self_bend, d.ring_ptr, d.ring_idx, d.bend_of, d.bend_ptr,
+  void* ptrs[] = {d.spring_k, d.pin_w, d.mass, d.ring_kappa, d.ring_bend, d.self_bend, d.ring_ptr, d.ring_idx, d.bend_of, d.bend_ptr,
                   d.bend_idx, d.bend_coef, d.bend_w, d.bend_rest, d.pin_term, d.ata_ptr, d.ata_col, d.ata_val,
                   d.perm, d.iperm, d.vmat, d.friction, d.tris, d.obstacles, d.vmesh, d.q, d.v, d.tn, d.qk,
                   d.cstep, d.bp, d.sn, d.rows, d.Wf64, d.Wb64, d.Wf32, d.Wb32, d.sync.queue, d.sync.epoch,

@@ -49,6 +49,9 @@ struct DModel {
   const double* bend_w;     // B
   const double* bend_rest;  // B
   const double* pin_term;   // 3N or null
+  const double* spring_k;   // N: stiffness of the vertex's springs
+  const double* pin_w;      // N or null: summed pin weight of the vertex
+  const double* tn;         // 3N: predictor t_n of the current step
   const int* ata_ptr;       // N+1, A^T A in CSR
   const int* ata_col;
   const double* ata_val;

@@ -19,6 +19,7 @@ struct DeviceBuffers {
   double *mass = nullptr, *ring_kappa = nullptr, *ring_bend = nullptr, *self_bend = nullptr;
   int *ring_ptr = nullptr, *ring_idx = nullptr, *bend_of = nullptr, *bend_ptr = nullptr, *bend_idx = nullptr;
   double *bend_coef = nullptr, *bend_w = nullptr, *bend_rest = nullptr, *pin_term = nullptr;
+  double *spring_k = nullptr, *pin_w = nullptr;
   int *ata_ptr = nullptr, *ata_col = nullptr;
   double* ata_val = nullptr;
   int *perm = nullptr, *iperm = nullptr, *vmat = nullptr;

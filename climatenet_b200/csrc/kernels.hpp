@@ -92,7 +92,8 @@ void mesh_bvh_free(MeshBVH* b);
 
 __global__ void k_step_init(DModel m, const double* q, double* v, double* tn, double* qk, double* cstep, double gx,
                             double gy, double gz, double dt);
-__global__ void k_bend_proj(DModel m, const double* qk, double* bp);
+// residual_mode 1: writes p_b - A_b q (the bending force's row value)
+__global__ void k_bend_proj(DModel m, const double* qk, double* bp, int residual_mode);
 // Iteration control of one step, on the device.  iter = PD iterations
 // completed in this step (kernels of iteration k read k from it); the last
 // block of the Alart-Curnier kernel closes the iteration: it advances iter and

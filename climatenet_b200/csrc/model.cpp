@@ -88,6 +88,8 @@ void build_model(const pdf_scene_desc& sc, const pdf_params& p, Model& m) {
   m.bend_of.assign(N, -1);
   m.self_bend.assign(N, 0.);
   m.pin_term.assign(3 * (size_t)N, 0.);
+  m.spring_k.assign(N, 0.);
+  m.pin_w.assign(N, 0.);
 
   // A rows: (vertex, value) lists, in the reference's row order: per mesh the
   // springs (edge creation order) then the bending rows (vertex order), then
@@ -152,6 +154,7 @@ void build_model(const pdf_scene_desc& sc, const pdf_params& p, Model& m) {
     for (int v = v0; v < v1; ++v) m.mass[v] /= 3;
     // springs, one per undirected edge in order of first appearance
     const double sk = std::sqrt(md.stretching);
+    for (int v = v0; v < v1; ++v) m.spring_k[v] = sk * sk;
     for (int h = 0; h < nh; ++h) {
       int o = he.opp[h];
       if (o >= 0 && o < h) continue;  // edge already created by its opposite
@@ -229,6 +232,7 @@ void build_model(const pdf_scene_desc& sc, const pdf_params& p, Model& m) {
     double sw = std::sqrt(w);
     push_row({{v, sw}});
     for (int c = 0; c < 3; ++c) m.pin_term[3 * (size_t)v + c] += sw * (sw * sc.pin_positions[3 * (size_t)k + c]);
+    m.pin_w[v] += sw * sw;
     m.has_pins = true;
   }
   m.n_rows = (int)row_ptr.size() - 1;

@@ -45,6 +45,10 @@ struct Model {
   std::vector<double> bend_coef, bend_w, bend_rest;
   // attachment term sum_pins sqrt(w) * (sqrt(w) x0) per vertex (3N), constant
   std::vector<double> pin_term;
+  // per vertex: the stiffness of its springs (the weight sqrt(k) squared, the
+  // same for every spring of a mesh) and the summed weight of its pins; with
+  // them the local step forms the residual in force form (FP32 mode)
+  std::vector<double> spring_k, pin_w;
   bool has_pins = false;
 
   // A^T A in CSR (full symmetric), sorted columns

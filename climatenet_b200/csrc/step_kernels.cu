@@ -48,19 +48,22 @@ __global__ void k_step_init(DModel m, const double* __restrict__ q, double* __re
 // Bending projections (BendingConstraint::addConstraintProjection,
 // BendingConstraint.cpp:106-138): p_b = sqrt(b) * (rest/|L x|) L x, or 0 when
 // |L x| <= 1e-25, with L x the mean-value Laplacian at the current iterate.
-__global__ void k_bend_proj(DModel m, const double* __restrict__ qk, double* __restrict__ bp) {
+// Residual mode (FP32 solves) writes p_b - A_b x instead (A_b x = sqrt(b) L x),
+// the row's part of the bending force A_b^T (p_b - A_b x).
+__global__ void k_bend_proj(DModel m, const double* __restrict__ qk, double* __restrict__ bp, int residual_mode) {
   trace_stamp(m.trace, DTrace::kLocal);
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= m.B) return;
   double3 lb = make_double3(0., 0., 0.);
   for (int k = m.bend_ptr[b]; k < m.bend_ptr[b + 1]; ++k) lb = lb + m.bend_coef[k] * ld3(qk, m.bend_idx[k]);
   const double n = sqrt(dot3(lb, lb));
+  const double w = m.bend_w[b];
   double3 p = make_double3(0., 0., 0.);
   if (n > 1e-25) {
     const double s = m.bend_rest[b] / n;
-    lb = make_double3(lb.x * s, lb.y * s, lb.z * s);
-    p = m.bend_w[b] * lb;
+    p = w * make_double3(lb.x * s, lb.y * s, lb.z * s);
   }
+  if (residual_mode) p = p - w * lb;
   st3(bp, b, p);
 }
 
@@ -73,7 +76,12 @@ __global__ void k_bend_proj(DModel m, const double* __restrict__ qk, double* __r
 // Vertex i gathers from its 1-ring, so no atomics are needed.  Output goes
 // straight to the solve's pivot order.  At contact vertices (slot >= 0) the
 // force estimate f = rhs - dt^2 (A^T A v)_i of SFE:337-347 is written too.
-// Residual mode (FP32 solves) writes r = rhs - (M + dt^2 A^T A) v instead.
+// Residual mode (FP32 solves) writes r = rhs - (M + dt^2 A^T A) v instead, in
+// its force form r = M (t_n - v) + dt (A^T p - A^T A q^k) - dt D v with
+// q^k = q_n + dt v: per spring k (L e - (q_i - q_j)), per bending row
+// A[b,i] (p_b - A_b q^k) (k_bend_proj's residual mode), per pin
+// w (x0 - q_i) — the same quantity without the A^T A product, each term a
+// small force instead of a difference of large ones; f = r + M v.
 template <typename T>
 __global__ void k_vertex_rhs(DModel m, const double* __restrict__ qk, const double* __restrict__ v,
                              const double* __restrict__ cstep, const double* __restrict__ bp,
@@ -86,10 +94,12 @@ __global__ void k_vertex_rhs(DModel m, const double* __restrict__ qk, const doub
   double3 acc = make_double3(0., 0., 0.);
   const int bo = m.bend_of[i];
   if (bo >= 0) acc = acc + m.self_bend[i] * ld3(bp, bo);
+  const double ks = residual_mode ? m.spring_k[i] : 0.;
   for (int s = m.ring_ptr[i]; s < m.ring_ptr[i + 1]; ++s) {
     const int j = m.ring_idx[s];
-    const double3 e = normalized3(qi - ld3(qk, j));
-    acc = acc + m.ring_kappa[s] * e;
+    const double3 d = qi - ld3(qk, j);
+    acc = acc + m.ring_kappa[s] * normalized3(d);
+    if (residual_mode) acc = acc - ks * d;
     const int bj = m.bend_of[j];
     if (bj >= 0) acc = acc + m.ring_bend[s] * ld3(bp, bj);
   }
@@ -97,25 +107,34 @@ __global__ void k_vertex_rhs(DModel m, const double* __restrict__ qk, const doub
   const int slot = slot_of[i];
   // air damping is switched off at every contact vertex (SimulationBase.cpp:347-396)
   const double di = slot >= 0 ? 0. : air_damping;
-  const double3 c = ld3(cstep, i);
-  const double3 rhs = make_double3(c.x + dt * (acc.x - di * vi.x), c.y + dt * (acc.y - di * vi.y),
-                                   c.z + dt * (acc.z - di * vi.z));
-  double3 out = rhs;
-  if (residual_mode || slot >= 0) {
-    double ax = 0, ay = 0, az = 0;
-    for (int k = m.ata_ptr[i]; k < m.ata_ptr[i + 1]; ++k) {
-      const double a = m.ata_val[k];
-      const int j = m.ata_col[k];
-      ax += a * v[3 * (int64_t)j];
-      ay += a * v[3 * (int64_t)j + 1];
-      az += a * v[3 * (int64_t)j + 2];
+  double3 out;
+  if (residual_mode) {
+    if (m.pin_term) {
+      const double pw = m.pin_w[i];
+      const double3 pt = ld3(m.pin_term, i);
+      acc = acc + make_double3(pt.x - pw * qi.x, pt.y - pw * qi.y, pt.z - pw * qi.z);
     }
-    const double dt2 = dt * dt;
-    const double3 f = make_double3(rhs.x - dt2 * ax, rhs.y - dt2 * ay, rhs.z - dt2 * az);
-    if (slot >= 0) st3(fslot, slot, f);
-    if (residual_mode) {
-      const double mi = m.mass[i];
-      out = make_double3(f.x - mi * vi.x, f.y - mi * vi.y, f.z - mi * vi.z);
+    const double mi = m.mass[i];
+    const double3 t = ld3(m.tn, i);
+    out = make_double3(mi * (t.x - vi.x) + dt * (acc.x - di * vi.x), mi * (t.y - vi.y) + dt * (acc.y - di * vi.y),
+                       mi * (t.z - vi.z) + dt * (acc.z - di * vi.z));
+    if (slot >= 0) st3(fslot, slot, make_double3(out.x + mi * vi.x, out.y + mi * vi.y, out.z + mi * vi.z));
+  } else {
+    const double3 c = ld3(cstep, i);
+    const double3 rhs = make_double3(c.x + dt * (acc.x - di * vi.x), c.y + dt * (acc.y - di * vi.y),
+                                     c.z + dt * (acc.z - di * vi.z));
+    out = rhs;
+    if (slot >= 0) {
+      double ax = 0, ay = 0, az = 0;
+      for (int k = m.ata_ptr[i]; k < m.ata_ptr[i + 1]; ++k) {
+        const double a = m.ata_val[k];
+        const int j = m.ata_col[k];
+        ax += a * v[3 * (int64_t)j];
+        ay += a * v[3 * (int64_t)j + 1];
+        az += a * v[3 * (int64_t)j + 2];
+      }
+      const double dt2 = dt * dt;
+      st3(fslot, slot, make_double3(rhs.x - dt2 * ax, rhs.y - dt2 * ay, rhs.z - dt2 * az));
     }
   }
   const int64_t p = m.iperm[i];

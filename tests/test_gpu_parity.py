@@ -155,7 +155,7 @@ def test_fp32_refine_matches_fp64_oracle():
         o.step(1)
     qg, _ = g.state()
     qo, _ = o.state()
-    assert rel_err(qg, qo) < 1e-5, rel_err(qg, qo)
+    assert rel_err(qg, qo) < REL, rel_err(qg, qo)
 
 
 def test_nan_state_is_rejected():
