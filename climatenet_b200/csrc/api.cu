@@ -115,6 +115,7 @@ void build_schedule(pdf_handle* h, int chunk, int cut_level) {
   P.bidx = upload(hp.bidx.empty() ? std::vector<int>(kSlab, 0) : hp.bidx);
   P.max_cols = hp.max_block_cols;
   P.max_ext = hp.max_block_ext;
+  P.max_items = hp.max_block_items;
   const bool fits = h->fp32 ? configure_solve<float>(P) : configure_solve<double>(P);
   if (!fits) throw CudaFail("the sweep's block kernels do not fit the device's shared memory");
   h->n_levels = f.n_levels;

@@ -472,19 +472,24 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
   plan.chunk = chunk;
   // subtree extents: supernodes are numbered in column order and every
   // parent comes after its children, so one ascending pass accumulates them
-  std::vector<int> lo(S), cnt(S, 0);
+  std::vector<int> lo(S), cnt(S, 0), ftiles(S, 0), btiles(S, 0);
   for (int s = 0; s < S; ++s) lo[s] = f.sn_c0[s];
   for (int s = 0; s < S; ++s) {
     cnt[s] += f.sn_ns[s];
+    ftiles[s] += (int)(f.sn_ftile0[s + 1] - f.sn_ftile0[s]);
+    btiles[s] += (int)(f.sn_btile0[s + 1] - f.sn_btile0[s]);
     const int p = f.sn_parent[s];
     if (p >= 0) {
       lo[p] = std::min(lo[p], lo[s]);
       cnt[p] += cnt[s];
+      ftiles[p] += ftiles[s];
+      btiles[p] += btiles[s];
     }
   }
   auto eligible = [&](int s) {
     return f.sn_level[s] <= cut_level && f.sn_level[s] < kMaxBlockLevels && cnt[s] <= kMaxBlockCols &&
-           f.sn_nr[s] <= kMaxBlockExt && f.sn_c0[s] + f.sn_ns[s] - lo[s] == cnt[s];
+           f.sn_nr[s] <= kMaxBlockExt && ftiles[s] <= kMaxBlockItems && btiles[s] <= kMaxBlockItems &&
+           f.sn_c0[s] + f.sn_ns[s] - lo[s] == cnt[s];
   };
   std::vector<int> blk(S, -1);
   std::vector<int> roots;
@@ -562,6 +567,7 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
         }
     }
     bb.lev[bb.nlev] = (int)plan.bitem.size() - bb.item0;
+    plan.max_block_items = std::max(plan.max_block_items, std::max(fb.lev[fb.nlev], bb.lev[bb.nlev]));
     plan.fblk.push_back(fb);
     plan.bblk.push_back(bb);
   }
@@ -625,7 +631,8 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
   const int64_t nloc = (int64_t)plan.rows_loc.size();
   for (const SweepBlock& B : plan.fblk) {
     const int nc = B.c1 - B.c0, ld = nc + B.next;
-    if (nc <= 0 || nc > plan.max_block_cols || B.next > plan.max_block_ext || B.nlev > kMaxBlockLevels) {
+    if (nc <= 0 || nc > plan.max_block_cols || B.next > plan.max_block_ext || B.nlev > kMaxBlockLevels ||
+        B.lev[B.nlev] > plan.max_block_items) {
       err = "bad block extent";
       return false;
     }

@@ -105,6 +105,7 @@ void build_sweep_tasks(const Factor& f, int chunk, std::vector<SweepTask>& fwd, 
 constexpr int kMaxBlockLevels = 16;
 constexpr int kMaxBlockCols = 1536;
 constexpr int kMaxBlockExt = 1024;
+constexpr int kMaxBlockItems = 768;  // tiles per block and sweep (staged in shared memory)
 constexpr int kSlab = 16;  // columns (forward) / rows (backward) per bulk copy
 
 struct SweepBlock {
@@ -157,13 +158,13 @@ struct SweepPlan {
   // its vector entry is: >= 0 the shared vector (x), < 0 the shared y slice
   // (entry -1 - k is column k of the block)
   std::vector<int> bidx;
-  int max_block_cols = 0, max_block_ext = 0;
+  int max_block_cols = 0, max_block_ext = 0, max_block_items = 0;
   int64_t block_elems = 0, upper_elems = 0;  // stored W elements per sweep copy
 };
 
 // Blocks are the largest subtrees whose root is at most cut_level and whose
 // columns are contiguous, at most kMaxBlockCols, with at most kMaxBlockExt
-// rows outside; the rest is upper.
+// rows outside and at most kMaxBlockItems tiles per sweep; the rest is upper.
 void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan);
 
 // Host emulation of the two device sweeps of a plan on the tiled layout (same

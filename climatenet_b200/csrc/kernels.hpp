@@ -40,6 +40,7 @@ struct DPlan {
   const int* bidx;      // backward block tiles: per-row vector index lists
   int max_cols;         // widest block (shared-memory slice, 3 planes)
   int max_ext;          // most rows outside a block
+  int max_items;        // most tiles of a block in one sweep
   int smem_f, smem_b;   // dynamic shared memory of the forward / backward block kernels
   int grid_bf, grid_bb, grid_uf, grid_ub;
 };

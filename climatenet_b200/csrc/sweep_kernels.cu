@@ -156,33 +156,35 @@ __device__ __forceinline__ int item_extent(const BlockItem& I) {
   return kFwd ? min(I.ns, kTile * I.tile + kTile) : I.ns - kTile * I.tile + I.nr;
 }
 
+// items and lev are the block's item descriptors and level offsets staged in
+// shared memory (indices relative to the block's first item)
 template <bool kFwd>
-__device__ __forceinline__ void cursor_settle(SlabCursor& c, const SweepBlock& B, const BlockItem* items, int warp,
-                                              int nw) {
-  while (c.L < B.nlev && c.it >= B.item0 + B.lev[c.L + 1]) {
+__device__ __forceinline__ void cursor_settle(SlabCursor& c, int nlev, const int* lev, const BlockItem* items,
+                                              int warp) {
+  while (c.L < nlev && c.it >= lev[c.L + 1]) {
     ++c.L;
-    if (c.L < B.nlev) c.it = B.item0 + B.lev[c.L] + warp;
+    if (c.L < nlev) c.it = lev[c.L] + warp;
   }
-  if (c.L < B.nlev) c.len = item_extent<kFwd>(items[c.it]);
+  if (c.L < nlev) c.len = item_extent<kFwd>(items[c.it]);
 }
 
 template <bool kFwd>
-__device__ __forceinline__ void cursor_start(SlabCursor& c, const SweepBlock& B, const BlockItem* items, int warp,
-                                             int nw) {
+__device__ __forceinline__ void cursor_start(SlabCursor& c, int nlev, const int* lev, const BlockItem* items,
+                                             int warp) {
   c.L = 0;
-  c.it = B.item0 + B.lev[0] + warp;
+  c.it = lev[0] + warp;
   c.j0 = 0;
-  cursor_settle<kFwd>(c, B, items, warp, nw);
+  cursor_settle<kFwd>(c, nlev, lev, items, warp);
 }
 
 template <bool kFwd>
-__device__ __forceinline__ void cursor_next(SlabCursor& c, const SweepBlock& B, const BlockItem* items, int warp,
+__device__ __forceinline__ void cursor_next(SlabCursor& c, int nlev, const int* lev, const BlockItem* items, int warp,
                                             int nw) {
   c.j0 += kSlab;
   if (c.j0 >= c.len) {
     c.j0 = 0;
     c.it += nw;
-    cursor_settle<kFwd>(c, B, items, warp, nw);
+    cursor_settle<kFwd>(c, nlev, lev, items, warp);
   }
 }
 
@@ -214,6 +216,7 @@ struct BlockSmem {
   T* sv;
   T* ys;
   T* vstage;
+  BlockItem* items;
 };
 
 template <typename T, bool kFwd>
@@ -232,15 +235,17 @@ __device__ __forceinline__ BlockSmem<T> block_smem(unsigned char* base, int nw, 
   s.ys = reinterpret_cast<T*>(base + off);
   if (!kFwd) off += 3 * (size_t)max_cols * sizeof(T);
   s.vstage = reinterpret_cast<T*>(base + off) + (size_t)warp * 3 * kSlab;
+  if (!kFwd) off += (size_t)nw * 3 * kSlab * sizeof(T);
+  s.items = reinterpret_cast<BlockItem*>(base + ((off + 15) & ~size_t(15)));
   return s;
 }
 
 template <typename T, bool kFwd>
-size_t block_smem_bytes(int nw, int max_ld, int max_cols) {
+size_t block_smem_bytes(int nw, int max_ld, int max_cols, int max_items) {
   constexpr int R = Stages<T>::R, KE = Stages<T>::kElems;
   size_t b = (size_t)nw * R * KE * sizeof(T) + (size_t)nw * R * sizeof(uint64_t) + 3 * (size_t)max_ld * sizeof(T);
   if (!kFwd) b += (size_t)nw * R * kSlab * sizeof(int) + 3 * (size_t)max_cols * sizeof(T) + (size_t)nw * 3 * kSlab * sizeof(T);
-  return b;
+  return ((b + 15) & ~size_t(15)) + (size_t)max_items * sizeof(BlockItem);
 }
 
 // After an mbarrier wait gave up: wait (bounded) for every copy this warp
@@ -259,6 +264,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_forward(DPlan P, con
   __shared__ int s_ticket;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const BlockSmem<T> sm = block_smem<T, true>(smem_raw, nw, warp, P.max_cols + P.max_ext, P.max_cols);
+  __shared__ int s_lev[kMaxBlockLevels + 1];
   if (lane == 0)
     for (int k = 0; k < R; ++k) mbar_init(sm.bar + k, 1);
   fence_mbar_init();
@@ -270,7 +276,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_forward(DPlan P, con
     const int bi = cta_ticket(sy.queue + 2, &s_ticket);
     if (bi >= P.nblk) break;
     const SweepBlock& B = P.fblk[bi];
-    const int c0b = B.c0, nc = B.c1 - B.c0, ld = nc + B.next;
+    const int c0b = B.c0, nc = B.c1 - B.c0, ld = nc + B.next, nlev = B.nlev, nitems = B.lev[B.nlev];
     T* sv = sm.sv;
     for (int k = threadIdx.x; k < nc; k += blockDim.x) {
       sv[k] = b[c0b + k];
@@ -278,21 +284,24 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_forward(DPlan P, con
       sv[2 * ld + k] = b[2 * (int64_t)n + c0b + k];
     }
     for (int e = threadIdx.x; e < B.next; e += blockDim.x) sv[nc + e] = sv[ld + nc + e] = sv[2 * ld + nc + e] = T(0);
+    for (int k = threadIdx.x; k < nitems; k += blockDim.x) sm.items[k] = P.fitem[B.item0 + k];
+    if (threadIdx.x <= nlev) s_lev[threadIdx.x] = B.lev[threadIdx.x];
+    __syncthreads();
+    const BlockItem* items = sm.items;
     SlabCursor pc;
-    cursor_start<true>(pc, B, P.fitem, warp, nw);
-    for (int k = 0; k < R && !pc.done(B.nlev) && !failed; ++k) {
+    cursor_start<true>(pc, nlev, s_lev, items, warp);
+    for (int k = 0; k < R && !pc.done(nlev) && !failed; ++k) {
       const int st = prod % R;
-      if (lane == 0) issue_slab<T, true>(pc, P.fitem, W, P.bidx, sm.ring + st * KE, nullptr, sm.bar + st);
+      if (lane == 0) issue_slab<T, true>(pc, items, W, P.bidx, sm.ring + st * KE, nullptr, sm.bar + st);
       pending |= 1u << st;
       ++prod;
-      cursor_next<true>(pc, B, P.fitem, warp, nw);
+      cursor_next<true>(pc, nlev, s_lev, items, warp, nw);
     }
-    __syncthreads();
-    for (int L = 0; L < B.nlev; ++L) {
-      const int i1 = B.item0 + B.lev[L + 1];
+    for (int L = 0; L < nlev; ++L) {
+      const int i1 = s_lev[L + 1];
 #pragma unroll 1
-      for (int it = B.item0 + B.lev[L] + warp; it < i1; it += nw) {
-        const BlockItem I = P.fitem[it];
+      for (int it = s_lev[L] + warp; it < i1; it += nw) {
+        const BlockItem I = items[it];
         const int m = min(kTile, I.ns + I.nr - kTile * I.tile);
         const int w = min(I.ns, kTile * I.tile + kTile);
         const int row = kTile * I.tile + lane;
@@ -328,14 +337,14 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_forward(DPlan P, con
           }
           __syncwarp();
           ++cons;
-          if (!pc.done(B.nlev) && !failed) {
+          if (!pc.done(nlev) && !failed) {
             if (lane == 0) {
               fence_proxy_async();
-              issue_slab<T, true>(pc, P.fitem, W, P.bidx, sm.ring + st * KE, nullptr, sm.bar + st);
+              issue_slab<T, true>(pc, items, W, P.bidx, sm.ring + st * KE, nullptr, sm.bar + st);
             }
             pending |= 1u << st;
             ++prod;
-            cursor_next<true>(pc, B, P.fitem, warp, nw);
+            cursor_next<true>(pc, nlev, s_lev, items, warp, nw);
           }
         }
         if (row < I.ns) {
@@ -371,6 +380,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_backward(DPlan P, co
   __shared__ int s_ticket;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const BlockSmem<T> sm = block_smem<T, false>(smem_raw, nw, warp, P.max_cols + P.max_ext, P.max_cols);
+  __shared__ int s_lev[kMaxBlockLevels + 1];
   if (lane == 0)
     for (int k = 0; k < R; ++k) mbar_init(sm.bar + k, 1);
   fence_mbar_init();
@@ -382,9 +392,11 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_backward(DPlan P, co
     const int bi = cta_ticket(sy.queue + 3, &s_ticket);
     if (bi >= P.nblk) break;
     const SweepBlock& B = P.bblk[bi];
-    const int c0b = B.c0, nc = B.c1 - B.c0, ld = nc + B.next;
+    const int c0b = B.c0, nc = B.c1 - B.c0, ld = nc + B.next, nlev = B.nlev, nitems = B.lev[B.nlev];
     T* sv = sm.sv;
     T* ys = sm.ys;
+    for (int k = threadIdx.x; k < nitems; k += blockDim.x) sm.items[k] = P.bitem[B.item0 + k];
+    if (threadIdx.x <= nlev) s_lev[threadIdx.x] = B.lev[threadIdx.x];
     // the y slice, and the final x of the ext rows (the upper supernodes
     // finished in the previous launch)
     for (int k = threadIdx.x; k < nc; k += blockDim.x) {
@@ -398,22 +410,24 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_backward(DPlan P, co
       sv[ld + nc + e] = x[r + n];
       sv[2 * ld + nc + e] = x[r + 2 * (int64_t)n];
     }
+    __syncthreads();
+    const BlockItem* items = sm.items;
     SlabCursor pc;
-    cursor_start<false>(pc, B, P.bitem, warp, nw);
-    for (int k = 0; k < R && !pc.done(B.nlev) && !failed; ++k) {
+    cursor_start<false>(pc, nlev, s_lev, items, warp);
+    for (int k = 0; k < R && !pc.done(nlev) && !failed; ++k) {
       const int st = prod % R;
       if (lane == 0)
-        issue_slab<T, false>(pc, P.bitem, W, P.bidx, sm.ring + st * KE, sm.iring + st * kSlab, sm.bar + st);
+        issue_slab<T, false>(pc, items, W, P.bidx, sm.ring + st * KE, sm.iring + st * kSlab, sm.bar + st);
       pending |= 1u << st;
       ++prod;
-      cursor_next<false>(pc, B, P.bitem, warp, nw);
+      cursor_next<false>(pc, nlev, s_lev, items, warp, nw);
     }
     __syncthreads();
-    for (int L = 0; L < B.nlev; ++L) {
-      const int i1 = B.item0 + B.lev[L + 1];
+    for (int L = 0; L < nlev; ++L) {
+      const int i1 = s_lev[L + 1];
 #pragma unroll 1
-      for (int it = B.item0 + B.lev[L] + warp; it < i1; it += nw) {
-        const BlockItem I = P.bitem[it];
+      for (int it = s_lev[L] + warp; it < i1; it += nw) {
+        const BlockItem I = items[it];
         const int j0t = kTile * I.tile, nd = I.ns - j0t, mc = min(kTile, nd), h = nd + I.nr;
         T ax = 0, ay = 0, az = 0;
 #pragma unroll 1
@@ -462,14 +476,14 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_backward(DPlan P, co
           }
           __syncwarp();
           ++cons;
-          if (!pc.done(B.nlev) && !failed) {
+          if (!pc.done(nlev) && !failed) {
             if (lane == 0) {
               fence_proxy_async();
-              issue_slab<T, false>(pc, P.bitem, W, P.bidx, sm.ring + st * KE, sm.iring + st * kSlab, sm.bar + st);
+              issue_slab<T, false>(pc, items, W, P.bidx, sm.ring + st * KE, sm.iring + st * kSlab, sm.bar + st);
             }
             pending |= 1u << st;
             ++prod;
-            cursor_next<false>(pc, B, P.bitem, warp, nw);
+            cursor_next<false>(pc, nlev, s_lev, items, warp, nw);
           }
         }
         if (lane < mc) {
@@ -691,8 +705,8 @@ template <typename T>
 bool configure_solve(DPlan& P) {
   const int nw = kSweepThreads / 32;
   const int max_ld = std::max(1, P.max_cols + P.max_ext);
-  P.smem_f = (int)block_smem_bytes<T, true>(nw, max_ld, std::max(1, P.max_cols));
-  P.smem_b = (int)block_smem_bytes<T, false>(nw, max_ld, std::max(1, P.max_cols));
+  P.smem_f = (int)block_smem_bytes<T, true>(nw, max_ld, std::max(1, P.max_cols), std::max(1, P.max_items));
+  P.smem_b = (int)block_smem_bytes<T, false>(nw, max_ld, std::max(1, P.max_cols), std::max(1, P.max_items));
   const int rf = resident_ctas(k_block_forward<T>, P.smem_f);
   const int rb = resident_ctas(k_block_backward<T>, P.smem_b);
   P.grid_bf = std::max(1, std::min(rf, std::max(1, P.nblk)));
