@@ -1518,6 +1518,51 @@ int pdf_get_residual_history(pdf_handle* h, double* out, int32_t cap, int32_t* n
 
 void pdf_destroy(pdf_handle* h) { free_handle(h); }
 
+int pdf_time_solve_parts(pdf_handle* h, int32_t reps, double* part_ms) {
+  if (!h || reps <= 0 || !part_ms) return fail(h, PDF_INVALID_ARG, "invalid solve timing request");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    DeviceBuffers& d = h->d;
+    const int N = h->dm.N;
+    cudaStream_t st = h->stream;
+    std::vector<double> vsave(3 * (size_t)N), qsave(3 * (size_t)N);
+    CK(cudaMemcpy(vsave.data(), d.v, vsave.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(qsave.data(), d.qk, qsave.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    const size_t bbytes = 3 * (size_t)N * (h->fp32 ? sizeof(float) : sizeof(double));
+    void* bsave = nullptr;
+    CK(cudaMalloc(&bsave, bbytes));
+    void* bcur = h->fp32 ? (void*)d.b32 : (void*)d.b64;
+    CK(cudaMemcpyAsync(bsave, bcur, bbytes, cudaMemcpyDeviceToDevice, st));
+    cudaEvent_t ev[6];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    double acc[5] = {0, 0, 0, 0, 0};
+    for (int r = 0; r < reps; ++r) {
+      CK(cudaMemcpyAsync(bcur, bsave, bbytes, cudaMemcpyDeviceToDevice, st));
+      CK(cudaEventRecord(ev[0], st));
+      WriteBack wb{d.v, d.qk, d.q, h->prm.time_step, h->fp32 ? 1 : 0};
+      if (h->fp32)
+        launch_solve_sweeps<float>(st, d.plan, d.Wf32, d.Wb32, d.b32, d.y32, d.x32, N, d.sync, wb, ev + 1);
+      else
+        launch_solve_sweeps<double>(st, d.plan, d.Wf64, d.Wb64, d.b64, d.y64, d.x64, N, d.sync, wb, ev + 1);
+      CK(cudaEventRecord(ev[5], st));
+      CK(cudaEventSynchronize(ev[5]));
+      for (int k = 0; k < 5; ++k) {
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+        acc[k] += ms;
+      }
+    }
+    for (int k = 0; k < 5; ++k) part_ms[k] = acc[k] / reps;
+    for (auto& e : ev) cudaEventDestroy(e);
+    CK(cudaMemcpyAsync(bcur, bsave, bbytes, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpy(d.v, vsave.data(), vsave.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.qk, qsave.data(), qsave.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaStreamSynchronize(st));
+    cudaFree(bsave);
+    return PDF_OK;
+  });
+}
+
 int pdf_check_wait_timeout(pdf_handle* h, int32_t max_spins) {
   if (!h || max_spins <= 0) return fail(h, PDF_INVALID_ARG, "invalid wait-timeout check");
   return guarded(h, [&]() -> int {

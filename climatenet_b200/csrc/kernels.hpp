@@ -153,7 +153,7 @@ template <typename T>
 bool configure_solve(DPlan& P);  // shared memory and grids; false if a block kernel does not fit
 template <typename T>
 void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
-                         SweepSync sy, WriteBack wb);
+                         SweepSync sy, WriteBack wb, cudaEvent_t* marks = nullptr);
 template <typename T>
 void launch_solve_prep(cudaStream_t st, int n, T* x, T* y, SweepSync sy);
 

@@ -718,11 +718,16 @@ bool configure_solve(DPlan& P) {
 
 template <typename T>
 void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
-                         SweepSync sy, WriteBack wb) {
+                         SweepSync sy, WriteBack wb, cudaEvent_t* marks) {
+  // marks (optional): 4 events recorded between the five launches
   k_block_forward<T><<<P.grid_bf, kSweepThreads, P.smem_f, st>>>(P, Wf, b, y, n, sy);
+  if (marks) cudaEventRecord(marks[0], st);
   k_upper_forward<T><<<P.grid_uf, kSweepThreads, 0, st>>>(P, Wf, b, y, n, sy);
+  if (marks) cudaEventRecord(marks[1], st);
   k_upper_backward<T><<<P.grid_ub, kSweepThreads, 0, st>>>(P, Wb, y, x, n, sy);
+  if (marks) cudaEventRecord(marks[2], st);
   k_block_backward<T><<<P.grid_bb, kSweepThreads, P.smem_b, st>>>(P, Wb, y, x, n, sy, wb);
+  if (marks) cudaEventRecord(marks[3], st);
   k_solve_post<T><<<std::max(1, std::min(148 * 4, (P.n_upper + 255) / 256)), 256, 0, st>>>(P, x, y, n, wb, sy);
 }
 template <typename T>
@@ -733,9 +738,9 @@ void launch_solve_prep(cudaStream_t st, int n, T* x, T* y, SweepSync sy) {
 template bool configure_solve<double>(DPlan&);
 template bool configure_solve<float>(DPlan&);
 template void launch_solve_sweeps<double>(cudaStream_t, const DPlan&, const double*, const double*, double*, double*,
-                                          double*, int, SweepSync, WriteBack);
+                                          double*, int, SweepSync, WriteBack, cudaEvent_t*);
 template void launch_solve_sweeps<float>(cudaStream_t, const DPlan&, const float*, const float*, float*, float*,
-                                         float*, int, SweepSync, WriteBack);
+                                         float*, int, SweepSync, WriteBack, cudaEvent_t*);
 template void launch_solve_prep<double>(cudaStream_t, int, double*, double*, SweepSync);
 template void launch_solve_prep<float>(cudaStream_t, int, float*, float*, SweepSync);
 

@@ -55,6 +55,7 @@ def lib():
     L.pdf_get_residual_history.argtypes = [vp, vp, i32, C.POINTER(i32)]
     L.pdf_time_phase.argtypes = [vp, i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.pdf_check_wait_timeout.argtypes = [vp, i32]
+    L.pdf_time_solve_parts.argtypes = [vp, i32, C.POINTER(C.c_double)]
     L.pdf_factor_check.argtypes = [C.POINTER(abi.pdf_scene_desc), C.POINTER(abi.pdf_params), vp, vp]
     L.pdf_detect_candidates_noalloc.argtypes = [vp, i32, vp, i32, C.c_double, vp, i32, C.POINTER(i32), vp]
     L.pdf_destroy.argtypes = [vp]
@@ -208,6 +209,13 @@ class Simulation:
         _check(lib().pdf_export_stats(self.h, os.fsencode(path)), self.h)
 
     exportStats = export_stats
+
+    def time_solve_parts(self, reps=10):
+        """Device ms of the five launches of one solve: block forward, upper
+        forward, upper backward, block backward, upper write-back."""
+        out = (C.c_double * 5)()
+        _check(lib().pdf_time_solve_parts(self.h, reps, out), self.h)
+        return list(out)
 
     def time_phase(self, phase, reps=10):
         """(ms per repetition, algorithmic bytes) of one phase run in isolation."""

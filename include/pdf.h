@@ -346,6 +346,14 @@ int pdf_get_residual_history(pdf_handle* h, double* out, int32_t cap,
 int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms,
                    double* bytes);
 
+/* Device time (CUDA events, average of reps) of the five launches of one
+ * global solve on the handle's current right-hand side: part_ms[0] block
+ * forward sweep, [1] upper forward items, [2] upper backward items, [3]
+ * block backward sweep with its write-back, [4] the upper columns'
+ * write-back.  The state is restored afterwards (no counterpart in the
+ * reference; a profiling aid). */
+int pdf_time_solve_parts(pdf_handle* h, int32_t reps, double* part_ms);
+
 /* Check of the bounded device waits (no counterpart in the reference): runs
  * one global solve whose dependency targets lie one solve ahead of the
  * completion counters, on a schedule whose blocks are only the leaves, so
