@@ -84,6 +84,7 @@ void free_plan(DPlan& P) {
   free_dev(P.upper_cols);
   free_dev(P.rows_loc);
   free_dev(P.bidx);
+  free_dev(P.child);
 }
 
 // Sweep plan (subtree blocks + upper work items, factor.hpp) on the device.
@@ -113,6 +114,7 @@ void build_schedule(pdf_handle* h, int chunk, int cut_level) {
   P.perm = h->d.perm;
   P.rows_loc = upload(hp.rows_loc);
   P.bidx = upload(hp.bidx.empty() ? std::vector<int>(kSlab, 0) : hp.bidx);
+  P.child = upload(hp.child.empty() ? std::vector<int>(2, 0) : hp.child);
   P.max_cols = hp.max_block_cols;
   P.max_ext = hp.max_block_ext;
   P.max_items = hp.max_block_items;

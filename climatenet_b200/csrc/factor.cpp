@@ -588,9 +588,20 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
   for (const SweepTask& t : plan.bup) plan.sn[t.sn].ntb++;
   // the blocks finish in an earlier launch than the upper items: an upper
   // supernode waits only for its upper children
-  std::vector<int> upper_children(S, 0);
+  std::vector<int> upper_children(S, 0), child0(S, 0);
+  std::vector<std::vector<int>> kids(S);
   for (int s = 0; s < S; ++s)
-    if (blk[s] < 0 && f.sn_parent[s] >= 0) upper_children[f.sn_parent[s]]++;
+    if (blk[s] < 0 && f.sn_parent[s] >= 0) {
+      upper_children[f.sn_parent[s]]++;
+      kids[f.sn_parent[s]].push_back(s);
+    }
+  for (int s = 0; s < S; ++s) {
+    child0[s] = (int)plan.child.size() / 2;
+    for (int c : kids[s]) {
+      plan.child.push_back(c);
+      plan.child.push_back(plan.sn[c].ntf);
+    }
+  }
   auto upper = [&](const SweepTask& t, bool fwd) {
     const SnInfo& q = plan.sn[t.sn];
     UpperItem u{};
@@ -606,6 +617,7 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
     u.parent = q.parent;
     u.wait = fwd ? upper_children[t.sn] : (q.parent >= 0 ? plan.sn[q.parent].ntb : 0);
     u.ntf = q.ntf;
+    u.child0 = fwd ? child0[t.sn] : 0;
     return u;
   };
   for (const SweepTask& t : plan.fup) plan.fupi.push_back(upper(t, true));
@@ -680,8 +692,13 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
     }
   }
   // forward, upper work items (the records the device reads)
+  const int64_t nchild = (int64_t)plan.child.size() / 2;
   for (const UpperItem& tk : plan.fupi) {
     const UpperItem& s = tk;
+    for (int c = 0; c < tk.wait; ++c) {
+      if (!chk(tk.child0 + c, nchild, "forward child list")) return false;
+      if (!chk(plan.child[2 * (tk.child0 + c)], f.n_sn, "forward child supernode")) return false;
+    }
     const int mrows = std::min(kTile, s.ns + s.nr - tk.tile * kTile);
     for (int l = 0; l < mrows; ++l) {
       const int row = tk.tile * kTile + l;

@@ -137,9 +137,10 @@ struct alignas(16) UpperItem {
   int sn, tile, a0, a1;
   int c0, ns, nr, roff;
   int parent;      // parent supernode, -1 if none
-  int wait;        // forward: children of sn; backward: work items of the parent
-  int ntf;         // forward: work items of sn (its last one signals the parent)
-  int pad[3];
+  int wait;        // forward: upper children of sn; backward: work items of the parent
+  int ntf;         // forward: work items of sn
+  int child0;      // forward: its upper children are SweepPlan::child[child0, child0 + wait)
+  int pad[2];
 };
 static_assert(sizeof(UpperItem) == 64, "UpperItem is one 64-byte record");
 
@@ -151,6 +152,9 @@ struct SweepPlan {
   std::vector<BlockItem> fitem, bitem;
   std::vector<UpperItem> fupi, bupi;   // the upper items as the device reads them
   std::vector<int> upper_cols;         // pivot positions of the upper supernodes' columns
+  // per upper supernode with upper children: (child, forward work items of
+  // the child), the counters a forward item polls before it starts
+  std::vector<int> child;              // pairs, flattened
   // per entry of Factor::rows of a block supernode: the row's place in the
   // block's shared vector (column - c0 inside the block, nc + ext index outside)
   std::vector<int> rows_loc;

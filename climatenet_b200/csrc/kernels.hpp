@@ -38,6 +38,7 @@ struct DPlan {
   const int* perm;      // pivot position -> vertex
   const int* rows_loc;  // block supernodes: place of each row in the block's shared vector
   const int* bidx;      // backward block tiles: per-row vector index lists
+  const int* child;     // forward upper items: (child, its work items) pairs
   int max_cols;         // widest block (shared-memory slice, 3 planes)
   int max_ext;          // most rows outside a block
   int max_items;        // most tiles of a block in one sweep

@@ -19,8 +19,9 @@
 //     The ext rows' updates are added to b with one atomic each per block.
 //  2. k_upper_forward — the supernodes above the blocks, split into 32-row
 //     tiles x column chunks, taken by warps from a queue in elimination-tree
-//     order; a warp waits (bounded spin) only until the supernode's upper
-//     children are complete (the blocks finished in launch 1).  Partial sums
+//     order; a warp waits (bounded spin) only until every work item of the
+//     supernode's upper children is counted (the blocks finished in launch 1);
+//     each item counts itself without reading the counter back.  Partial sums
 //     land in y / b_R with atomics.
 //  3. k_upper_backward — the same supernodes top-down in 32-column tiles x row
 //     chunks; an item waits until its parent is complete; sums land in x.
@@ -537,8 +538,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_forward(DPlan P, const 
     T w[32];
     load_tile(w, wbase + (int64_t)tk.a0 * mrows, min(32, tk.a1 - tk.a0), mrows, lane < mrows);
     int ok = 1;
-    if (lane == 0 && tk.wait > 0)
-      ok = wait_counter(sy.fchild + tk.sn, ep * (unsigned long long)tk.wait, sy.err, sy.max_spins);
+    if (lane == 0)
+      for (int c = 0; c < tk.wait && ok; ++c) {
+        const int2 ch = reinterpret_cast<const int2*>(P.child)[tk.child0 + c];
+        ok = wait_counter(sy.fdone + ch.x, ep * (unsigned long long)ch.y, sy.err, sy.max_spins);
+      }
     ok = __shfl_sync(0xffffffffu, ok, 0);
     const int row = tk.tile * kTile + lane;
     T ax = 0, ay = 0, az = 0;
@@ -574,15 +578,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_forward(DPlan P, const 
         atomicAdd(b + r + 2 * (int64_t)n, -az);
       }
     }
+    // the item's updates are performed before its count: a parent item that
+    // sees every item of this supernode counted sees all of them
     fence_acq_rel_gpu();
     __syncwarp();
-    if (lane == 0) {
-      const unsigned long long done = atomicAdd(sy.fdone + tk.sn, 1ULL) + 1ULL;
-      if (done == ep * (unsigned long long)tk.ntf && tk.parent >= 0) {
-        fence_acq_rel_gpu();
-        atomicAdd(sy.fchild + tk.parent, 1ULL);
-      }
-    }
+    if (lane == 0) atomicAdd(sy.fdone + tk.sn, 1ULL);
   }
 }
 
