@@ -125,6 +125,8 @@ class pdf_stats(C.Structure):
         ("sweep_cut_level", C.c_int32), ("sweep_blocks", C.c_int32),
         ("sweep_block_elems", C.c_int64), ("sweep_upper_elems", C.c_int64),
         ("sweep_cut_ms", C.c_double * 8),
+        ("sweep_upper_mode", C.c_int32), ("sweep_upper_levels", C.c_int32),
+        ("sweep_cut_level_ms", C.c_double * 8),
     ]
 
 

@@ -89,7 +89,7 @@ void free_plan(DPlan& P) {
 
 // Sweep plan (subtree blocks + upper work items, factor.hpp) on the device.
 // The completion counters are cumulative per schedule, so they restart here.
-void build_schedule(pdf_handle* h, int chunk, int cut_level) {
+void build_schedule(pdf_handle* h, int chunk, int cut_level, int upper_mode = 0) {
   const Factor& f = h->fac;
   SweepPlan& hp = h->d.host_plan;
   build_sweep_plan(f, chunk, cut_level, hp);
@@ -118,11 +118,21 @@ void build_schedule(pdf_handle* h, int chunk, int cut_level) {
   P.max_cols = hp.max_block_cols;
   P.max_ext = hp.max_block_ext;
   P.max_items = hp.max_block_items;
+  P.n_flev = (int)hp.fup_lev.size() - 1;
+  P.n_blev = (int)hp.bup_lev.size() - 1;
+  const bool levels_fit = P.n_flev <= kMaxUpperLevels && P.n_blev <= kMaxUpperLevels;
+  P.upper_mode = upper_mode == 1 && levels_fit ? 1 : 0;
+  for (int k = 0; k <= kMaxUpperLevels; ++k) {
+    P.flev[k] = levels_fit && k <= P.n_flev ? hp.fup_lev[k] : 0;
+    P.blev[k] = levels_fit && k <= P.n_blev ? hp.bup_lev[k] : 0;
+  }
   const bool fits = h->fp32 ? configure_solve<float>(P) : configure_solve<double>(P);
   if (!fits) throw CudaFail("the sweep's block kernels do not fit the device's shared memory");
   h->n_levels = f.n_levels;
   h->stats.sweep_chunk = chunk;
   h->stats.sweep_cut_level = cut_level;
+  h->stats.sweep_upper_mode = P.upper_mode;
+  h->stats.sweep_upper_levels = P.n_flev;
   h->stats.sweep_blocks = P.nblk;
   h->stats.sweep_block_elems = hp.block_elems;
   h->stats.sweep_upper_elems = hp.upper_elems;
@@ -547,8 +557,9 @@ void launch_solve_with(pdf_handle* h, const SweepSync& sy, T* b, T* y, T* x, con
 }
 
 // Schedule autotuner: times the global solve of this scene's factor with
-// each candidate cut level (work-item width 64), then with each work-item
-// width at the best cut level, and keeps the fastest.  The right-hand side is
+// each candidate cut level and both upper modes (work-item width 64), then
+// with each work-item width at the best cut level and mode, and keeps the
+// fastest.  The right-hand side is
 // zero (the sweeps read the same data and wait on the same dependencies
 // whatever the values); v and q^k, which the solve writes, are restored.
 void autotune_schedule(pdf_handle* h) {
@@ -558,8 +569,9 @@ void autotune_schedule(pdf_handle* h) {
   std::vector<double> vsave(3 * (size_t)N), qsave(3 * (size_t)N);
   CK(cudaMemcpy(vsave.data(), d.v, vsave.size() * sizeof(double), cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(qsave.data(), d.qk, qsave.size() * sizeof(double), cudaMemcpyDeviceToHost));
-  auto time_plan = [&](int chunk, int cut) {
-    build_schedule(h, chunk, cut);
+  auto time_plan = [&](int chunk, int cut, int mode) {
+    build_schedule(h, chunk, cut, mode);
+    if (h->d.plan.upper_mode != mode) return 0.;
     double total = 0.;
     for (int r = 0; r < 4; ++r) {
       if (h->fp32) {
@@ -586,25 +598,33 @@ void autotune_schedule(pdf_handle* h) {
     return total / 3.;
   };
   double best = 1e300;
-  int best_cut = kCutLevel, best_chunk = kChunk;
-  for (int cut = 0; cut < kCutCandidates; ++cut) {
-    const double ms = time_plan(kChunk, cut);
-    h->stats.sweep_cut_ms[cut] = ms;
-    if (ms < best) {
-      best = ms;
-      best_cut = cut;
+  int best_cut = kCutLevel, best_chunk = kChunk, best_mode = 0;
+  double cut_ms[2][kCutCandidates] = {};
+  for (int cut = 0; cut < kCutCandidates; ++cut)
+    for (int mode = 0; mode < 2; ++mode) {
+      const double ms = time_plan(kChunk, cut, mode);
+      cut_ms[mode][cut] = ms;
+      if (ms > 0. && ms < best) {
+        best = ms;
+        best_cut = cut;
+        best_mode = mode;
+      }
     }
+  for (int cut = 0; cut < kCutCandidates; ++cut) {
+    h->stats.sweep_cut_ms[cut] = cut_ms[0][cut];
+    h->stats.sweep_cut_level_ms[cut] = cut_ms[1][cut];
   }
+  const double best_default_chunk = best;
   for (int ci = 0; ci < 3; ++ci) {
     const int chunk = kChunkCandidates[ci];
-    const double ms = chunk == kChunk ? h->stats.sweep_cut_ms[best_cut] : time_plan(chunk, best_cut);
+    const double ms = chunk == kChunk ? best_default_chunk : time_plan(chunk, best_cut, best_mode);
     h->stats.sweep_chunk_ms[ci] = ms;
     if (ms < best) {
       best = ms;
       best_chunk = chunk;
     }
   }
-  build_schedule(h, best_chunk, best_cut);
+  build_schedule(h, best_chunk, best_cut, best_mode);
   if (h->fp32)
     launch_solve_prep<float>(st, N, d.x32, d.y32, d.sync);
   else

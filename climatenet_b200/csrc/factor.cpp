@@ -622,6 +622,15 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
   };
   for (const SweepTask& t : plan.fup) plan.fupi.push_back(upper(t, true));
   for (const SweepTask& t : plan.bup) plan.bupi.push_back(upper(t, false));
+  // level boundaries (the items are in level order: ascending forward,
+  // descending backward)
+  auto bounds = [&](const std::vector<SweepTask>& v, std::vector<int>& lev) {
+    lev.assign(1, 0);
+    for (size_t k = 1; k <= v.size(); ++k)
+      if (k == v.size() || f.sn_level[v[k].sn] != f.sn_level[v[k - 1].sn]) lev.push_back((int)k);
+  };
+  bounds(plan.fup, plan.fup_lev);
+  bounds(plan.bup, plan.bup_lev);
 }
 
 bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<double>& bin,
@@ -689,6 +698,37 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
         return false;
       }
       for (int c = 0; c < 3; ++c) b[r + c * n] += sv[nc + e + c * ld];
+    }
+  }
+  // the level launches: the items of one supernode share a level, and a
+  // supernode's level comes after its children's forward and before them
+  // backward (no item reads what another item of its own launch writes)
+  {
+    auto groups = [&](const std::vector<UpperItem>& v, const std::vector<int>& lev, std::vector<int>& grp) {
+      grp.assign(f.n_sn, -1);
+      if (lev.empty() || lev.front() != 0 || lev.back() != (int)v.size()) return false;
+      for (size_t g = 0; g + 1 < lev.size(); ++g) {
+        if (lev[g] >= lev[g + 1]) return false;
+        for (int t = lev[g]; t < lev[g + 1]; ++t) {
+          const int sn = v[t].sn;
+          if (sn < 0 || sn >= f.n_sn || (grp[sn] >= 0 && grp[sn] != (int)g)) return false;
+          grp[sn] = (int)g;
+        }
+      }
+      return true;
+    };
+    std::vector<int> gf, gb;
+    if (!groups(plan.fupi, plan.fup_lev, gf) || !groups(plan.bupi, plan.bup_lev, gb)) {
+      err = "upper level boundaries do not partition the work items";
+      return false;
+    }
+    for (int s = 0; s < f.n_sn; ++s) {
+      const int p = f.sn_parent[s];
+      if (gf[s] < 0 || p < 0 || gf[p] < 0) continue;
+      if (!(gf[p] > gf[s]) || !(gb[p] < gb[s])) {
+        err = "an upper supernode shares a level launch with its parent";
+        return false;
+      }
     }
   }
   // forward, upper work items (the records the device reads)

@@ -151,6 +151,9 @@ struct SweepPlan {
   std::vector<SweepBlock> fblk, bblk;  // blocks, item offsets in forward / backward order
   std::vector<BlockItem> fitem, bitem;
   std::vector<UpperItem> fupi, bupi;   // the upper items as the device reads them
+  // the upper items by elimination-tree level, in sweep order: forward level
+  // k is fupi[fup_lev[k], fup_lev[k+1]), backward level k bupi[bup_lev[k], ...)
+  std::vector<int> fup_lev, bup_lev;
   std::vector<int> upper_cols;         // pivot positions of the upper supernodes' columns
   // per upper supernode with upper children: (child, forward work items of
   // the child), the counters a forward item polls before it starts

@@ -21,6 +21,8 @@ struct SweepSync {
   DTrace trace;                // iteration clock (forward sweep row)
 };
 
+constexpr int kMaxUpperLevels = 32;
+
 // Device view of a SweepPlan (factor.hpp) and its launch shape.
 struct DPlan {
   const UpperItem* fup;
@@ -44,6 +46,12 @@ struct DPlan {
   int max_items;        // most tiles of a block in one sweep
   int smem_f, smem_b;   // dynamic shared memory of the forward / backward block kernels
   int grid_bf, grid_bb, grid_uf, grid_ub;
+  // upper supernodes: 0 = dependency-driven items in one launch per sweep,
+  // 1 = one launch per elimination-tree level (no waits; the launch boundary
+  // orders the levels), with the level boundaries of fup / bup
+  int upper_mode;
+  int n_flev, n_blev;
+  int flev[kMaxUpperLevels + 1], blev[kMaxUpperLevels + 1];
 };
 
 // Write-back of the solution: v[perm] = x (mode 0) or v[perm] += x (mode 1,

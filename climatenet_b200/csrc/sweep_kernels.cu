@@ -652,6 +652,106 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_backward(DPlan P, const
   }
 }
 
+// ---------------------------------------------- upper items, level by level
+
+// One elimination-tree level of upper items per launch, spread over all warps
+// (grid-stride); the launches follow one another in sweep order, so an item
+// needs no dependency wait and signals nothing.
+template <typename T>
+__global__ void __launch_bounds__(kSweepThreads) k_upper_level_forward(DPlan P, int lo, int hi,
+                                                                       const T* __restrict__ W, T* b, T* y, int n) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+#pragma unroll 1
+  for (int t = lo + gw; t < hi; t += nwarps) {
+    const UpperItem tk = P.fup[t];
+    const int mrows = min(kTile, tk.ns + tk.nr - tk.tile * kTile);
+    const T* wbase = W + tk.off + lane;
+    const int row = tk.tile * kTile + lane;
+    const T* bx = b + tk.c0;
+    const T* by = bx + n;
+    const T* bz = by + n;
+    T ax = 0, ay = 0, az = 0;
+    for (int j0 = tk.a0; j0 < tk.a1; j0 += 32) {
+      T w[32];
+      load_tile(w, wbase + (int64_t)j0 * mrows, min(32, tk.a1 - j0), mrows, lane < mrows);
+      const int jl = j0 + lane;
+      T vx = 0, vy = 0, vz = 0;
+      if (jl < tk.a1) {
+        vx = ldcg(bx + jl);
+        vy = ldcg(by + jl);
+        vz = ldcg(bz + jl);
+      }
+#pragma unroll
+      for (int u = 0; u < 32; ++u) {
+        ax += w[u] * __shfl_sync(0xffffffffu, vx, u);
+        ay += w[u] * __shfl_sync(0xffffffffu, vy, u);
+        az += w[u] * __shfl_sync(0xffffffffu, vz, u);
+      }
+    }
+    if (row < tk.ns) {
+      const int64_t o = (int64_t)tk.c0 + row;
+      atomicAdd(y + o, ax);
+      atomicAdd(y + o + n, ay);
+      atomicAdd(y + o + 2 * (int64_t)n, az);
+    } else if (row < tk.ns + tk.nr) {
+      const int64_t r = P.rows[tk.roff + row - tk.ns];
+      atomicAdd(b + r, -ax);
+      atomicAdd(b + r + n, -ay);
+      atomicAdd(b + r + 2 * (int64_t)n, -az);
+    }
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P, int lo, int hi,
+                                                                        const T* __restrict__ W,
+                                                                        const T* __restrict__ y, T* x, int n) {
+  const int lane = threadIdx.x & 31;
+  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+#pragma unroll 1
+  for (int t = lo + gw; t < hi; t += nwarps) {
+    const UpperItem tk = P.bup[t];
+    const int mcols = min(kTile, tk.ns - tk.tile * kTile);
+    const T* wbase = W + tk.off + lane;
+    const int j0t = tk.tile * kTile;
+    const int col = j0t + lane;
+    const int nd = tk.ns - j0t;
+    T ax = 0, ay = 0, az = 0;
+    for (int i0 = tk.a0; i0 < tk.a1; i0 += 32) {
+      T w[32];
+      load_tile(w, wbase + (int64_t)i0 * mcols, min(32, tk.a1 - i0), mcols, lane < mcols);
+      const int il = i0 + lane;
+      T vx = 0, vy = 0, vz = 0;
+      if (il < tk.a1) {
+        if (il < nd) {
+          const int64_t o = (int64_t)tk.c0 + j0t + il;
+          vx = ldcg(y + o);
+          vy = ldcg(y + o + n);
+          vz = ldcg(y + o + 2 * (int64_t)n);
+        } else {
+          const int64_t r = P.rows[tk.roff + il - nd];
+          vx = -ldcg(x + r);
+          vy = -ldcg(x + r + n);
+          vz = -ldcg(x + r + 2 * (int64_t)n);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 32; ++u) {
+        ax += w[u] * __shfl_sync(0xffffffffu, vx, u);
+        ay += w[u] * __shfl_sync(0xffffffffu, vy, u);
+        az += w[u] * __shfl_sync(0xffffffffu, vz, u);
+      }
+    }
+    if (col < tk.ns) {
+      const int64_t o = (int64_t)tk.c0 + col;
+      atomicAdd(x + o, ax);
+      atomicAdd(x + o + n, ay);
+      atomicAdd(x + o + 2 * (int64_t)n, az);
+    }
+  }
+}
+
 // After the backward sweep, for the upper supernodes' columns: v[perm] = x
 // (mode 0) or v[perm] += x (mode 1), q^k = q_n + dt v, and x, y cleared for
 // the next solve (the blocks' columns are written back by the backward sweep
@@ -713,6 +813,9 @@ bool configure_solve(DPlan& P) {
   P.grid_bb = std::max(1, std::min(rb, std::max(1, P.nblk)));
   P.grid_uf = std::max(1, resident_ctas(k_upper_forward<T>, 0));
   P.grid_ub = std::max(1, resident_ctas(k_upper_backward<T>, 0));
+  // the level kernels use the same launch shape; make sure they can launch
+  resident_ctas(k_upper_level_forward<T>, 0);
+  resident_ctas(k_upper_level_backward<T>, 0);
   return rf > 0 && rb > 0;
 }
 
@@ -722,9 +825,27 @@ void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* 
   // marks (optional): 4 events recorded between the five launches
   k_block_forward<T><<<P.grid_bf, kSweepThreads, P.smem_f, st>>>(P, Wf, b, y, n, sy);
   if (marks) cudaEventRecord(marks[0], st);
-  k_upper_forward<T><<<P.grid_uf, kSweepThreads, 0, st>>>(P, Wf, b, y, n, sy);
+  if (P.upper_mode == 1) {
+    const int wpc = kSweepThreads / 32;
+    for (int k = 0; k < P.n_flev; ++k) {
+      const int lo = P.flev[k], hi = P.flev[k + 1];
+      const int grid = std::max(1, std::min(P.grid_uf, (hi - lo + wpc - 1) / wpc));
+      k_upper_level_forward<T><<<grid, kSweepThreads, 0, st>>>(P, lo, hi, Wf, b, y, n);
+    }
+  } else {
+    k_upper_forward<T><<<P.grid_uf, kSweepThreads, 0, st>>>(P, Wf, b, y, n, sy);
+  }
   if (marks) cudaEventRecord(marks[1], st);
-  k_upper_backward<T><<<P.grid_ub, kSweepThreads, 0, st>>>(P, Wb, y, x, n, sy);
+  if (P.upper_mode == 1) {
+    const int wpc = kSweepThreads / 32;
+    for (int k = 0; k < P.n_blev; ++k) {
+      const int lo = P.blev[k], hi = P.blev[k + 1];
+      const int grid = std::max(1, std::min(P.grid_ub, (hi - lo + wpc - 1) / wpc));
+      k_upper_level_backward<T><<<grid, kSweepThreads, 0, st>>>(P, lo, hi, Wb, y, x, n);
+    }
+  } else {
+    k_upper_backward<T><<<P.grid_ub, kSweepThreads, 0, st>>>(P, Wb, y, x, n, sy);
+  }
   if (marks) cudaEventRecord(marks[2], st);
   k_block_backward<T><<<P.grid_bb, kSweepThreads, P.smem_b, st>>>(P, Wb, y, x, n, sy, wb);
   if (marks) cudaEventRecord(marks[3], st);

@@ -188,6 +188,12 @@ typedef struct pdf_stats {
   int32_t sweep_cut_level, sweep_blocks;
   int64_t sweep_block_elems, sweep_upper_elems;
   double sweep_cut_ms[8];           /* solve time measured for cut levels 0-7   */
+  /* the supernodes above the blocks: 0 = dependency-driven work items in one
+   * launch per sweep, 1 = one launch per elimination-tree level; the number
+   * of such levels, and the solve time in mode 1 for cut levels 0-7 (0 where
+   * the levels exceed the launch table) */
+  int32_t sweep_upper_mode, sweep_upper_levels;
+  double sweep_cut_level_ms[8];
 } pdf_stats;
 
 /* One contact, as the reference's CollisionInfo / SelfCollisionInfo plus
