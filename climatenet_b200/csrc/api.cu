@@ -1585,6 +1585,33 @@ int pdf_time_solve_parts(pdf_handle* h, int32_t reps, double* part_ms) {
   });
 }
 
+int pdf_set_sweep_schedule(pdf_handle* h, int32_t chunk, int32_t cut_level, int32_t upper_mode) {
+  if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
+  if (std::find(std::begin(kChunkCandidates), std::end(kChunkCandidates), chunk) == std::end(kChunkCandidates) ||
+      cut_level < 0 || cut_level >= kCutCandidates || (upper_mode != 0 && upper_mode != 1))
+    return fail(h, PDF_INVALID_ARG, "sweep schedule outside chunk {32, 64, 128}, cut level 0-7, mode 0/1");
+  return guarded(h, [&]() -> int {
+    CK(cudaSetDevice(h->prm.device));
+    CK(cudaStreamSynchronize(h->stream));
+    build_schedule(h, chunk, cut_level, upper_mode);
+    const bool mode_ok = h->d.plan.upper_mode == upper_mode;
+    if (!mode_ok) build_schedule(h, chunk, cut_level, 0);
+    DeviceBuffers& d = h->d;
+    if (h->fp32)
+      launch_solve_prep<float>(h->stream, h->dm.N, d.x32, d.y32, d.sync);
+    else
+      launch_solve_prep<double>(h->stream, h->dm.N, d.x64, d.y64, d.sync);
+    // a captured iteration graph holds the old schedule's launch parameters
+    if (h->graph) {
+      CK(cudaGraphExecDestroy(h->graph));
+      h->graph = nullptr;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    if (!mode_ok) return fail(h, PDF_INVALID_ARG, "the scene has more upper levels than the level launch table holds");
+    return PDF_OK;
+  });
+}
+
 int pdf_check_wait_timeout(pdf_handle* h, int32_t max_spins) {
   if (!h || max_spins <= 0) return fail(h, PDF_INVALID_ARG, "invalid wait-timeout check");
   return guarded(h, [&]() -> int {

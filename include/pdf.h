@@ -360,6 +360,17 @@ int pdf_time_phase(pdf_handle* h, int32_t phase, int32_t reps, double* ms,
  * reference; a profiling aid). */
 int pdf_time_solve_parts(pdf_handle* h, int32_t reps, double* part_ms);
 
+/* Replaces the solve schedule the autotuner chose at create (no counterpart
+ * in the reference): work-item width chunk (32, 64 or 128), subtree-block
+ * cut level 0-7, and the mode of the supernodes above the blocks (0 =
+ * dependency-driven work items, 1 = one launch per elimination-tree level).
+ * Every schedule solves the same system; the results agree to rounding.
+ * PDF_INVALID_ARG for values outside these sets, or for mode 1 on a scene
+ * with more upper levels than the launch table holds (stats
+ * sweep_upper_levels). */
+int pdf_set_sweep_schedule(pdf_handle* h, int32_t chunk, int32_t cut_level,
+                           int32_t upper_mode);
+
 /* Check of the bounded device waits (no counterpart in the reference): runs
  * one global solve whose dependency targets lie one solve ahead of the
  * completion counters, on a schedule whose blocks are only the leaves, so
