@@ -4,6 +4,8 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdint>
+#include <stdexcept>
 #include <cmath>
 #include <cstdlib>
 #include <numeric>
@@ -465,6 +467,23 @@ void build_sweep_tasks(const Factor& f, int chunk, std::vector<SweepTask>& fa, s
   for (const auto& t : ba) sn[t.sn].ntb++;
 }
 
+static BlockItem block_item(int64_t off, int roff, int idx0, int c0l, int ns, int nr, int tile, int a0, int a1) {
+  // the eligibility bounds of a block keep these within 16 bits
+  if (c0l < 0 || c0l > INT16_MAX || ns > INT16_MAX || nr > INT16_MAX || tile > INT16_MAX || a1 > INT16_MAX)
+    throw std::runtime_error("block work item field out of range");
+  BlockItem I{};
+  I.off = off;
+  I.roff = roff;
+  I.idx0 = idx0;
+  I.c0l = (int16_t)c0l;
+  I.ns = (int16_t)ns;
+  I.nr = (int16_t)nr;
+  I.tile = (int16_t)tile;
+  I.a0 = (int16_t)a0;
+  I.a1 = (int16_t)a1;
+  return I;
+}
+
 void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan) {
   const int S = f.n_sn;
   plan = SweepPlan{};
@@ -473,11 +492,15 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
   // subtree extents: supernodes are numbered in column order and every
   // parent comes after its children, so one ascending pass accumulates them
   std::vector<int> lo(S), cnt(S, 0), ftiles(S, 0), btiles(S, 0);
+  auto spans = [](int len) { return (len + kBlockSpan - 1) / kBlockSpan; };
   for (int s = 0; s < S; ++s) lo[s] = f.sn_c0[s];
   for (int s = 0; s < S; ++s) {
     cnt[s] += f.sn_ns[s];
-    ftiles[s] += (int)(f.sn_ftile0[s + 1] - f.sn_ftile0[s]);
-    btiles[s] += (int)(f.sn_btile0[s + 1] - f.sn_btile0[s]);
+    // block work items of the supernode (tiles split into kBlockSpan spans)
+    for (int tl = 0; tl < (int)(f.sn_ftile0[s + 1] - f.sn_ftile0[s]); ++tl)
+      ftiles[s] += spans(std::min(f.sn_ns[s], kTile * tl + kTile));
+    for (int tl = 0; tl < (int)(f.sn_btile0[s + 1] - f.sn_btile0[s]); ++tl)
+      btiles[s] += spans(f.sn_ns[s] - kTile * tl + f.sn_nr[s]);
     const int p = f.sn_parent[s];
     if (p >= 0) {
       lo[p] = std::min(lo[p], lo[s]);
@@ -546,9 +569,13 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
     for (int L = 0; L < fb.nlev; ++L) {
       fb.lev[L] = (int)plan.fitem.size() - fb.item0;
       for (int s : by_lev[L])
-        for (int64_t t = f.sn_ftile0[s]; t < f.sn_ftile0[s + 1]; ++t)
-          plan.fitem.push_back({f.ftile_off[t], f.sn_c0[s] - fb.c0, f.sn_ns[s], f.sn_nr[s],
-                                (int)(t - f.sn_ftile0[s]), (int)f.sn_roff[s], 0});
+        for (int64_t t = f.sn_ftile0[s]; t < f.sn_ftile0[s + 1]; ++t) {
+          const int tl = (int)(t - f.sn_ftile0[s]);
+          const int w = std::min(f.sn_ns[s], kTile * tl + kTile);
+          for (int a = 0; a < w; a += kBlockSpan)
+            plan.fitem.push_back(block_item(f.ftile_off[t], (int)f.sn_roff[s], 0, f.sn_c0[s] - fb.c0, f.sn_ns[s],
+                                            f.sn_nr[s], tl, a, std::min(w, a + kBlockSpan)));
+        }
     }
     fb.lev[fb.nlev] = (int)plan.fitem.size() - fb.item0;
     bb.item0 = (int)plan.bitem.size();
@@ -559,8 +586,9 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
         for (int64_t t = f.sn_btile0[s]; t < f.sn_btile0[s + 1]; ++t) {
           const int tl = (int)(t - f.sn_btile0[s]);
           const int c0l = f.sn_c0[s] - bb.c0, j0t = kTile * tl, nd = f.sn_ns[s] - j0t, h = nd + f.sn_nr[s];
-          plan.bitem.push_back({f.btile_off[t], c0l, f.sn_ns[s], f.sn_nr[s], tl, (int)f.sn_roff[s],
-                                (int)plan.bidx.size()});
+          for (int a = 0; a < h; a += kBlockSpan)
+            plan.bitem.push_back(block_item(f.btile_off[t], (int)f.sn_roff[s], (int)plan.bidx.size(), c0l,
+                                            f.sn_ns[s], f.sn_nr[s], tl, a, std::min(h, a + kBlockSpan)));
           for (int i = 0; i < h; ++i)
             plan.bidx.push_back(i < nd ? -1 - (c0l + j0t + i) : plan.rows_loc[f.sn_roff[s] + i - nd]);
           while (plan.bidx.size() % kSlab) plan.bidx.push_back(0);
@@ -665,14 +693,14 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
       for (int it = B.item0 + B.lev[L]; it < B.item0 + B.lev[L + 1]; ++it) {
         if (!chk(it, nfi, "forward block items")) return false;
         const BlockItem& I = plan.fitem[it];
-        const int m = std::min(kTile, I.ns + I.nr - kTile * I.tile), w = std::min(I.ns, kTile * I.tile + kTile);
-        if ((I.off % kTilePad) != 0) {
-          err = "forward tile not aligned";
+        const int m = std::min(kTile, I.ns + I.nr - kTile * I.tile), w = std::min((int)I.ns, kTile * I.tile + (int)kTile);
+        if ((I.off % kTilePad) != 0 || I.a0 % kSlab != 0 || I.a0 < 0 || I.a0 >= I.a1 || I.a1 > w) {
+          err = "forward block item not aligned or out of its tile";
           return false;
         }
         for (int l = 0; l < m; ++l) {
           double acc[3] = {0, 0, 0};
-          for (int j = 0; j < w; ++j) {
+          for (int j = I.a0; j < I.a1; ++j) {
             const int64_t wi = I.off + (int64_t)j * m + l;
             if (!chk(wi, nWf, "forward block tile") || !chk(I.c0l + j, nc, "forward block vector")) return false;
             for (int c = 0; c < 3; ++c) acc[c] += f.Wf[wi] * sv[I.c0l + j + c * ld];
@@ -680,7 +708,7 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
           const int row = kTile * I.tile + l;
           if (row < I.ns) {
             if (!chk(I.c0l + row, nc, "forward block y")) return false;
-            for (int c = 0; c < 3; ++c) y[B.c0 + I.c0l + row + c * n] = acc[c];
+            for (int c = 0; c < 3; ++c) y[B.c0 + I.c0l + row + c * n] += acc[c];
           } else {
             if (!chk(I.roff + row - I.ns, nloc, "forward block rows")) return false;
             const int loc = plan.rows_loc[I.roff + row - I.ns];
@@ -804,13 +832,14 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
         if (!chk(it, nbi, "backward block items")) return false;
         const BlockItem& I = plan.bitem[it];
         const int j0t = kTile * I.tile, nd = I.ns - j0t, mc = std::min(kTile, nd), h = nd + I.nr;
-        if ((I.off % kTilePad) != 0 || (I.idx0 % kSlab) != 0) {
-          err = "backward tile or index list not aligned";
+        if ((I.off % kTilePad) != 0 || (I.idx0 % kSlab) != 0 || I.a0 % kSlab != 0 || I.a0 < 0 || I.a0 >= I.a1 ||
+            I.a1 > h) {
+          err = "backward block item not aligned or out of its tile";
           return false;
         }
         for (int l = 0; l < mc; ++l) {
           double acc[3] = {0, 0, 0};
-          for (int i = 0; i < h; ++i) {
+          for (int i = I.a0; i < I.a1; ++i) {
             const int64_t wi = I.off + (int64_t)i * mc + l;
             if (!chk(wi, nWb, "backward block tile") || !chk(I.idx0 + i, nbidx, "backward block index")) return false;
             const int idx = plan.bidx[I.idx0 + i];
@@ -824,7 +853,7 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
             }
             for (int c = 0; c < 3; ++c) acc[c] += f.Wb[wi] * v[c];
           }
-          for (int c = 0; c < 3; ++c) sx[I.c0l + j0t + l + c * ld] = acc[c];
+          for (int c = 0; c < 3; ++c) sx[I.c0l + j0t + l + c * ld] += acc[c];
         }
       }
     for (int k = 0; k < nc; ++k)

@@ -105,8 +105,13 @@ void build_sweep_tasks(const Factor& f, int chunk, std::vector<SweepTask>& fwd, 
 constexpr int kMaxBlockLevels = 16;
 constexpr int kMaxBlockCols = 1536;
 constexpr int kMaxBlockExt = 1024;
-constexpr int kMaxBlockItems = 768;  // tiles per block and sweep (staged in shared memory)
+constexpr int kMaxBlockItems = 768;  // work items per block and sweep (staged in shared memory)
 constexpr int kSlab = 16;  // columns (forward) / rows (backward) per bulk copy
+// A tile longer than this (forward columns, backward rows) is split into
+// items of this span whose partial sums meet in atomics, so that the long
+// tiles at the top of a block (a backward tile spans the root's ext rows) do
+// not hold one warp while the others wait at the level barrier.
+constexpr int kBlockSpan = 128;  // multiple of kSlab
 
 struct SweepBlock {
   int c0, c1;    // columns [c0, c1) of the subtree
@@ -117,17 +122,24 @@ struct SweepBlock {
   int next;
   int lev[kMaxBlockLevels + 1];  // item offsets (from item0) per level, in sweep order
 };
-// One tile of a supernode inside a block: forward, rows [32 tile, 32 tile + m)
-// of W_s over its w = min(ns, 32 tile + 32) columns; backward, columns
-// [32 tile, 32 tile + mc) over its h = ns - 32 tile + nr rows.
+// One work item of a tile of a supernode inside a block: forward, rows
+// [32 tile, 32 tile + m) of W_s over its columns [a0, a1) of
+// w = min(ns, 32 tile + 32); backward, columns [32 tile, 32 tile + mc) over
+// its rows [a0, a1) of h = ns - 32 tile + nr.  a0 is a multiple of kSlab.
+// The small fields are 16-bit (a block has at most kMaxBlockCols columns and
+// kMaxBlockExt ext rows), so that an item is 32 bytes of shared memory.
 struct BlockItem {
   int64_t off;   // tile offset in the forward (backward) tiled copy
-  int c0l;       // first column of the supernode, relative to the block
-  int ns, nr;
-  int tile;
   int roff;      // offset of the supernode's row set in Factor::rows (and rows_loc)
-  int idx0;      // backward: offset of the tile's row-index list in bidx (multiple of 4)
+  int idx0;      // backward: offset of the tile's row-index list in bidx (multiple of kSlab)
+  int16_t c0l;   // first column of the supernode, relative to the block
+  int16_t ns, nr;
+  int16_t tile;
+  int16_t a0, a1;
+  int16_t pad[2];
 };
+static_assert(sizeof(BlockItem) == 32, "BlockItem is 32 bytes");
+static_assert(kBlockSpan % kSlab == 0, "items start on a slab");
 
 // An upper work item as the device reads it: the SweepTask with the fields
 // of its supernode it needs and its dependency targets per solve, so that one

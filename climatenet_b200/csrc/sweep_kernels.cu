@@ -11,8 +11,9 @@
 //     subtrees with contiguous columns ("blocks"), one CTA per block: the
 //     block's slice of b and its rows outside the block ("ext" rows, the row
 //     set of the block's root) sit in shared memory, the block's levels are
-//     separated by CTA barriers, each tile of each supernode is one warp's
-//     item, and the factor streams in through bulk asynchronous copies
+//     separated by CTA barriers, each tile of each supernode (each span of
+//     kBlockSpan columns / rows of a longer tile, the spans meeting in
+//     atomics) is one warp's item, and the factor streams in through bulk asynchronous copies
 //     (cp.async.bulk, global -> shared, completion on an mbarrier) into a ring
 //     of stages per warp, kept several slabs ahead of the warp's arithmetic
 //     (across level barriers too: the factor does not depend on the data).
@@ -148,14 +149,9 @@ __device__ __forceinline__ int cta_ticket(int* queue, int* slot) {
 // items of level L taken round-robin by warp (item0 + lev[L] + warp, + nw,
 // ...), the slabs of an item in order.  Every lane holds the same cursor.
 struct SlabCursor {
-  int L, it, j0, len;  // len: the current item's columns (forward) / rows (backward)
+  int L, it, j0, len;  // j0: next slab's first column (forward) / row (backward); len: the item's end
   __device__ __forceinline__ bool done(int nlev) const { return L >= nlev; }
 };
-
-template <bool kFwd>
-__device__ __forceinline__ int item_extent(const BlockItem& I) {
-  return kFwd ? min(I.ns, kTile * I.tile + kTile) : I.ns - kTile * I.tile + I.nr;
-}
 
 // items and lev are the block's item descriptors and level offsets staged in
 // shared memory (indices relative to the block's first item)
@@ -166,7 +162,10 @@ __device__ __forceinline__ void cursor_settle(SlabCursor& c, int nlev, const int
     ++c.L;
     if (c.L < nlev) c.it = lev[c.L] + warp;
   }
-  if (c.L < nlev) c.len = item_extent<kFwd>(items[c.it]);
+  if (c.L < nlev) {
+    c.j0 = items[c.it].a0;
+    c.len = items[c.it].a1;
+  }
 }
 
 template <bool kFwd>
@@ -174,7 +173,6 @@ __device__ __forceinline__ void cursor_start(SlabCursor& c, int nlev, const int*
                                              int warp) {
   c.L = 0;
   c.it = lev[0] + warp;
-  c.j0 = 0;
   cursor_settle<kFwd>(c, nlev, lev, items, warp);
 }
 
@@ -183,7 +181,6 @@ __device__ __forceinline__ void cursor_next(SlabCursor& c, int nlev, const int* 
                                             int nw) {
   c.j0 += kSlab;
   if (c.j0 >= c.len) {
-    c.j0 = 0;
     c.it += nw;
     cursor_settle<kFwd>(c, nlev, lev, items, warp);
   }
@@ -304,13 +301,14 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_forward(DPlan P, con
       for (int it = s_lev[L] + warp; it < i1; it += nw) {
         const BlockItem I = items[it];
         const int m = min(kTile, I.ns + I.nr - kTile * I.tile);
-        const int w = min(I.ns, kTile * I.tile + kTile);
+        const int w = min((int)I.ns, kTile * I.tile + kTile);
+        const int a1 = I.a1;
         const int row = kTile * I.tile + lane;
         const int loc = (row >= I.ns && row < I.ns + I.nr) ? P.rows_loc[I.roff + row - I.ns] : -1;
         const T* vx = sv + I.c0l;
         T ax = 0, ay = 0, az = 0;
 #pragma unroll 1
-        for (int j0 = 0; j0 < w; j0 += kSlab) {
+        for (int j0 = I.a0; j0 < a1; j0 += kSlab) {
           const int st = cons % R;
           if (!failed && !mbar_wait_warp(sm.bar + st, (par >> st) & 1u, sy.max_spins)) {
             failed = true;
@@ -320,7 +318,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_forward(DPlan P, con
             // nothing valid in this stage
           } else {
             const T* sp = sm.ring + st * KE;
-            const int cnt = min(kSlab, w - j0);
+            const int cnt = min(kSlab, a1 - j0);
             if (lane < m) {
 #pragma unroll
               for (int u = 0; u < kSlab; ++u)
@@ -350,9 +348,15 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_forward(DPlan P, con
         }
         if (row < I.ns) {
           const int64_t o = (int64_t)c0b + I.c0l + row;
-          y[o] = ax;
-          y[o + n] = ay;
-          y[o + 2 * (int64_t)n] = az;
+          if (I.a0 == 0 && a1 == w) {
+            y[o] = ax;
+            y[o + n] = ay;
+            y[o + 2 * (int64_t)n] = az;
+          } else {  // one span of a split tile (y starts at zero)
+            atomicAdd(y + o, ax);
+            atomicAdd(y + o + n, ay);
+            atomicAdd(y + o + 2 * (int64_t)n, az);
+          }
         } else if (loc >= 0) {
           atomicAdd(sv + loc, -ax);
           atomicAdd(sv + ld + loc, -ay);
@@ -411,6 +415,8 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_backward(DPlan P, co
       sv[ld + nc + e] = x[r + n];
       sv[2 * ld + nc + e] = x[r + 2 * (int64_t)n];
     }
+    // the block's columns start at zero: the spans of a split tile add into them
+    for (int k = threadIdx.x; k < nc; k += blockDim.x) sv[k] = sv[ld + k] = sv[2 * ld + k] = T(0);
     __syncthreads();
     const BlockItem* items = sm.items;
     SlabCursor pc;
@@ -430,15 +436,16 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_backward(DPlan P, co
       for (int it = s_lev[L] + warp; it < i1; it += nw) {
         const BlockItem I = items[it];
         const int j0t = kTile * I.tile, nd = I.ns - j0t, mc = min(kTile, nd), h = nd + I.nr;
+        const int a1 = I.a1;
         T ax = 0, ay = 0, az = 0;
 #pragma unroll 1
-        for (int i0 = 0; i0 < h; i0 += kSlab) {
+        for (int i0 = I.a0; i0 < a1; i0 += kSlab) {
           const int st = cons % R;
           if (!failed && !mbar_wait_warp(sm.bar + st, (par >> st) & 1u, sy.max_spins)) {
             failed = true;
             if (lane == 0) atomicOr(sy.err, 1);
           }
-          const int cnt = min(kSlab, h - i0);
+          const int cnt = min(kSlab, a1 - i0);
           const bool valid = (pending & (1u << st)) && !failed;
           if (lane < kSlab) {
             T vx = 0, vy = 0, vz = 0;
@@ -489,9 +496,15 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_backward(DPlan P, co
         }
         if (lane < mc) {
           T* s = sv + I.c0l + j0t + lane;
-          s[0] = ax;
-          s[ld] = ay;
-          s[2 * ld] = az;
+          if (I.a0 == 0 && a1 == h) {
+            s[0] = ax;
+            s[ld] = ay;
+            s[2 * ld] = az;
+          } else {  // one span of a split tile
+            atomicAdd(s, ax);
+            atomicAdd(s + ld, ay);
+            atomicAdd(s + 2 * ld, az);
+          }
         }
       }
       __syncthreads();
