@@ -64,6 +64,7 @@ constexpr int kCutLevel = 4;  // host emulation check (pdf_factor_check)
 constexpr int kRecords = 64;  // step records in flight before the oldest is harvested
 constexpr int kChunkCandidates[3] = {32, 64, 128};
 constexpr int kCutCandidates = 8;  // cut levels 0 .. 7
+constexpr int kBlockShape = 1;     // block kernels: 2 CTAs of 8 warps per SM
 // polls of a dependency counter before a sweep gives up (each poll sleeps
 // about 32 ns): far above any legitimate wait
 constexpr int kMaxSpins = 1 << 22;
@@ -89,7 +90,7 @@ void free_plan(DPlan& P) {
 
 // Sweep plan (subtree blocks + upper work items, factor.hpp) on the device.
 // The completion counters are cumulative per schedule, so they restart here.
-void build_schedule(pdf_handle* h, int chunk, int cut_level, int upper_mode = 0) {
+void build_schedule(pdf_handle* h, int chunk, int cut_level, int upper_mode = 0, int shape = kBlockShape) {
   const Factor& f = h->fac;
   SweepPlan& hp = h->d.host_plan;
   build_sweep_plan(f, chunk, cut_level, hp);
@@ -126,12 +127,20 @@ void build_schedule(pdf_handle* h, int chunk, int cut_level, int upper_mode = 0)
     P.flev[k] = levels_fit && k <= P.n_flev ? hp.fup_lev[k] : 0;
     P.blev[k] = levels_fit && k <= P.n_blev ? hp.bup_lev[k] : 0;
   }
-  const bool fits = h->fp32 ? configure_solve<float>(P) : configure_solve<double>(P);
-  if (!fits) throw CudaFail("the sweep's block kernels do not fit the device's shared memory");
+  // the requested launch shape of the block kernels, else one CTA of 8 warps
+  // per SM (P.block_shape tells which)
+  auto configure = [&](int sh) { return h->fp32 ? configure_solve<float>(P, sh) : configure_solve<double>(P, sh); };
+  if (!configure(shape) && !configure(0))
+    throw CudaFail("the sweep's block kernels do not fit the device's shared memory");
   h->n_levels = f.n_levels;
   h->stats.sweep_chunk = chunk;
   h->stats.sweep_cut_level = cut_level;
   h->stats.sweep_upper_mode = P.upper_mode;
+  h->stats.sweep_block_shape = P.block_shape;
+  h->stats.sweep_block_warps = P.block_warps;
+  h->stats.sweep_block_ctas = P.block_ctas;
+  h->stats.sweep_ring_stages[0] = P.ring_f;
+  h->stats.sweep_ring_stages[1] = P.ring_b;
   h->stats.sweep_upper_levels = P.n_flev;
   h->stats.sweep_blocks = P.nblk;
   h->stats.sweep_block_elems = hp.block_elems;
@@ -557,9 +566,10 @@ void launch_solve_with(pdf_handle* h, const SweepSync& sy, T* b, T* y, T* x, con
 }
 
 // Schedule autotuner: times the global solve of this scene's factor with
-// each candidate cut level and both upper modes (work-item width 64), then
-// with each work-item width at the best cut level and mode, and keeps the
-// fastest.  The right-hand side is
+// each candidate cut level and both upper modes (work-item width 64, block
+// kernels at 2 CTAs of 8 warps per SM where they fit), then with each launch
+// shape of the block kernels at the best cut level and mode, then with each
+// work-item width, and keeps the fastest.  The right-hand side is
 // zero (the sweeps read the same data and wait on the same dependencies
 // whatever the values); v and q^k, which the solve writes, are restored.
 void autotune_schedule(pdf_handle* h) {
@@ -569,9 +579,11 @@ void autotune_schedule(pdf_handle* h) {
   std::vector<double> vsave(3 * (size_t)N), qsave(3 * (size_t)N);
   CK(cudaMemcpy(vsave.data(), d.v, vsave.size() * sizeof(double), cudaMemcpyDeviceToHost));
   CK(cudaMemcpy(qsave.data(), d.qk, qsave.size() * sizeof(double), cudaMemcpyDeviceToHost));
-  auto time_plan = [&](int chunk, int cut, int mode) {
-    build_schedule(h, chunk, cut, mode);
-    if (h->d.plan.upper_mode != mode) return 0.;
+  // 0 when the schedule built is not the one asked for (upper levels beyond
+  // the launch table, or a block shape that does not fit)
+  auto time_plan = [&](int chunk, int cut, int mode, int shape, bool exact_shape) {
+    build_schedule(h, chunk, cut, mode, shape);
+    if (h->d.plan.upper_mode != mode || (exact_shape && h->d.plan.block_shape != shape)) return 0.;
     double total = 0.;
     for (int r = 0; r < 4; ++r) {
       if (h->fp32) {
@@ -598,12 +610,14 @@ void autotune_schedule(pdf_handle* h) {
     return total / 3.;
   };
   double best = 1e300;
-  int best_cut = kCutLevel, best_chunk = kChunk, best_mode = 0;
+  int best_cut = kCutLevel, best_chunk = kChunk, best_mode = 0, best_shape = kBlockShape;
   double cut_ms[2][kCutCandidates] = {};
+  int cut_shape[2][kCutCandidates] = {};
   for (int cut = 0; cut < kCutCandidates; ++cut)
     for (int mode = 0; mode < 2; ++mode) {
-      const double ms = time_plan(kChunk, cut, mode);
+      const double ms = time_plan(kChunk, cut, mode, kBlockShape, false);
       cut_ms[mode][cut] = ms;
+      cut_shape[mode][cut] = h->d.plan.block_shape;
       if (ms > 0. && ms < best) {
         best = ms;
         best_cut = cut;
@@ -614,17 +628,28 @@ void autotune_schedule(pdf_handle* h) {
     h->stats.sweep_cut_ms[cut] = cut_ms[0][cut];
     h->stats.sweep_cut_level_ms[cut] = cut_ms[1][cut];
   }
+  // the block kernels' launch shapes at the best cut level and mode
+  best_shape = cut_shape[best_mode][best_cut];
+  for (int sh = 0; sh < kBlockShapes; ++sh) {
+    const double ms = sh == best_shape ? best : time_plan(kChunk, best_cut, best_mode, sh, true);
+    h->stats.sweep_shape_ms[sh] = ms;
+    if (ms > 0. && ms < best) {
+      best = ms;
+      best_shape = sh;
+    }
+  }
   const double best_default_chunk = best;
   for (int ci = 0; ci < 3; ++ci) {
     const int chunk = kChunkCandidates[ci];
-    const double ms = chunk == kChunk ? best_default_chunk : time_plan(chunk, best_cut, best_mode);
+    const double ms =
+        chunk == kChunk ? best_default_chunk : time_plan(chunk, best_cut, best_mode, best_shape, true);
     h->stats.sweep_chunk_ms[ci] = ms;
-    if (ms < best) {
+    if (ms > 0. && ms < best) {
       best = ms;
       best_chunk = chunk;
     }
   }
-  build_schedule(h, best_chunk, best_cut, best_mode);
+  build_schedule(h, best_chunk, best_cut, best_mode, best_shape);
   if (h->fp32)
     launch_solve_prep<float>(st, N, d.x32, d.y32, d.sync);
   else
@@ -1585,17 +1610,20 @@ int pdf_time_solve_parts(pdf_handle* h, int32_t reps, double* part_ms) {
   });
 }
 
-int pdf_set_sweep_schedule(pdf_handle* h, int32_t chunk, int32_t cut_level, int32_t upper_mode) {
+int pdf_set_sweep_schedule(pdf_handle* h, int32_t chunk, int32_t cut_level, int32_t upper_mode,
+                           int32_t block_shape) {
   if (!h) return fail(h, PDF_INVALID_ARG, "null handle");
   if (std::find(std::begin(kChunkCandidates), std::end(kChunkCandidates), chunk) == std::end(kChunkCandidates) ||
-      cut_level < 0 || cut_level >= kCutCandidates || (upper_mode != 0 && upper_mode != 1))
-    return fail(h, PDF_INVALID_ARG, "sweep schedule outside chunk {32, 64, 128}, cut level 0-7, mode 0/1");
+      cut_level < 0 || cut_level >= kCutCandidates || (upper_mode != 0 && upper_mode != 1) || block_shape < 0 ||
+      block_shape >= kBlockShapes)
+    return fail(h, PDF_INVALID_ARG,
+                "sweep schedule outside chunk {32, 64, 128}, cut level 0-7, mode 0/1, block shape 0-3");
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->prm.device));
     CK(cudaStreamSynchronize(h->stream));
-    build_schedule(h, chunk, cut_level, upper_mode);
-    const bool mode_ok = h->d.plan.upper_mode == upper_mode;
-    if (!mode_ok) build_schedule(h, chunk, cut_level, 0);
+    build_schedule(h, chunk, cut_level, upper_mode, block_shape);
+    const bool mode_ok = h->d.plan.upper_mode == upper_mode && h->d.plan.block_shape == block_shape;
+    if (!mode_ok) build_schedule(h, chunk, cut_level, 0, 0);
     DeviceBuffers& d = h->d;
     if (h->fp32)
       launch_solve_prep<float>(h->stream, h->dm.N, d.x32, d.y32, d.sync);
@@ -1607,7 +1635,10 @@ int pdf_set_sweep_schedule(pdf_handle* h, int32_t chunk, int32_t cut_level, int3
       h->graph = nullptr;
     }
     CK(cudaStreamSynchronize(h->stream));
-    if (!mode_ok) return fail(h, PDF_INVALID_ARG, "the scene has more upper levels than the level launch table holds");
+    if (!mode_ok)
+      return fail(h, PDF_INVALID_ARG,
+                  "the scene has more upper levels than the level launch table holds, or its blocks do not fit "
+                  "the launch shape");
     return PDF_OK;
   });
 }

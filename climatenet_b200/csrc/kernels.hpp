@@ -23,6 +23,12 @@ struct SweepSync {
 
 constexpr int kMaxUpperLevels = 32;
 
+// Launch shapes of the block kernels: warps per CTA and CTAs per SM (the
+// ring of bulk-copy stages shrinks to fit); the schedule autotuner picks one.
+constexpr int kBlockShapes = 4;
+constexpr int kBlockShapeWarps[kBlockShapes] = {8, 8, 4, 4};
+constexpr int kBlockShapeCtas[kBlockShapes] = {1, 2, 3, 4};
+
 // Device view of a SweepPlan (factor.hpp) and its launch shape.
 struct DPlan {
   const UpperItem* fup;
@@ -46,6 +52,9 @@ struct DPlan {
   int max_items;        // most tiles of a block in one sweep
   int smem_f, smem_b;   // dynamic shared memory of the forward / backward block kernels
   int grid_bf, grid_bb, grid_uf, grid_ub;
+  // launch shape of the block kernels (kBlockShapes): warps per CTA, CTAs
+  // per SM it was sized for, and bulk-copy stages per warp (forward, backward)
+  int block_shape, block_warps, block_ctas, ring_f, ring_b;
   // upper supernodes: 0 = dependency-driven items in one launch per sweep,
   // 1 = one launch per elimination-tree level (no waits; the launch boundary
   // orders the levels), with the level boundaries of fup / bup
@@ -159,7 +168,7 @@ void launch_friction_self(dim3 grid, dim3 block, cudaStream_t st, DModel m, DCon
 // forward sweep, the backward sweep (with the blocks' write-back) and the
 // write-back of the upper columns.
 template <typename T>
-bool configure_solve(DPlan& P);  // shared memory and grids; false if a block kernel does not fit
+bool configure_solve(DPlan& P, int shape);  // shared memory and grids; false if the shape does not fit
 template <typename T>
 void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
                          SweepSync sy, WriteBack wb, cudaEvent_t* marks = nullptr);

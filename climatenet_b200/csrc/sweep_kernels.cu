@@ -48,12 +48,15 @@ constexpr int kTicketBatch = 2;
 constexpr int kSweepThreads = 256;
 
 // Bulk-copy stages per warp: one slab (32 rows x kSlab columns, or kSlab rows
-// x 32 columns) each, 12 KB per warp in both precisions.
+// x 32 columns) each.  kDeep stages (12 KB per warp in both precisions) when
+// one CTA of 8 warps holds the SM; fewer when the launch shape packs several
+// CTAs per SM (DPlan::ring_f / ring_b, at least kMinRing).
 template <typename T>
 struct Stages {
-  static constexpr int R = sizeof(T) == 8 ? 3 : 6;
+  static constexpr int kDeep = sizeof(T) == 8 ? 3 : 6;
   static constexpr int kElems = kTile * kSlab;
 };
+constexpr int kMinRing = 2;
 
 __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long* p) {
   return *reinterpret_cast<const volatile unsigned long long*>(p);
@@ -218,8 +221,9 @@ struct BlockSmem {
 };
 
 template <typename T, bool kFwd>
-__device__ __forceinline__ BlockSmem<T> block_smem(unsigned char* base, int nw, int warp, int max_ld, int max_cols) {
-  constexpr int R = Stages<T>::R, KE = Stages<T>::kElems;
+__device__ __forceinline__ BlockSmem<T> block_smem(unsigned char* base, int nw, int warp, int max_ld, int max_cols,
+                                                   int R) {
+  constexpr int KE = Stages<T>::kElems;
   BlockSmem<T> s;
   size_t off = 0;
   s.ring = reinterpret_cast<T*>(base) + (size_t)warp * R * KE;
@@ -239,8 +243,8 @@ __device__ __forceinline__ BlockSmem<T> block_smem(unsigned char* base, int nw, 
 }
 
 template <typename T, bool kFwd>
-size_t block_smem_bytes(int nw, int max_ld, int max_cols, int max_items) {
-  constexpr int R = Stages<T>::R, KE = Stages<T>::kElems;
+size_t block_smem_bytes(int nw, int max_ld, int max_cols, int max_items, int R) {
+  constexpr int KE = Stages<T>::kElems;
   size_t b = (size_t)nw * R * KE * sizeof(T) + (size_t)nw * R * sizeof(uint64_t) + 3 * (size_t)max_ld * sizeof(T);
   if (!kFwd) b += (size_t)nw * R * kSlab * sizeof(int) + 3 * (size_t)max_cols * sizeof(T) + (size_t)nw * 3 * kSlab * sizeof(T);
   return ((b + 15) & ~size_t(15)) + (size_t)max_items * sizeof(BlockItem);
@@ -254,14 +258,15 @@ __device__ __forceinline__ void drain_stages(uint64_t* bar, uint32_t pending, ui
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kSweepThreads, 1) k_block_forward(DPlan P, const T* __restrict__ W, T* b, T* y,
+__global__ void __launch_bounds__(kSweepThreads, 2) k_block_forward(DPlan P, const T* __restrict__ W, T* b, T* y,
                                                                     int n, SweepSync sy) {
   trace_stamp(sy.trace, DTrace::kSolve);
-  constexpr int R = Stages<T>::R, KE = Stages<T>::kElems;
+  constexpr int KE = Stages<T>::kElems;
+  const int R = P.ring_f;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int s_ticket;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const BlockSmem<T> sm = block_smem<T, true>(smem_raw, nw, warp, P.max_cols + P.max_ext, P.max_cols);
+  const BlockSmem<T> sm = block_smem<T, true>(smem_raw, nw, warp, P.max_cols + P.max_ext, P.max_cols, R);
   __shared__ int s_lev[kMaxBlockLevels + 1];
   if (lane == 0)
     for (int k = 0; k < R; ++k) mbar_init(sm.bar + k, 1);
@@ -377,14 +382,15 @@ __global__ void __launch_bounds__(kSweepThreads, 1) k_block_forward(DPlan P, con
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kSweepThreads, 1) k_block_backward(DPlan P, const T* __restrict__ W,
+__global__ void __launch_bounds__(kSweepThreads, 2) k_block_backward(DPlan P, const T* __restrict__ W,
                                                                      const T* __restrict__ y, const T* x, int n,
                                                                      SweepSync sy, WriteBack wb) {
-  constexpr int R = Stages<T>::R, KE = Stages<T>::kElems;
+  constexpr int KE = Stages<T>::kElems;
+  const int R = P.ring_b;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int s_ticket;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const BlockSmem<T> sm = block_smem<T, false>(smem_raw, nw, warp, P.max_cols + P.max_ext, P.max_cols);
+  const BlockSmem<T> sm = block_smem<T, false>(smem_raw, nw, warp, P.max_cols + P.max_ext, P.max_cols, R);
   __shared__ int s_lev[kMaxBlockLevels + 1];
   if (lane == 0)
     for (int k = 0; k < R; ++k) mbar_init(sm.bar + k, 1);
@@ -802,7 +808,7 @@ __global__ void k_solve_prep(int n, T* x, T* y, SweepSync sy) {
 // Persistent grid: as many CTAs as can be resident at once with this dynamic
 // shared memory (0 when the kernel does not fit).
 template <typename K>
-int resident_ctas(K kernel, size_t smem) {
+int resident_ctas(K kernel, size_t smem, int threads = kSweepThreads) {
   int dev = 0, sms = 148, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -810,18 +816,40 @@ int resident_ctas(K kernel, size_t smem) {
     cudaGetLastError();
     return 0;
   }
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kSweepThreads, smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
   return per_sm * sms;
 }
 
-template <typename T>
-bool configure_solve(DPlan& P) {
-  const int nw = kSweepThreads / 32;
+// The deepest ring (kMinRing .. kDeep stages per warp) with which `ctas`
+// CTAs of `warps` warps of this block kernel are resident per SM; 0 if none.
+template <typename T, bool kFwd, typename K>
+int ring_for(K kernel, const DPlan& P, int warps, int ctas, int* smem) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int max_ld = std::max(1, P.max_cols + P.max_ext);
-  P.smem_f = (int)block_smem_bytes<T, true>(nw, max_ld, std::max(1, P.max_cols), std::max(1, P.max_items));
-  P.smem_b = (int)block_smem_bytes<T, false>(nw, max_ld, std::max(1, P.max_cols), std::max(1, P.max_items));
-  const int rf = resident_ctas(k_block_forward<T>, P.smem_f);
-  const int rb = resident_ctas(k_block_backward<T>, P.smem_b);
+  for (int R = Stages<T>::kDeep; R >= kMinRing; --R) {
+    const size_t b = block_smem_bytes<T, kFwd>(warps, max_ld, std::max(1, P.max_cols), std::max(1, P.max_items), R);
+    if (resident_ctas(kernel, b, 32 * warps) >= ctas * sms) {
+      *smem = (int)b;
+      return R;
+    }
+  }
+  return 0;
+}
+
+template <typename T>
+bool configure_solve(DPlan& P, int shape) {
+  if (shape < 0 || shape >= kBlockShapes) return false;
+  const int warps = kBlockShapeWarps[shape], ctas = kBlockShapeCtas[shape];
+  P.block_shape = shape;
+  P.block_warps = warps;
+  P.block_ctas = ctas;
+  P.ring_f = ring_for<T, true>(k_block_forward<T>, P, warps, ctas, &P.smem_f);
+  P.ring_b = ring_for<T, false>(k_block_backward<T>, P, warps, ctas, &P.smem_b);
+  if (!P.ring_f || !P.ring_b) return false;
+  const int rf = resident_ctas(k_block_forward<T>, P.smem_f, 32 * warps);
+  const int rb = resident_ctas(k_block_backward<T>, P.smem_b, 32 * warps);
   P.grid_bf = std::max(1, std::min(rf, std::max(1, P.nblk)));
   P.grid_bb = std::max(1, std::min(rb, std::max(1, P.nblk)));
   P.grid_uf = std::max(1, resident_ctas(k_upper_forward<T>, 0));
@@ -836,7 +864,7 @@ template <typename T>
 void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
                          SweepSync sy, WriteBack wb, cudaEvent_t* marks) {
   // marks (optional): 4 events recorded between the five launches
-  k_block_forward<T><<<P.grid_bf, kSweepThreads, P.smem_f, st>>>(P, Wf, b, y, n, sy);
+  k_block_forward<T><<<P.grid_bf, 32 * P.block_warps, P.smem_f, st>>>(P, Wf, b, y, n, sy);
   if (marks) cudaEventRecord(marks[0], st);
   if (P.upper_mode == 1) {
     const int wpc = kSweepThreads / 32;
@@ -860,7 +888,7 @@ void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* 
     k_upper_backward<T><<<P.grid_ub, kSweepThreads, 0, st>>>(P, Wb, y, x, n, sy);
   }
   if (marks) cudaEventRecord(marks[2], st);
-  k_block_backward<T><<<P.grid_bb, kSweepThreads, P.smem_b, st>>>(P, Wb, y, x, n, sy, wb);
+  k_block_backward<T><<<P.grid_bb, 32 * P.block_warps, P.smem_b, st>>>(P, Wb, y, x, n, sy, wb);
   if (marks) cudaEventRecord(marks[3], st);
   k_solve_post<T><<<std::max(1, std::min(148 * 4, (P.n_upper + 255) / 256)), 256, 0, st>>>(P, x, y, n, wb, sy);
 }
@@ -869,8 +897,8 @@ void launch_solve_prep(cudaStream_t st, int n, T* x, T* y, SweepSync sy) {
   k_solve_prep<T><<<std::min(148 * 4, (3 * n + 255) / 256), 256, 0, st>>>(n, x, y, sy);
 }
 
-template bool configure_solve<double>(DPlan&);
-template bool configure_solve<float>(DPlan&);
+template bool configure_solve<double>(DPlan&, int);
+template bool configure_solve<float>(DPlan&, int);
 template void launch_solve_sweeps<double>(cudaStream_t, const DPlan&, const double*, const double*, double*, double*,
                                           double*, int, SweepSync, WriteBack, cudaEvent_t*);
 template void launch_solve_sweeps<float>(cudaStream_t, const DPlan&, const float*, const float*, float*, float*,

@@ -55,7 +55,7 @@ def lib():
     L.pdf_get_residual_history.argtypes = [vp, vp, i32, C.POINTER(i32)]
     L.pdf_time_phase.argtypes = [vp, i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.pdf_check_wait_timeout.argtypes = [vp, i32]
-    L.pdf_set_sweep_schedule.argtypes = [vp, i32, i32, i32]
+    L.pdf_set_sweep_schedule.argtypes = [vp, i32, i32, i32, i32]
     L.pdf_time_solve_parts.argtypes = [vp, i32, C.POINTER(C.c_double)]
     L.pdf_factor_check.argtypes = [C.POINTER(abi.pdf_scene_desc), C.POINTER(abi.pdf_params), vp, vp]
     L.pdf_detect_candidates_noalloc.argtypes = [vp, i32, vp, i32, C.c_double, vp, i32, C.POINTER(i32), vp]
@@ -211,10 +211,11 @@ class Simulation:
 
     exportStats = export_stats
 
-    def set_sweep_schedule(self, chunk, cut_level, upper_mode):
+    def set_sweep_schedule(self, chunk, cut_level, upper_mode, block_shape=1):
         """Pin the solve schedule (work-item width, subtree-block cut level,
-        upper mode 0 = dependency-driven items / 1 = level launches)."""
-        _check(lib().pdf_set_sweep_schedule(self.h, chunk, cut_level, upper_mode), self.h)
+        upper mode 0 = dependency-driven items / 1 = level launches, block
+        kernel launch shape 0-3)."""
+        _check(lib().pdf_set_sweep_schedule(self.h, chunk, cut_level, upper_mode, block_shape), self.h)
 
     def time_solve_parts(self, reps=10):
         """Device ms of the five launches of one solve: block forward, upper

@@ -4,10 +4,11 @@ The global solve (SimulationSpeed::solve, the reference's sparse Cholesky
 back-substitution) runs on the device under a schedule the autotuner picks at
 create: work-item width, subtree-block cut level, and the mode of the
 supernodes above the blocks (dependency-driven work items in one launch, or
-one launch per elimination-tree level).  Every schedule must give the
-oracle's trajectory: 1e-6 relative on positions and speeds over 4 steps with
-contacts (the schedules differ only in the order of FP64
-additions), and identical contact counts.  Pinning a schedule after steps
+one launch per elimination-tree level), and the launch shape of the block
+kernels (warps per CTA, CTAs per SM, bulk-copy ring depth).  Every schedule
+must give the oracle's trajectory: 1e-6 relative on positions and speeds
+over 4 steps with contacts (the schedules differ only in
+the order of FP64 additions), and identical contact counts.  Pinning a schedule after steps
 were taken under a captured CUDA graph must replace the graph's launches.
 """
 import numpy as np
@@ -44,14 +45,14 @@ def oracle_run():
 
 
 @pytest.mark.parametrize("precision", [abi.PDF_FP64, abi.PDF_FP32_REFINE])
-@pytest.mark.parametrize("chunk,cut,mode", [(64, 0, 0), (64, 0, 1), (32, 3, 0), (32, 3, 1),
-                                            (128, 5, 1), (64, 7, 0), (64, 7, 1)])
-def test_schedule_matches_oracle(oracle_run, chunk, cut, mode, precision):
+@pytest.mark.parametrize("chunk,cut,mode,shape", [(64, 0, 0, 1), (64, 0, 1, 3), (32, 3, 0, 2), (32, 3, 1, 1),
+                                                  (128, 5, 1, 0), (64, 7, 0, 1), (64, 7, 1, 0), (64, 7, 1, 3)])
+def test_schedule_matches_oracle(oracle_run, chunk, cut, mode, shape, precision):
     s, traj, counts = oracle_run
     g = native.Simulation(s, abi.params(time_step=5e-3, iterations=20, precision=precision))
-    g.set_sweep_schedule(chunk, cut, mode)
+    g.set_sweep_schedule(chunk, cut, mode, shape)
     st = g.stats()
-    assert (st.sweep_chunk, st.sweep_cut_level, st.sweep_upper_mode) == (chunk, cut, mode)
+    assert (st.sweep_chunk, st.sweep_cut_level, st.sweep_upper_mode, st.sweep_block_shape) == (chunk, cut, mode, shape)
     for k in range(4):
         r = g.step(1)
         assert r.n_contacts == counts[k]
@@ -63,9 +64,9 @@ def test_schedule_matches_oracle(oracle_run, chunk, cut, mode, precision):
 def test_schedule_change_replaces_captured_graph(oracle_run):
     s, traj, counts = oracle_run
     g = native.Simulation(s, abi.params(time_step=5e-3, iterations=20, use_graph=1))
-    g.set_sweep_schedule(64, 2, 0)
+    g.set_sweep_schedule(64, 2, 0, 0)
     g.step(2)
-    g.set_sweep_schedule(32, 4, 1)
+    g.set_sweep_schedule(32, 4, 1, 3)
     g.step(2)
     q, v = g.state()
     assert rel_err(q, traj[3][0]) < REL and rel_err(v, traj[3][1]) < REL
@@ -75,7 +76,7 @@ def test_schedule_change_replaces_captured_graph(oracle_run):
 def test_schedule_rejects_values_outside_the_tuned_sets(oracle_run):
     s, _, _ = oracle_run
     g = native.Simulation(s, abi.params(time_step=5e-3, iterations=20))
-    for args in ((48, 0, 0), (64, 8, 0), (64, -1, 0), (64, 0, 2)):
+    for args in ((48, 0, 0, 1), (64, 8, 0, 1), (64, -1, 0, 1), (64, 0, 2, 1), (64, 0, 0, 4), (64, 0, 0, -1)):
         with pytest.raises(native.PdfError):
             g.set_sweep_schedule(*args)
     g.close()
