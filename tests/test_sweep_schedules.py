@@ -66,7 +66,7 @@ def test_schedule_change_replaces_captured_graph(oracle_run):
     g = native.Simulation(s, abi.params(time_step=5e-3, iterations=20, use_graph=1))
     g.set_sweep_schedule(64, 2, 0, 0)
     g.step(2)
-    g.set_sweep_schedule(32, 4, 1, 3)
+    g.set_sweep_schedule(32, 2, 1, 3)
     g.step(2)
     q, v = g.state()
     assert rel_err(q, traj[3][0]) < REL and rel_err(v, traj[3][1]) < REL
