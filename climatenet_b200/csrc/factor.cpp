@@ -492,15 +492,15 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
   // subtree extents: supernodes are numbered in column order and every
   // parent comes after its children, so one ascending pass accumulates them
   std::vector<int> lo(S), cnt(S, 0), ftiles(S, 0), btiles(S, 0);
-  auto spans = [](int len) { return (len + kBlockSpan - 1) / kBlockSpan; };
+  auto spans = [](int len, int span) { return (len + span - 1) / span; };
   for (int s = 0; s < S; ++s) lo[s] = f.sn_c0[s];
   for (int s = 0; s < S; ++s) {
     cnt[s] += f.sn_ns[s];
-    // block work items of the supernode (tiles split into kBlockSpan spans)
+    // block work items of the supernode (tiles split into spans)
     for (int tl = 0; tl < (int)(f.sn_ftile0[s + 1] - f.sn_ftile0[s]); ++tl)
-      ftiles[s] += spans(std::min(f.sn_ns[s], kTile * tl + kTile));
+      ftiles[s] += spans(std::min(f.sn_ns[s], kTile * tl + kTile), kBlockSpanF);
     for (int tl = 0; tl < (int)(f.sn_btile0[s + 1] - f.sn_btile0[s]); ++tl)
-      btiles[s] += spans(f.sn_ns[s] - kTile * tl + f.sn_nr[s]);
+      btiles[s] += spans(f.sn_ns[s] - kTile * tl + f.sn_nr[s], kBlockSpanB);
     const int p = f.sn_parent[s];
     if (p >= 0) {
       lo[p] = std::min(lo[p], lo[s]);
@@ -572,9 +572,9 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
         for (int64_t t = f.sn_ftile0[s]; t < f.sn_ftile0[s + 1]; ++t) {
           const int tl = (int)(t - f.sn_ftile0[s]);
           const int w = std::min(f.sn_ns[s], kTile * tl + kTile);
-          for (int a = 0; a < w; a += kBlockSpan)
+          for (int a = 0; a < w; a += kBlockSpanF)
             plan.fitem.push_back(block_item(f.ftile_off[t], (int)f.sn_roff[s], 0, f.sn_c0[s] - fb.c0, f.sn_ns[s],
-                                            f.sn_nr[s], tl, a, std::min(w, a + kBlockSpan)));
+                                            f.sn_nr[s], tl, a, std::min(w, a + kBlockSpanF)));
         }
     }
     fb.lev[fb.nlev] = (int)plan.fitem.size() - fb.item0;
@@ -586,9 +586,9 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
         for (int64_t t = f.sn_btile0[s]; t < f.sn_btile0[s + 1]; ++t) {
           const int tl = (int)(t - f.sn_btile0[s]);
           const int c0l = f.sn_c0[s] - bb.c0, j0t = kTile * tl, nd = f.sn_ns[s] - j0t, h = nd + f.sn_nr[s];
-          for (int a = 0; a < h; a += kBlockSpan)
+          for (int a = 0; a < h; a += kBlockSpanB)
             plan.bitem.push_back(block_item(f.btile_off[t], (int)f.sn_roff[s], (int)plan.bidx.size(), c0l,
-                                            f.sn_ns[s], f.sn_nr[s], tl, a, std::min(h, a + kBlockSpan)));
+                                            f.sn_ns[s], f.sn_nr[s], tl, a, std::min(h, a + kBlockSpanB)));
           for (int i = 0; i < h; ++i)
             plan.bidx.push_back(i < nd ? -1 - (c0l + j0t + i) : plan.rows_loc[f.sn_roff[s] + i - nd]);
           while (plan.bidx.size() % kSlab) plan.bidx.push_back(0);

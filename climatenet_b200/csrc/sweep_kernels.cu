@@ -12,8 +12,8 @@
 //     block's slice of b and its rows outside the block ("ext" rows, the row
 //     set of the block's root) sit in shared memory, the block's levels are
 //     separated by CTA barriers, each tile of each supernode (each span of
-//     kBlockSpan columns / rows of a longer tile, the spans meeting in
-//     atomics) is one warp's item, and the factor streams in through bulk asynchronous copies
+//     kBlockSpanF columns / kBlockSpanB rows of a longer tile, the spans
+//     meeting in atomics) is one warp's item, and the factor streams in through bulk asynchronous copies
 //     (cp.async.bulk, global -> shared, completion on an mbarrier) into a ring
 //     of stages per warp, kept several slabs ahead of the warp's arithmetic
 //     (across level barriers too: the factor does not depend on the data).
@@ -435,7 +435,6 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_block_backward(DPlan P, co
       ++prod;
       cursor_next<false>(pc, nlev, s_lev, items, warp, nw);
     }
-    __syncthreads();
     for (int L = 0; L < nlev; ++L) {
       const int i1 = s_lev[L + 1];
 #pragma unroll 1
