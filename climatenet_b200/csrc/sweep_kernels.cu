@@ -776,18 +776,30 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P,
 // and their y is overwritten by the next forward sweep); one thread rewinds
 // the work queues and advances the solve counter.
 template <typename T>
-__global__ void k_solve_post(DPlan P, T* x, T* y, int n, WriteBack wb, SweepSync sy) {
+__global__ void k_solve_post(DPlan P, T* __restrict__ x, T* __restrict__ y, int n, WriteBack wb, SweepSync sy) {
+  double* __restrict__ v = wb.v;
+  double* __restrict__ qk = wb.qk;
+  const double* __restrict__ q = wb.q;
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < P.n_upper; k += gridDim.x * blockDim.x) {
     const int col = P.upper_cols[k];
     const int64_t vtx = P.perm[col];
+    // every load before the first store (the arrays do not alias)
+    double val[3], qv[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      val[c] = (double)x[col + (int64_t)c * n];
+      qv[c] = q[3 * vtx + c];
+    }
+    if (wb.mode == 1)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) val[c] += v[3 * vtx + c];
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
       const int64_t o = col + (int64_t)c * n;
-      double val = (double)x[o];
       x[o] = 0;
       y[o] = 0;
-      if (wb.mode == 1) val += wb.v[3 * vtx + c];
-      wb.v[3 * vtx + c] = val;
-      wb.qk[3 * vtx + c] = wb.q[3 * vtx + c] + wb.dt * val;
+      v[3 * vtx + c] = val[c];
+      qk[3 * vtx + c] = qv[c] + wb.dt * val[c];
     }
   }
   if (blockIdx.x == 0 && threadIdx.x < 4) sy.queue[threadIdx.x] = 0;
