@@ -146,6 +146,38 @@ __device__ __forceinline__ int cta_ticket(int* queue, int* slot) {
   return *slot;
 }
 
+// L2 prefetch of [p, p + bytes), shrunk to 16-byte boundaries (a hint: no
+// completion to wait for, nothing lands in shared memory)
+__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uintptr_t s = (a + 15) & ~uintptr_t(15);
+  const uintptr_t e = (a + bytes) & ~uintptr_t(15);
+  if (e > s) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(s), "r"((uint32_t)(e - s)) : "memory");
+}
+
+// Lane j of a warp prefetches into L2 the factor of the warp's j-th item
+// among items[first + j * stride] (< hi): its tile rows (forward) or
+// columns (backward) over [a0, a1), contiguous in the tiled copy.
+template <typename T>
+__device__ __forceinline__ void prefetch_items(const UpperItem* items, bool fwd, int first, int hi, int stride,
+                                               const T* W, int lane) {
+  const int t = first + lane * stride;
+  if (first < hi && t < hi) {
+    const UpperItem tk = items[t];
+    const int m = fwd ? min(kTile, tk.ns + tk.nr - tk.tile * kTile) : min(kTile, tk.ns - tk.tile * kTile);
+    prefetch_l2(W + tk.off + (int64_t)tk.a0 * m, (size_t)(tk.a1 - tk.a0) * m * sizeof(T));
+  }
+}
+
+// What a launch prefetches into L2 for the launch after it: items [lo, hi)
+// of the forward (fwd) or backward upper items, from the tiled copy W.
+template <typename T>
+struct NextPrefetch {
+  int lo, hi;
+  bool fwd;
+  const T* W;
+};
+
 // ---------------------------------------------------------------- blocks
 
 // Walks one warp's slabs of a block in the order the warp consumes them: the
@@ -379,6 +411,9 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_block_forward(DPlan P, con
     }
   }
   if (failed) drain_stages(sm.bar, pending, par, R, sy.max_spins);
+  // no block left: the first upper level's factor into L2 for the next launch
+  if (P.upper_mode == 1)
+    prefetch_items<T>(P.fup, true, P.flev[0] + blockIdx.x * nw + warp, P.flev[1], gridDim.x * nw, W, lane);
 }
 
 template <typename T>
@@ -672,14 +707,18 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_backward(DPlan P, const
 
 // ---------------------------------------------- upper items, level by level
 
-// One elimination-tree level of upper items per launch, spread over all warps
-// (grid-stride); the launches follow one another in sweep order, so an item
-// needs no dependency wait and signals nothing.
+// One elimination-tree level of upper items per launch, [lo, hi), spread
+// over all warps (grid-stride); the launches follow one another in sweep
+// order, so an item needs no dependency wait and signals nothing.  Each warp
+// first prefetches the factor of all its items of this level into L2, and
+// when done those of its share of the next level [nlo, nhi): the factor does
+// not depend on the solve, so the next launch finds it in L2.
 template <typename T>
-__global__ void __launch_bounds__(kSweepThreads) k_upper_level_forward(DPlan P, int lo, int hi,
+__global__ void __launch_bounds__(kSweepThreads) k_upper_level_forward(DPlan P, int lo, int hi, NextPrefetch<T> nx,
                                                                        const T* __restrict__ W, T* b, T* y, int n) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+  prefetch_items<T>(P.fup, true, lo + gw, hi, nwarps, W, lane);
 #pragma unroll 1
   for (int t = lo + gw; t < hi; t += nwarps) {
     const UpperItem tk = P.fup[t];
@@ -719,14 +758,16 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_forward(DPlan P, 
       atomicAdd(b + r + 2 * (int64_t)n, -az);
     }
   }
+  prefetch_items<T>(nx.fwd ? P.fup : P.bup, nx.fwd, nx.lo + gw, nx.hi, nwarps, nx.W, lane);
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P, int lo, int hi,
+__global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P, int lo, int hi, NextPrefetch<T> nx,
                                                                         const T* __restrict__ W,
                                                                         const T* __restrict__ y, T* x, int n) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+  prefetch_items<T>(P.bup, false, lo + gw, hi, nwarps, W, lane);
 #pragma unroll 1
   for (int t = lo + gw; t < hi; t += nwarps) {
     const UpperItem tk = P.bup[t];
@@ -768,6 +809,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P,
       atomicAdd(x + o + 2 * (int64_t)n, az);
     }
   }
+  prefetch_items<T>(nx.fwd ? P.fup : P.bup, nx.fwd, nx.lo + gw, nx.hi, nwarps, nx.W, lane);
 }
 
 // After the backward sweep, for the upper supernodes' columns: v[perm] = x
@@ -881,8 +923,12 @@ void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* 
     const int wpc = kSweepThreads / 32;
     for (int k = 0; k < P.n_flev; ++k) {
       const int lo = P.flev[k], hi = P.flev[k + 1];
+      // the next level, and after the last (the root) the backward sweep's
+      // first level (the root again, in the backward copy)
+      const NextPrefetch<T> nx = k + 1 < P.n_flev ? NextPrefetch<T>{hi, P.flev[k + 2], true, Wf}
+                                                   : NextPrefetch<T>{P.blev[0], P.blev[1], false, Wb};
       const int grid = std::max(1, std::min(P.grid_uf, (hi - lo + wpc - 1) / wpc));
-      k_upper_level_forward<T><<<grid, kSweepThreads, 0, st>>>(P, lo, hi, Wf, b, y, n);
+      k_upper_level_forward<T><<<grid, kSweepThreads, 0, st>>>(P, lo, hi, nx, Wf, b, y, n);
     }
   } else {
     k_upper_forward<T><<<P.grid_uf, kSweepThreads, 0, st>>>(P, Wf, b, y, n, sy);
@@ -892,8 +938,10 @@ void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* 
     const int wpc = kSweepThreads / 32;
     for (int k = 0; k < P.n_blev; ++k) {
       const int lo = P.blev[k], hi = P.blev[k + 1];
+      const NextPrefetch<T> nx = k + 1 < P.n_blev ? NextPrefetch<T>{hi, P.blev[k + 2], false, Wb}
+                                                   : NextPrefetch<T>{0, 0, false, Wb};
       const int grid = std::max(1, std::min(P.grid_ub, (hi - lo + wpc - 1) / wpc));
-      k_upper_level_backward<T><<<grid, kSweepThreads, 0, st>>>(P, lo, hi, Wb, y, x, n);
+      k_upper_level_backward<T><<<grid, kSweepThreads, 0, st>>>(P, lo, hi, nx, Wb, y, x, n);
     }
   } else {
     k_upper_backward<T><<<P.grid_ub, kSweepThreads, 0, st>>>(P, Wb, y, x, n, sy);
