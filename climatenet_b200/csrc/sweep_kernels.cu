@@ -38,6 +38,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <utility>
 
 #include "device.cuh"
 #include "kernels.hpp"
@@ -96,6 +97,16 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
 // orders this thread's (and, after __syncwarp, the warp's) generic-proxy
 // reads of a stage before the bulk copy that overwrites it
+// Programmatic dependent launch: a kernel launched with the programmatic
+// stream serialization attribute may start while the kernel before it in the
+// stream still runs; griddep_wait() returns once that kernel has completed
+// and its memory operations are visible.  Before it, such a kernel reads
+// only data no kernel of the solve writes (the factor, the plan).
+// griddep_launch_dependents() lets the next such kernel start launching.
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void griddep_launch_dependents() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
@@ -293,6 +304,7 @@ template <typename T>
 __global__ void __launch_bounds__(kSweepThreads, 2) k_block_forward(DPlan P, const T* __restrict__ W, T* b, T* y,
                                                                     int n, SweepSync sy) {
   trace_stamp(sy.trace, DTrace::kSolve);
+  griddep_launch_dependents();  // the first upper level may start on SMs this sweep leaves
   constexpr int KE = Stages<T>::kElems;
   const int R = P.ring_f;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -420,6 +432,7 @@ template <typename T>
 __global__ void __launch_bounds__(kSweepThreads, 2) k_block_backward(DPlan P, const T* __restrict__ W,
                                                                      const T* __restrict__ y, const T* x, int n,
                                                                      SweepSync sy, WriteBack wb) {
+  griddep_launch_dependents();
   constexpr int KE = Stages<T>::kElems;
   const int R = P.ring_b;
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -444,7 +457,9 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_block_backward(DPlan P, co
     for (int k = threadIdx.x; k < nitems; k += blockDim.x) sm.items[k] = P.bitem[B.item0 + k];
     if (threadIdx.x <= nlev) s_lev[threadIdx.x] = B.lev[threadIdx.x];
     // the y slice, and the final x of the ext rows (the upper supernodes
-    // finished in the previous launch)
+    // finished in the previous launches: this kernel is their programmatic
+    // dependent)
+    griddep_wait();
     for (int k = threadIdx.x; k < nc; k += blockDim.x) {
       ys[k] = y[c0b + k];
       ys[nc + k] = y[(int64_t)n + c0b + k];
@@ -561,6 +576,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_block_backward(DPlan P, co
       }
   }
   if (failed) drain_stages(sm.bar, pending, par, R, sy.max_spins);
+  griddep_wait();  // a CTA without a block completes after the launch before it too
 }
 
 // ---------------------------------------------------------- upper items
@@ -718,13 +734,16 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_forward(DPlan P, 
                                                                        const T* __restrict__ W, T* b, T* y, int n) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+  griddep_launch_dependents();
   prefetch_items<T>(P.fup, true, lo + gw, hi, nwarps, W, lane);
+  bool waited = false;
 #pragma unroll 1
   for (int t = lo + gw; t < hi; t += nwarps) {
     const UpperItem tk = P.fup[t];
     const int mrows = min(kTile, tk.ns + tk.nr - tk.tile * kTile);
     const T* wbase = W + tk.off + lane;
     const int row = tk.tile * kTile + lane;
+    const int64_t r = (row >= tk.ns && row < tk.ns + tk.nr) ? P.rows[tk.roff + row - tk.ns] : -1;
     const T* bx = b + tk.c0;
     const T* by = bx + n;
     const T* bz = by + n;
@@ -732,6 +751,10 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_forward(DPlan P, 
     for (int j0 = tk.a0; j0 < tk.a1; j0 += 32) {
       T w[32];
       load_tile(w, wbase + (int64_t)j0 * mrows, min(32, tk.a1 - j0), mrows, lane < mrows);
+      if (!waited) {  // the factor is in flight; b comes from the previous launches
+        griddep_wait();
+        waited = true;
+      }
       const int jl = j0 + lane;
       T vx = 0, vy = 0, vz = 0;
       if (jl < tk.a1) {
@@ -751,14 +774,16 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_forward(DPlan P, 
       atomicAdd(y + o, ax);
       atomicAdd(y + o + n, ay);
       atomicAdd(y + o + 2 * (int64_t)n, az);
-    } else if (row < tk.ns + tk.nr) {
-      const int64_t r = P.rows[tk.roff + row - tk.ns];
+    } else if (r >= 0) {
       atomicAdd(b + r, -ax);
       atomicAdd(b + r + n, -ay);
       atomicAdd(b + r + 2 * (int64_t)n, -az);
     }
   }
   prefetch_items<T>(nx.fwd ? P.fup : P.bup, nx.fwd, nx.lo + gw, nx.hi, nwarps, nx.W, lane);
+  // every thread waits before it exits, so that this launch completes only
+  // after the one before it (the next programmatic dependent relies on it)
+  if (!waited) griddep_wait();
 }
 
 template <typename T>
@@ -767,7 +792,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P,
                                                                         const T* __restrict__ y, T* x, int n) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
+  griddep_launch_dependents();
   prefetch_items<T>(P.bup, false, lo + gw, hi, nwarps, W, lane);
+  bool waited = false;
 #pragma unroll 1
   for (int t = lo + gw; t < hi; t += nwarps) {
     const UpperItem tk = P.bup[t];
@@ -781,6 +808,11 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P,
       T w[32];
       load_tile(w, wbase + (int64_t)i0 * mcols, min(32, tk.a1 - i0), mcols, lane < mcols);
       const int il = i0 + lane;
+      const int64_t r = (il < tk.a1 && il >= nd) ? P.rows[tk.roff + il - nd] : 0;
+      if (!waited) {  // the factor and row indices are in flight; y and x come from the previous launches
+        griddep_wait();
+        waited = true;
+      }
       T vx = 0, vy = 0, vz = 0;
       if (il < tk.a1) {
         if (il < nd) {
@@ -789,7 +821,6 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P,
           vy = ldcg(y + o + n);
           vz = ldcg(y + o + 2 * (int64_t)n);
         } else {
-          const int64_t r = P.rows[tk.roff + il - nd];
           vx = -ldcg(x + r);
           vy = -ldcg(x + r + n);
           vz = -ldcg(x + r + 2 * (int64_t)n);
@@ -810,6 +841,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P,
     }
   }
   prefetch_items<T>(nx.fwd ? P.fup : P.bup, nx.fwd, nx.lo + gw, nx.hi, nwarps, nx.W, lane);
+  // every thread waits before it exits, so that this launch completes only
+  // after the one before it (the next programmatic dependent relies on it)
+  if (!waited) griddep_wait();
 }
 
 // After the backward sweep, for the upper supernodes' columns: v[perm] = x
@@ -819,6 +853,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P,
 // the work queues and advances the solve counter.
 template <typename T>
 __global__ void k_solve_post(DPlan P, T* __restrict__ x, T* __restrict__ y, int n, WriteBack wb, SweepSync sy) {
+  griddep_wait();  // launched as a programmatic dependent of the block backward sweep
   double* __restrict__ v = wb.v;
   double* __restrict__ qk = wb.qk;
   const double* __restrict__ q = wb.q;
@@ -913,6 +948,24 @@ bool configure_solve(DPlan& P, int shape) {
   return rf > 0 && rb > 0;
 }
 
+// Launch as a programmatic dependent of the previous kernel in the stream
+// (the kernel calls griddep_wait() before it reads what that kernel writes).
+template <typename... Params, typename... Args>
+void launch_dependent(void (*kernel)(Params...), int grid, int block, size_t smem, cudaStream_t st,
+                      Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 template <typename T>
 void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
                          SweepSync sy, WriteBack wb, cudaEvent_t* marks) {
@@ -928,7 +981,7 @@ void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* 
       const NextPrefetch<T> nx = k + 1 < P.n_flev ? NextPrefetch<T>{hi, P.flev[k + 2], true, Wf}
                                                    : NextPrefetch<T>{P.blev[0], P.blev[1], false, Wb};
       const int grid = std::max(1, std::min(P.grid_uf, (hi - lo + wpc - 1) / wpc));
-      k_upper_level_forward<T><<<grid, kSweepThreads, 0, st>>>(P, lo, hi, nx, Wf, b, y, n);
+      launch_dependent(k_upper_level_forward<T>, grid, kSweepThreads, 0, st, P, lo, hi, nx, Wf, b, y, n);
     }
   } else {
     k_upper_forward<T><<<P.grid_uf, kSweepThreads, 0, st>>>(P, Wf, b, y, n, sy);
@@ -941,15 +994,18 @@ void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* 
       const NextPrefetch<T> nx = k + 1 < P.n_blev ? NextPrefetch<T>{hi, P.blev[k + 2], false, Wb}
                                                    : NextPrefetch<T>{0, 0, false, Wb};
       const int grid = std::max(1, std::min(P.grid_ub, (hi - lo + wpc - 1) / wpc));
-      k_upper_level_backward<T><<<grid, kSweepThreads, 0, st>>>(P, lo, hi, nx, Wb, y, x, n);
+      launch_dependent(k_upper_level_backward<T>, grid, kSweepThreads, 0, st, P, lo, hi, nx, Wb,
+                       static_cast<const T*>(y), x, n);
     }
   } else {
     k_upper_backward<T><<<P.grid_ub, kSweepThreads, 0, st>>>(P, Wb, y, x, n, sy);
   }
   if (marks) cudaEventRecord(marks[2], st);
-  k_block_backward<T><<<P.grid_bb, 32 * P.block_warps, P.smem_b, st>>>(P, Wb, y, x, n, sy, wb);
+  launch_dependent(k_block_backward<T>, P.grid_bb, 32 * P.block_warps, (size_t)P.smem_b, st, P, Wb,
+                   static_cast<const T*>(y), static_cast<const T*>(x), n, sy, wb);
   if (marks) cudaEventRecord(marks[3], st);
-  k_solve_post<T><<<std::max(1, std::min(148 * 4, (P.n_upper + 255) / 256)), 256, 0, st>>>(P, x, y, n, wb, sy);
+  launch_dependent(k_solve_post<T>, std::max(1, std::min(148 * 4, (P.n_upper + 255) / 256)), 256, 0, st, P, x, y, n,
+                   wb, sy);
 }
 template <typename T>
 void launch_solve_prep(cudaStream_t st, int n, T* x, T* y, SweepSync sy) {
