@@ -551,11 +551,6 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
     fb.nlev = bb.nlev = f.sn_level[r] + 1;
     fb.ext0 = bb.ext0 = (int)f.sn_roff[r];
     fb.next = bb.next = f.sn_nr[r];
-    const int s_first = *std::min_element(members[b].begin(), members[b].end());
-    fb.woff = f.ftile_off[f.sn_ftile0[s_first]];
-    fb.wlen = f.ftile_off[f.sn_ftile0[r + 1]] - fb.woff;
-    bb.woff = f.btile_off[f.sn_btile0[s_first]];
-    bb.wlen = f.btile_off[f.sn_btile0[r + 1]] - bb.woff;
     plan.max_block_cols = std::max(plan.max_block_cols, fb.c1 - fb.c0);
     plan.max_block_ext = std::max(plan.max_block_ext, fb.next);
     // where each row of each member lives in the block's shared vector
@@ -691,10 +686,6 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
       return false;
     }
     if (!chk(B.c0, n, "block columns") || !chk(B.c1 - 1, n, "block columns")) return false;
-    if (B.woff < 0 || B.wlen < 0 || B.woff + B.wlen > nWf) {
-      err = "forward block tile range outside the tiled copy";
-      return false;
-    }
     std::vector<double> sv(3 * (size_t)ld, 0.);
     for (int k = 0; k < nc; ++k)
       for (int c = 0; c < 3; ++c) sv[k + c * ld] = b[B.c0 + k + c * n];
@@ -705,10 +696,6 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
         const int m = std::min(kTile, I.ns + I.nr - kTile * I.tile), w = std::min((int)I.ns, kTile * I.tile + (int)kTile);
         if ((I.off % kTilePad) != 0 || I.a0 % kSlab != 0 || I.a0 < 0 || I.a0 >= I.a1 || I.a1 > w) {
           err = "forward block item not aligned or out of its tile";
-          return false;
-        }
-        if (I.off < B.woff || I.off + (int64_t)m * w > B.woff + B.wlen) {
-          err = "forward block item outside the block's tile range";
           return false;
         }
         for (int l = 0; l < m; ++l) {
@@ -831,10 +818,6 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
   const int64_t nbidx = (int64_t)plan.bidx.size();
   for (const SweepBlock& B : plan.bblk) {
     const int nc = B.c1 - B.c0, ld = nc + B.next;
-    if (B.woff < 0 || B.wlen < 0 || B.woff + B.wlen > nWb) {
-      err = "backward block tile range outside the tiled copy";
-      return false;
-    }
     std::vector<double> sx(3 * (size_t)ld, 0.), ys(3 * (size_t)nc, 0.);
     for (int e = 0; e < B.next; ++e) {
       if (!chk(B.ext0 + e, nrows, "backward block ext rows")) return false;
@@ -852,10 +835,6 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
         if ((I.off % kTilePad) != 0 || (I.idx0 % kSlab) != 0 || I.a0 % kSlab != 0 || I.a0 < 0 || I.a0 >= I.a1 ||
             I.a1 > h) {
           err = "backward block item not aligned or out of its tile";
-          return false;
-        }
-        if (I.off < B.woff || I.off + (int64_t)mc * h > B.woff + B.wlen) {
-          err = "backward block item outside the block's tile range";
           return false;
         }
         for (int l = 0; l < mc; ++l) {

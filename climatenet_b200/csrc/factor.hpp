@@ -124,9 +124,6 @@ struct SweepBlock {
   int ext0;      // its ext rows are Factor::rows[ext0, ext0 + next) (R of the root)
   int next;
   int lev[kMaxBlockLevels + 1];  // item offsets (from item0) per level, in sweep order
-  // the block's tiles in the sweep's tiled copy: elements [woff, woff + wlen)
-  // (its supernodes are consecutive, so their tiles are too)
-  int64_t woff, wlen;
 };
 // One work item of a tile of a supernode inside a block: forward, rows
 // [32 tile, 32 tile + m) of W_s over its columns [a0, a1) of

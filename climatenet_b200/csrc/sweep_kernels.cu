@@ -180,14 +180,6 @@ __device__ __forceinline__ void prefetch_items(const UpperItem* items, bool fwd,
   }
 }
 
-// The lanes of one warp prefetch W[off, off + len) into L2 in 32 pieces.
-template <typename T>
-__device__ __forceinline__ void prefetch_range(const T* W, int64_t off, int64_t len, int lane) {
-  const int64_t piece = (len + 31) / 32;
-  const int64_t a = off + lane * piece, e = min(off + len, a + piece);
-  if (e > a) prefetch_l2(W + a, (size_t)(e - a) * sizeof(T));
-}
-
 // What a launch prefetches into L2 for the launch after it: items [lo, hi)
 // of the forward (fwd) or backward upper items, from the tiled copy W.
 template <typename T>
@@ -331,8 +323,6 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_block_forward(DPlan P, con
     const int bi = cta_ticket(sy.queue + 2, &s_ticket);
     if (bi >= P.nblk) break;
     const SweepBlock& B = P.fblk[bi];
-    // the whole block's factor streams into L2 while the first slabs are copied
-    if (warp == nw - 1) prefetch_range(W, B.woff, B.wlen, lane);
     const int c0b = B.c0, nc = B.c1 - B.c0, ld = nc + B.next, nlev = B.nlev, nitems = B.lev[B.nlev];
     T* sv = sm.sv;
     for (int k = threadIdx.x; k < nc; k += blockDim.x) {
@@ -461,7 +451,6 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_block_backward(DPlan P, co
     const int bi = cta_ticket(sy.queue + 3, &s_ticket);
     if (bi >= P.nblk) break;
     const SweepBlock& B = P.bblk[bi];
-    if (warp == nw - 1) prefetch_range(W, B.woff, B.wlen, lane);
     const int c0b = B.c0, nc = B.c1 - B.c0, ld = nc + B.next, nlev = B.nlev, nitems = B.lev[B.nlev];
     T* sv = sm.sv;
     T* ys = sm.ys;
