@@ -149,45 +149,27 @@ __device__ __forceinline__ void load_tile(T (&w)[32], const T* p, int m, int str
   for (int u = 0; u < 32; ++u) w[u] = (act && u < m) ? ldw(p + u * stride) : T(0);
 }
 
-// CTA-wide ticket: thread 0 draws, everyone reads it after the barrier.
-__device__ __forceinline__ int cta_ticket(int* queue, int* slot) {
-  __syncthreads();  // every thread has read the previous ticket
-  if (threadIdx.x == 0) *slot = atomicAdd(queue, 1);
-  __syncthreads();
-  return *slot;
+// Asynchronous global -> shared copy of N = 4, 8 or 16 bytes (both
+// addresses N-byte aligned); cp_async_wait_all() waits for this thread's.
+template <int N>
+__device__ __forceinline__ void cp_async(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(smem_u32(dst)), "l"(src), "n"(N) : "memory");
 }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
-// L2 prefetch of [p, p + bytes), shrunk to 16-byte boundaries (a hint: no
-// completion to wait for, nothing lands in shared memory)
-__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
-  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
-  const uintptr_t s = (a + 15) & ~uintptr_t(15);
-  const uintptr_t e = (a + bytes) & ~uintptr_t(15);
-  if (e > s) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(s), "r"((uint32_t)(e - s)) : "memory");
-}
-
-// Lane j of a warp prefetches into L2 the factor of the warp's j-th item
-// among items[first + j * stride] (< hi): its tile rows (forward) or
-// columns (backward) over [a0, a1), contiguous in the tiled copy.
-template <typename T>
-__device__ __forceinline__ void prefetch_items(const UpperItem* items, bool fwd, int first, int hi, int stride,
-                                               const T* W, int lane) {
-  const int t = first + lane * stride;
-  if (first < hi && t < hi) {
-    const UpperItem tk = items[t];
-    const int m = fwd ? min(kTile, tk.ns + tk.nr - tk.tile * kTile) : min(kTile, tk.ns - tk.tile * kTile);
-    prefetch_l2(W + tk.off + (int64_t)tk.a0 * m, (size_t)(tk.a1 - tk.a0) * m * sizeof(T));
+// A block's item descriptors into shared memory (32 bytes each, two copies).
+__device__ __forceinline__ void stage_items(BlockItem* dst, const BlockItem* src, int nitems) {
+  for (int k = threadIdx.x; k < nitems; k += blockDim.x) {
+    cp_async<16>(reinterpret_cast<char*>(dst + k), reinterpret_cast<const char*>(src + k));
+    cp_async<16>(reinterpret_cast<char*>(dst + k) + 16, reinterpret_cast<const char*>(src + k) + 16);
   }
 }
 
-// What a launch prefetches into L2 for the launch after it: items [lo, hi)
-// of the forward (fwd) or backward upper items, from the tiled copy W.
-template <typename T>
-struct NextPrefetch {
-  int lo, hi;
-  bool fwd;
-  const T* W;
-};
+// Block tickets: thread 0 draws the first one before the loop and the next
+// one when a block enters its last level (its round trip overlaps that
+// level, and blocks are still claimed in about the order CTAs free up); the
+// ticket is published in shared memory between two barriers at the block's
+// end, after every thread has read the current one.
 
 // ---------------------------------------------------------------- blocks
 
@@ -319,20 +301,26 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_block_forward(DPlan P, con
   uint32_t par = 0, pending = 0;  // per stage: wait parity, fill in flight
   int prod = 0, cons = 0;         // slabs issued / consumed by this warp
   bool failed = false;
+  int next_ticket = 0;  // thread 0
+  if (threadIdx.x == 0) s_ticket = atomicAdd(sy.queue + 2, 1);
+  __syncthreads();
   for (;;) {
-    const int bi = cta_ticket(sy.queue + 2, &s_ticket);
+    const int bi = s_ticket;
     if (bi >= P.nblk) break;
     const SweepBlock& B = P.fblk[bi];
     const int c0b = B.c0, nc = B.c1 - B.c0, ld = nc + B.next, nlev = B.nlev, nitems = B.lev[B.nlev];
     T* sv = sm.sv;
+    // b of the block's columns and the item descriptors: every copy in
+    // flight at once
     for (int k = threadIdx.x; k < nc; k += blockDim.x) {
-      sv[k] = b[c0b + k];
-      sv[ld + k] = b[(int64_t)n + c0b + k];
-      sv[2 * ld + k] = b[2 * (int64_t)n + c0b + k];
+      cp_async<sizeof(T)>(sv + k, b + c0b + k);
+      cp_async<sizeof(T)>(sv + ld + k, b + (int64_t)n + c0b + k);
+      cp_async<sizeof(T)>(sv + 2 * ld + k, b + 2 * (int64_t)n + c0b + k);
     }
+    stage_items(sm.items, P.fitem + B.item0, nitems);
     for (int e = threadIdx.x; e < B.next; e += blockDim.x) sv[nc + e] = sv[ld + nc + e] = sv[2 * ld + nc + e] = T(0);
-    for (int k = threadIdx.x; k < nitems; k += blockDim.x) sm.items[k] = P.fitem[B.item0 + k];
     if (threadIdx.x <= nlev) s_lev[threadIdx.x] = B.lev[threadIdx.x];
+    cp_async_wait_all();
     __syncthreads();
     const BlockItem* items = sm.items;
     SlabCursor pc;
@@ -345,6 +333,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_block_forward(DPlan P, con
       cursor_next<true>(pc, nlev, s_lev, items, warp, nw);
     }
     for (int L = 0; L < nlev; ++L) {
+      if (L == nlev - 1 && threadIdx.x == 0) next_ticket = atomicAdd(sy.queue + 2, 1);
       const int i1 = s_lev[L + 1];
 #pragma unroll 1
       for (int it = s_lev[L] + warp; it < i1; it += nw) {
@@ -421,11 +410,54 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_block_forward(DPlan P, con
       atomicAdd(b + r + n, sv[ld + nc + e]);
       atomicAdd(b + r + 2 * (int64_t)n, sv[2 * ld + nc + e]);
     }
+    __syncthreads();  // the shared vector is free, every thread has read s_ticket
+    if (threadIdx.x == 0) s_ticket = next_ticket;
+    __syncthreads();
   }
   if (failed) drain_stages(sm.bar, pending, par, R, sy.max_spins);
-  // no block left: the first upper level's factor into L2 for the next launch
-  if (P.upper_mode == 1)
-    prefetch_items<T>(P.fup, true, P.flev[0] + blockIdx.x * nw + warp, P.flev[1], gridDim.x * nw, W, lane);
+}
+
+// v[perm[k]] = x_k (mode 0) or += x_k (mode 1) and q^k = q_n + dt v for the
+// nc columns of a block, x in shared memory (3 planes of stride ld).  Each
+// thread takes kWbCols columns a pass and issues every load of the pass
+// before its stores, so that a pass costs two dependent memory round trips
+// (the permutation, then the vertex gathers) instead of several per column.
+constexpr int kWbCols = 4;
+constexpr int kExtBatch = 4;  // ext rows per thread whose indices are loaded together
+template <typename T>
+__device__ __forceinline__ void write_back_columns(const T* sv, int ld, int nc, const int* __restrict__ perm,
+                                                   const WriteBack& wb) {
+  double* __restrict__ v = wb.v;
+  double* __restrict__ qk = wb.qk;
+  const double* __restrict__ q = wb.q;
+  for (int k0 = threadIdx.x; k0 < nc; k0 += kWbCols * blockDim.x) {
+    int64_t vtx[kWbCols];
+    double val[kWbCols][3], qv[kWbCols][3];
+#pragma unroll
+    for (int j = 0; j < kWbCols; ++j) {
+      const int k = k0 + j * blockDim.x;
+      vtx[j] = k < nc ? perm[k] : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < kWbCols; ++j)
+      if (vtx[j] >= 0) {
+        const int k = k0 + j * blockDim.x;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          val[j][c] = (double)sv[k + c * ld];
+          qv[j][c] = q[3 * vtx[j] + c];
+          if (wb.mode == 1) val[j][c] += v[3 * vtx[j] + c];
+        }
+      }
+#pragma unroll
+    for (int j = 0; j < kWbCols; ++j)
+      if (vtx[j] >= 0)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          v[3 * vtx[j] + c] = val[j][c];
+          qk[3 * vtx[j] + c] = qv[j][c] + wb.dt * val[j][c];
+        }
+  }
 }
 
 template <typename T>
@@ -447,32 +479,51 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_block_backward(DPlan P, co
   uint32_t par = 0, pending = 0;
   int prod = 0, cons = 0;
   bool failed = false;
+  int next_ticket = 0;  // thread 0
+  if (threadIdx.x == 0) s_ticket = atomicAdd(sy.queue + 3, 1);
+  __syncthreads();
   for (;;) {
-    const int bi = cta_ticket(sy.queue + 3, &s_ticket);
+    const int bi = s_ticket;
     if (bi >= P.nblk) break;
     const SweepBlock& B = P.bblk[bi];
     const int c0b = B.c0, nc = B.c1 - B.c0, ld = nc + B.next, nlev = B.nlev, nitems = B.lev[B.nlev];
     T* sv = sm.sv;
     T* ys = sm.ys;
-    for (int k = threadIdx.x; k < nitems; k += blockDim.x) sm.items[k] = P.bitem[B.item0 + k];
+    stage_items(sm.items, P.bitem + B.item0, nitems);
     if (threadIdx.x <= nlev) s_lev[threadIdx.x] = B.lev[threadIdx.x];
-    // the y slice, and the final x of the ext rows (the upper supernodes
-    // finished in the previous launches: this kernel is their programmatic
-    // dependent)
+    // the ext rows' indices (constant), then the y slice and the final x of
+    // the ext rows (the upper supernodes finished in the previous launches:
+    // this kernel is their programmatic dependent), every copy in flight at once
+    const int* ext_rows = P.rows + B.ext0;
+    int64_t er[kExtBatch];
+#pragma unroll
+    for (int j = 0; j < kExtBatch; ++j) {
+      const int e = threadIdx.x + j * blockDim.x;
+      er[j] = e < B.next ? ext_rows[e] : -1;
+    }
     griddep_wait();
     for (int k = threadIdx.x; k < nc; k += blockDim.x) {
-      ys[k] = y[c0b + k];
-      ys[nc + k] = y[(int64_t)n + c0b + k];
-      ys[2 * nc + k] = y[2 * (int64_t)n + c0b + k];
+      cp_async<sizeof(T)>(ys + k, y + c0b + k);
+      cp_async<sizeof(T)>(ys + nc + k, y + (int64_t)n + c0b + k);
+      cp_async<sizeof(T)>(ys + 2 * nc + k, y + 2 * (int64_t)n + c0b + k);
     }
-    for (int e = threadIdx.x; e < B.next; e += blockDim.x) {
-      const int64_t r = P.rows[B.ext0 + e];
-      sv[nc + e] = x[r];
-      sv[ld + nc + e] = x[r + n];
-      sv[2 * ld + nc + e] = x[r + 2 * (int64_t)n];
+#pragma unroll
+    for (int j = 0; j < kExtBatch; ++j)
+      if (er[j] >= 0) {
+        const int e = threadIdx.x + j * blockDim.x;
+        cp_async<sizeof(T)>(sv + nc + e, x + er[j]);
+        cp_async<sizeof(T)>(sv + ld + nc + e, x + er[j] + n);
+        cp_async<sizeof(T)>(sv + 2 * ld + nc + e, x + er[j] + 2 * (int64_t)n);
+      }
+    for (int e = threadIdx.x + kExtBatch * blockDim.x; e < B.next; e += blockDim.x) {  // beyond the batch
+      const int64_t r = ext_rows[e];
+      cp_async<sizeof(T)>(sv + nc + e, x + r);
+      cp_async<sizeof(T)>(sv + ld + nc + e, x + r + n);
+      cp_async<sizeof(T)>(sv + 2 * ld + nc + e, x + r + 2 * (int64_t)n);
     }
     // the block's columns start at zero: the spans of a split tile add into them
     for (int k = threadIdx.x; k < nc; k += blockDim.x) sv[k] = sv[ld + k] = sv[2 * ld + k] = T(0);
+    cp_async_wait_all();
     __syncthreads();
     const BlockItem* items = sm.items;
     SlabCursor pc;
@@ -486,6 +537,7 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_block_backward(DPlan P, co
       cursor_next<false>(pc, nlev, s_lev, items, warp, nw);
     }
     for (int L = 0; L < nlev; ++L) {
+      if (L == nlev - 1 && threadIdx.x == 0) next_ticket = atomicAdd(sy.queue + 3, 1);
       const int i1 = s_lev[L + 1];
 #pragma unroll 1
       for (int it = s_lev[L] + warp; it < i1; it += nw) {
@@ -564,16 +616,10 @@ __global__ void __launch_bounds__(kSweepThreads, 2) k_block_backward(DPlan P, co
       }
       __syncthreads();
     }
-    if (!failed)
-      for (int k = threadIdx.x; k < nc; k += blockDim.x) {
-        const int64_t vtx = P.perm[c0b + k];
-        for (int c = 0; c < 3; ++c) {
-          double val = (double)sv[k + c * ld];
-          if (wb.mode == 1) val += wb.v[3 * vtx + c];
-          wb.v[3 * vtx + c] = val;
-          wb.qk[3 * vtx + c] = wb.q[3 * vtx + c] + wb.dt * val;
-        }
-      }
+    if (!failed) write_back_columns(sv, ld, nc, P.perm + c0b, wb);
+    __syncthreads();  // the shared vectors are free, every thread has read s_ticket
+    if (threadIdx.x == 0) s_ticket = next_ticket;
+    __syncthreads();
   }
   if (failed) drain_stages(sm.bar, pending, par, R, sy.max_spins);
   griddep_wait();  // a CTA without a block completes after the launch before it too
@@ -725,17 +771,15 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_backward(DPlan P, const
 
 // One elimination-tree level of upper items per launch, [lo, hi), spread
 // over all warps (grid-stride); the launches follow one another in sweep
-// order, so an item needs no dependency wait and signals nothing.  Each warp
-// first prefetches the factor of all its items of this level into L2, and
-// when done those of its share of the next level [nlo, nhi): the factor does
-// not depend on the solve, so the next launch finds it in L2.
+// order, so an item needs no dependency wait and signals nothing.  Launched
+// as programmatic dependents: an item's factor tile and row indices are
+// loaded before the wait for the previous launch, its vector after it.
 template <typename T>
-__global__ void __launch_bounds__(kSweepThreads) k_upper_level_forward(DPlan P, int lo, int hi, NextPrefetch<T> nx,
+__global__ void __launch_bounds__(kSweepThreads) k_upper_level_forward(DPlan P, int lo, int hi,
                                                                        const T* __restrict__ W, T* b, T* y, int n) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
   griddep_launch_dependents();
-  prefetch_items<T>(P.fup, true, lo + gw, hi, nwarps, W, lane);
   bool waited = false;
 #pragma unroll 1
   for (int t = lo + gw; t < hi; t += nwarps) {
@@ -780,20 +824,18 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_forward(DPlan P, 
       atomicAdd(b + r + 2 * (int64_t)n, -az);
     }
   }
-  prefetch_items<T>(nx.fwd ? P.fup : P.bup, nx.fwd, nx.lo + gw, nx.hi, nwarps, nx.W, lane);
   // every thread waits before it exits, so that this launch completes only
   // after the one before it (the next programmatic dependent relies on it)
   if (!waited) griddep_wait();
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P, int lo, int hi, NextPrefetch<T> nx,
+__global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P, int lo, int hi,
                                                                         const T* __restrict__ W,
                                                                         const T* __restrict__ y, T* x, int n) {
   const int lane = threadIdx.x & 31;
   const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nwarps = (gridDim.x * blockDim.x) >> 5;
   griddep_launch_dependents();
-  prefetch_items<T>(P.bup, false, lo + gw, hi, nwarps, W, lane);
   bool waited = false;
 #pragma unroll 1
   for (int t = lo + gw; t < hi; t += nwarps) {
@@ -840,7 +882,6 @@ __global__ void __launch_bounds__(kSweepThreads) k_upper_level_backward(DPlan P,
       atomicAdd(x + o + 2 * (int64_t)n, az);
     }
   }
-  prefetch_items<T>(nx.fwd ? P.fup : P.bup, nx.fwd, nx.lo + gw, nx.hi, nwarps, nx.W, lane);
   // every thread waits before it exits, so that this launch completes only
   // after the one before it (the next programmatic dependent relies on it)
   if (!waited) griddep_wait();
@@ -976,12 +1017,8 @@ void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* 
     const int wpc = kSweepThreads / 32;
     for (int k = 0; k < P.n_flev; ++k) {
       const int lo = P.flev[k], hi = P.flev[k + 1];
-      // the next level, and after the last (the root) the backward sweep's
-      // first level (the root again, in the backward copy)
-      const NextPrefetch<T> nx = k + 1 < P.n_flev ? NextPrefetch<T>{hi, P.flev[k + 2], true, Wf}
-                                                   : NextPrefetch<T>{P.blev[0], P.blev[1], false, Wb};
       const int grid = std::max(1, std::min(P.grid_uf, (hi - lo + wpc - 1) / wpc));
-      launch_dependent(k_upper_level_forward<T>, grid, kSweepThreads, 0, st, P, lo, hi, nx, Wf, b, y, n);
+      launch_dependent(k_upper_level_forward<T>, grid, kSweepThreads, 0, st, P, lo, hi, Wf, b, y, n);
     }
   } else {
     k_upper_forward<T><<<P.grid_uf, kSweepThreads, 0, st>>>(P, Wf, b, y, n, sy);
@@ -991,10 +1028,8 @@ void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* 
     const int wpc = kSweepThreads / 32;
     for (int k = 0; k < P.n_blev; ++k) {
       const int lo = P.blev[k], hi = P.blev[k + 1];
-      const NextPrefetch<T> nx = k + 1 < P.n_blev ? NextPrefetch<T>{hi, P.blev[k + 2], false, Wb}
-                                                   : NextPrefetch<T>{0, 0, false, Wb};
       const int grid = std::max(1, std::min(P.grid_ub, (hi - lo + wpc - 1) / wpc));
-      launch_dependent(k_upper_level_backward<T>, grid, kSweepThreads, 0, st, P, lo, hi, nx, Wb,
+      launch_dependent(k_upper_level_backward<T>, grid, kSweepThreads, 0, st, P, lo, hi, Wb,
                        static_cast<const T*>(y), x, n);
     }
   } else {
