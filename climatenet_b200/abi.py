@@ -129,7 +129,7 @@ class pdf_stats(C.Structure):
         ("sweep_cut_level_ms", C.c_double * 8),
         ("sweep_block_shape", C.c_int32), ("sweep_block_warps", C.c_int32),
         ("sweep_block_ctas", C.c_int32), ("sweep_ring_stages", C.c_int32 * 2),
-        ("sweep_shape_ms", C.c_double * 4),
+        ("sweep_shape_ms", C.c_double * 5),
     ]
 
 

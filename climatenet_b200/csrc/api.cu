@@ -1617,7 +1617,7 @@ int pdf_set_sweep_schedule(pdf_handle* h, int32_t chunk, int32_t cut_level, int3
       cut_level < 0 || cut_level >= kCutCandidates || (upper_mode != 0 && upper_mode != 1) || block_shape < 0 ||
       block_shape >= kBlockShapes)
     return fail(h, PDF_INVALID_ARG,
-                "sweep schedule outside chunk {32, 64, 128}, cut level 0-7, mode 0/1, block shape 0-3");
+                "sweep schedule outside chunk {32, 64, 128}, cut level 0-7, mode 0/1, block shape 0-4");
   return guarded(h, [&]() -> int {
     CK(cudaSetDevice(h->prm.device));
     CK(cudaStreamSynchronize(h->stream));

@@ -25,9 +25,9 @@ constexpr int kMaxUpperLevels = 32;
 
 // Launch shapes of the block kernels: warps per CTA and CTAs per SM (the
 // ring of bulk-copy stages shrinks to fit); the schedule autotuner picks one.
-constexpr int kBlockShapes = 4;
-constexpr int kBlockShapeWarps[kBlockShapes] = {8, 8, 4, 4};
-constexpr int kBlockShapeCtas[kBlockShapes] = {1, 2, 3, 4};
+constexpr int kBlockShapes = 5;
+constexpr int kBlockShapeWarps[kBlockShapes] = {8, 8, 4, 4, 16};
+constexpr int kBlockShapeCtas[kBlockShapes] = {1, 2, 3, 4, 1};
 
 // Device view of a SweepPlan (factor.hpp) and its launch shape.
 struct DPlan {

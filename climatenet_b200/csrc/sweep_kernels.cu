@@ -47,14 +47,15 @@ namespace pdfb {
 
 constexpr int kTicketBatch = 2;
 constexpr int kSweepThreads = 256;
+constexpr int kBlockMaxThreads = 512;  // block kernels: up to 16 warps per CTA (at most 128 registers a thread)
 
 // Bulk-copy stages per warp: one slab (32 rows x kSlab columns, or kSlab rows
-// x 32 columns) each.  kDeep stages (12 KB per warp in both precisions) when
-// one CTA of 8 warps holds the SM; fewer when the launch shape packs several
-// CTAs per SM (DPlan::ring_f / ring_b, at least kMinRing).
+// x 32 columns) each.  The deepest ring (at most kDeep stages, 16 KB per warp
+// in both precisions) with which the launch shape's CTAs fit an SM
+// (DPlan::ring_f / ring_b, at least kMinRing).
 template <typename T>
 struct Stages {
-  static constexpr int kDeep = sizeof(T) == 8 ? 3 : 6;
+  static constexpr int kDeep = sizeof(T) == 8 ? 4 : 8;
   static constexpr int kElems = kTile * kSlab;
 };
 constexpr int kMinRing = 2;
@@ -283,7 +284,7 @@ __device__ __forceinline__ void drain_stages(uint64_t* bar, uint32_t pending, ui
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kSweepThreads, 2) k_block_forward(DPlan P, const T* __restrict__ W, T* b, T* y,
+__global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, const T* __restrict__ W, T* b, T* y,
                                                                     int n, SweepSync sy) {
   trace_stamp(sy.trace, DTrace::kSolve);
   griddep_launch_dependents();  // the first upper level may start on SMs this sweep leaves
@@ -461,7 +462,7 @@ __device__ __forceinline__ void write_back_columns(const T* sv, int ld, int nc, 
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kSweepThreads, 2) k_block_backward(DPlan P, const T* __restrict__ W,
+__global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P, const T* __restrict__ W,
                                                                      const T* __restrict__ y, const T* x, int n,
                                                                      SweepSync sy, WriteBack wb) {
   griddep_launch_dependents();

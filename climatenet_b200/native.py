@@ -214,7 +214,7 @@ class Simulation:
     def set_sweep_schedule(self, chunk, cut_level, upper_mode, block_shape=1):
         """Pin the solve schedule (work-item width, subtree-block cut level,
         upper mode 0 = dependency-driven items / 1 = level launches, block
-        kernel launch shape 0-3)."""
+        kernel launch shape 0-4)."""
         _check(lib().pdf_set_sweep_schedule(self.h, chunk, cut_level, upper_mode, block_shape), self.h)
 
     def time_solve_parts(self, reps=10):

@@ -194,13 +194,14 @@ typedef struct pdf_stats {
    * the levels exceed the launch table) */
   int32_t sweep_upper_mode, sweep_upper_levels;
   double sweep_cut_level_ms[8];
-  /* launch shape of the block kernels: 0-3 = 1 CTA of 8 warps, 2 CTAs of 8
-   * warps, 3 CTAs of 4 warps, 4 CTAs of 4 warps per SM; its warps and CTAs,
+  /* launch shape of the block kernels: 0-4 = 1 CTA of 8 warps, 2 CTAs of 8
+   * warps, 3 CTAs of 4 warps, 4 CTAs of 4 warps, 1 CTA of 16 warps per SM;
+   * its warps and CTAs,
    * the bulk-copy stages per warp (forward, backward), and the solve time of
    * each shape at the chosen cut level (0 where it does not fit) */
   int32_t sweep_block_shape, sweep_block_warps, sweep_block_ctas;
   int32_t sweep_ring_stages[2];
-  double sweep_shape_ms[4];
+  double sweep_shape_ms[5];
 } pdf_stats;
 
 /* One contact, as the reference's CollisionInfo / SelfCollisionInfo plus
@@ -371,7 +372,7 @@ int pdf_time_solve_parts(pdf_handle* h, int32_t reps, double* part_ms);
  * in the reference): work-item width chunk (32, 64 or 128), subtree-block
  * cut level 0-7, the mode of the supernodes above the blocks (0 =
  * dependency-driven work items, 1 = one launch per elimination-tree level),
- * and the launch shape of the block kernels (0-3, as stats
+ * and the launch shape of the block kernels (0-4, as stats
  * sweep_block_shape).  Every schedule solves the same system; the results
  * agree to rounding.  PDF_INVALID_ARG for values outside these sets, for
  * mode 1 on a scene with more upper levels than the launch table holds

@@ -46,7 +46,8 @@ def oracle_run():
 
 @pytest.mark.parametrize("precision", [abi.PDF_FP64, abi.PDF_FP32_REFINE])
 @pytest.mark.parametrize("chunk,cut,mode,shape", [(64, 0, 0, 1), (64, 0, 1, 3), (32, 3, 0, 2), (32, 3, 1, 1),
-                                                  (128, 5, 1, 0), (64, 7, 0, 1), (64, 7, 1, 0), (64, 2, 1, 3)])
+                                                  (128, 5, 1, 0), (64, 7, 0, 1), (64, 7, 1, 0), (64, 2, 1, 3),
+                                                  (64, 3, 1, 4)])
 def test_schedule_matches_oracle(oracle_run, chunk, cut, mode, shape, precision):
     s, traj, counts = oracle_run
     g = native.Simulation(s, abi.params(time_step=5e-3, iterations=20, precision=precision))
@@ -76,7 +77,7 @@ def test_schedule_change_replaces_captured_graph(oracle_run):
 def test_schedule_rejects_values_outside_the_tuned_sets(oracle_run):
     s, traj, _ = oracle_run
     g = native.Simulation(s, abi.params(time_step=5e-3, iterations=20))
-    for args in ((48, 0, 0, 1), (64, 8, 0, 1), (64, -1, 0, 1), (64, 0, 2, 1), (64, 0, 0, 4), (64, 0, 0, -1)):
+    for args in ((48, 0, 0, 1), (64, 8, 0, 1), (64, -1, 0, 1), (64, 0, 2, 1), (64, 0, 0, 5), (64, 0, 0, -1)):
         with pytest.raises(native.PdfError):
             g.set_sweep_schedule(*args)
     # one block of this scene at cut level 7 holds about 1500 columns in FP64:
