@@ -172,13 +172,13 @@ __device__ __forceinline__ void stage_items(BlockItem* dst, const BlockItem* src
 // ticket is published in shared memory between two barriers at the block's
 // end, after every thread has read the current one.
 
-// L2 prefetch of the 128-byte lines of [p, p + bytes) by one thread, with
-// the load/store unit's prefetch (the bulk-copy unit stays free for the
-// slab rings)
+// L2 prefetch of [p, p + bytes), shrunk to 16-byte boundaries (a hint: no
+// completion to wait for, nothing lands in shared memory)
 __device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
-  const char* a = reinterpret_cast<const char*>(reinterpret_cast<uintptr_t>(p) & ~uintptr_t(127));
-  const char* e = reinterpret_cast<const char*>(p) + bytes;
-  for (; a < e; a += 128) asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+  const uintptr_t s = (a + 15) & ~uintptr_t(15);
+  const uintptr_t e = (a + bytes) & ~uintptr_t(15);
+  if (e > s) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(s), "r"((uint32_t)(e - s)) : "memory");
 }
 
 // The factor of a block's items of levels [L0, L1) into L2.  The slab rings
