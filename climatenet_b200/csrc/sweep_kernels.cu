@@ -172,30 +172,6 @@ __device__ __forceinline__ void stage_items(BlockItem* dst, const BlockItem* src
 // ticket is published in shared memory between two barriers at the block's
 // end, after every thread has read the current one.
 
-// L2 prefetch of [p, p + bytes), shrunk to 16-byte boundaries (a hint: no
-// completion to wait for, nothing lands in shared memory)
-__device__ __forceinline__ void prefetch_l2(const void* p, size_t bytes) {
-  const uintptr_t a = reinterpret_cast<uintptr_t>(p);
-  const uintptr_t s = (a + 15) & ~uintptr_t(15);
-  const uintptr_t e = (a + bytes) & ~uintptr_t(15);
-  if (e > s) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(s), "r"((uint32_t)(e - s)) : "memory");
-}
-
-// The factor of a block's items of levels [L0, L1) into L2.  The slab rings
-// run only a few slabs ahead, so without it each of the block's small levels
-// (above the leaves) would begin with a wait for HBM; the leaves, about half
-// of a block's factor, stream through the rings at full rate and are not
-// prefetched (forward: L0 = 1, L1 = nlev; backward: L0 = 1, L1 = nlev - 1).
-template <typename T, bool kFwd>
-__device__ __forceinline__ void prefetch_levels(const BlockItem* items, const int* lev, int L0, int L1, const T* W) {
-  if (L0 >= L1) return;
-  for (int k = lev[L0] + threadIdx.x; k < lev[L1]; k += blockDim.x) {
-    const BlockItem I = items[k];
-    const int m = kFwd ? min(kTile, I.ns + I.nr - kTile * I.tile) : min(kTile, I.ns - kTile * I.tile);
-    prefetch_l2(W + I.off + (int64_t)m * I.a0, (size_t)m * (I.a1 - I.a0) * sizeof(T));
-  }
-}
-
 // ---------------------------------------------------------------- blocks
 
 // Walks one warp's slabs of a block in the order the warp consumes them: the
@@ -357,7 +333,6 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
       ++prod;
       cursor_next<true>(pc, nlev, s_lev, items, warp, nw);
     }
-    prefetch_levels<T, true>(items, s_lev, 1, nlev, W);
     for (int L = 0; L < nlev; ++L) {
       if (L == nlev - 1 && threadIdx.x == 0) next_ticket = atomicAdd(sy.queue + 2, 1);
       const int i1 = s_lev[L + 1];
@@ -562,7 +537,6 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
       ++prod;
       cursor_next<false>(pc, nlev, s_lev, items, warp, nw);
     }
-    prefetch_levels<T, false>(items, s_lev, 1, nlev - 1, W);
     for (int L = 0; L < nlev; ++L) {
       if (L == nlev - 1 && threadIdx.x == 0) next_ticket = atomicAdd(sy.queue + 3, 1);
       const int i1 = s_lev[L + 1];
