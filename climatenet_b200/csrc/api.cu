@@ -114,7 +114,7 @@ void build_schedule(pdf_handle* h, int chunk, int cut_level, int upper_mode = 0,
   P.n_upper = (int)hp.upper_cols.size();
   P.perm = h->d.perm;
   P.rows_loc = upload(hp.rows_loc);
-  P.bidx = upload(hp.bidx.empty() ? std::vector<int>(kSlab, 0) : hp.bidx);
+  P.bidx = upload(hp.bidx.empty() ? std::vector<int>(kSlabMax, 0) : hp.bidx);
   P.child = upload(hp.child.empty() ? std::vector<int>(2, 0) : hp.child);
   P.max_cols = hp.max_block_cols;
   P.max_ext = hp.max_block_ext;

@@ -591,7 +591,7 @@ void build_sweep_plan(const Factor& f, int chunk, int cut_level, SweepPlan& plan
                                             f.sn_ns[s], f.sn_nr[s], tl, a, std::min(h, a + kBlockSpanB)));
           for (int i = 0; i < h; ++i)
             plan.bidx.push_back(i < nd ? -1 - (c0l + j0t + i) : plan.rows_loc[f.sn_roff[s] + i - nd]);
-          while (plan.bidx.size() % kSlab) plan.bidx.push_back(0);
+          while (plan.bidx.size() % kSlabMax) plan.bidx.push_back(0);
         }
     }
     bb.lev[bb.nlev] = (int)plan.bitem.size() - bb.item0;
@@ -694,7 +694,7 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
         if (!chk(it, nfi, "forward block items")) return false;
         const BlockItem& I = plan.fitem[it];
         const int m = std::min(kTile, I.ns + I.nr - kTile * I.tile), w = std::min((int)I.ns, kTile * I.tile + (int)kTile);
-        if ((I.off % kTilePad) != 0 || I.a0 % kSlab != 0 || I.a0 < 0 || I.a0 >= I.a1 || I.a1 > w) {
+        if ((I.off % kTilePad) != 0 || I.a0 % kSlabMax != 0 || I.a0 < 0 || I.a0 >= I.a1 || I.a1 > w) {
           err = "forward block item not aligned or out of its tile";
           return false;
         }
@@ -832,7 +832,7 @@ bool emulate_sweeps(const Factor& f, const SweepPlan& plan, const std::vector<do
         if (!chk(it, nbi, "backward block items")) return false;
         const BlockItem& I = plan.bitem[it];
         const int j0t = kTile * I.tile, nd = I.ns - j0t, mc = std::min(kTile, nd), h = nd + I.nr;
-        if ((I.off % kTilePad) != 0 || (I.idx0 % kSlab) != 0 || I.a0 % kSlab != 0 || I.a0 < 0 || I.a0 >= I.a1 ||
+        if ((I.off % kTilePad) != 0 || (I.idx0 % kSlabMax) != 0 || I.a0 % kSlabMax != 0 || I.a0 < 0 || I.a0 >= I.a1 ||
             I.a1 > h) {
           err = "backward block item not aligned or out of its tile";
           return false;

@@ -106,14 +106,18 @@ constexpr int kMaxBlockLevels = 16;
 constexpr int kMaxBlockCols = 1536;
 constexpr int kMaxBlockExt = 1024;
 constexpr int kMaxBlockItems = 768;  // work items per block and sweep (staged in shared memory)
-constexpr int kSlab = 16;  // columns (forward) / rows (backward) per bulk copy
+// columns (forward) / rows (backward) per bulk copy: 16 in FP64, 32 in FP32
+// (4 KB either way); item starts and the backward index lists are aligned to
+// the larger
+constexpr int kSlab = 16;
+constexpr int kSlabMax = 32;
 // A tile longer than its sweep's span (forward columns, backward rows) is
 // split into items of that span whose partial sums meet in atomics, so that
 // long tiles do not hold one warp while the others wait at the level
 // barrier.  Backward tiles run over the supernode's rows below it (often
 // several times its width), so their span is short: per level, the longest
 // warp's work comes within 1.3x of an even split on the 500 x 500 cloth.
-constexpr int kBlockSpanF = 128;  // multiples of kSlab
+constexpr int kBlockSpanF = 128;  // multiples of kSlabMax
 constexpr int kBlockSpanB = 32;
 
 struct SweepBlock {
@@ -128,13 +132,13 @@ struct SweepBlock {
 // One work item of a tile of a supernode inside a block: forward, rows
 // [32 tile, 32 tile + m) of W_s over its columns [a0, a1) of
 // w = min(ns, 32 tile + 32); backward, columns [32 tile, 32 tile + mc) over
-// its rows [a0, a1) of h = ns - 32 tile + nr.  a0 is a multiple of kSlab.
+// its rows [a0, a1) of h = ns - 32 tile + nr.  a0 is a multiple of kSlabMax.
 // The small fields are 16-bit (a block has at most kMaxBlockCols columns and
 // kMaxBlockExt ext rows), so that an item is 32 bytes of shared memory.
 struct BlockItem {
   int64_t off;   // tile offset in the forward (backward) tiled copy
   int roff;      // offset of the supernode's row set in Factor::rows (and rows_loc)
-  int idx0;      // backward: offset of the tile's row-index list in bidx (multiple of kSlab)
+  int idx0;      // backward: offset of the tile's row-index list in bidx (multiple of kSlabMax)
   int16_t c0l;   // first column of the supernode, relative to the block
   int16_t ns, nr;
   int16_t tile;
@@ -142,7 +146,7 @@ struct BlockItem {
   int16_t pad[2];
 };
 static_assert(sizeof(BlockItem) == 32, "BlockItem is 32 bytes");
-static_assert(kBlockSpanF % kSlab == 0 && kBlockSpanB % kSlab == 0, "items start on a slab");
+static_assert(kBlockSpanF % kSlabMax == 0 && kBlockSpanB % kSlabMax == 0, "items start on a slab");
 
 // An upper work item as the device reads it: the SweepTask with the fields
 // of its supernode it needs and its dependency targets per solve, so that one
@@ -176,7 +180,7 @@ struct SweepPlan {
   // per entry of Factor::rows of a block supernode: the row's place in the
   // block's shared vector (column - c0 inside the block, nc + ext index outside)
   std::vector<int> rows_loc;
-  // backward tiles of blocks: per row of the tile, padded to kSlab rows, where
+  // backward tiles of blocks: per row of the tile, padded to kSlabMax rows, where
   // its vector entry is: >= 0 the shared vector (x), < 0 the shared y slice
   // (entry -1 - k is column k of the block)
   std::vector<int> bidx;

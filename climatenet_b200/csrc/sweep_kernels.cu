@@ -49,14 +49,15 @@ constexpr int kTicketBatch = 2;
 constexpr int kSweepThreads = 256;
 constexpr int kBlockMaxThreads = 512;  // block kernels: up to 16 warps per CTA (at most 128 registers a thread)
 
-// Bulk-copy stages per warp: one slab (32 rows x kSlab columns, or kSlab rows
-// x 32 columns) each.  The deepest ring (at most kDeep stages, 16 KB per warp
-// in both precisions) with which the launch shape's CTAs fit an SM
+// Bulk-copy stages per warp: one slab (32 rows x kCols columns, or kCols rows
+// x 32 columns; 4 KB in both precisions) each.  The deepest ring (at most
+// kDeep stages) with which the launch shape's CTAs fit an SM
 // (DPlan::ring_f / ring_b, at least kMinRing).
 template <typename T>
 struct Stages {
-  static constexpr int kDeep = sizeof(T) == 8 ? 4 : 8;
-  static constexpr int kElems = kTile * kSlab;
+  static constexpr int kCols = sizeof(T) == 8 ? kSlab : kSlabMax;
+  static constexpr int kDeep = 4;
+  static constexpr int kElems = kTile * kCols;
 };
 constexpr int kMinRing = 2;
 
@@ -205,10 +206,10 @@ __device__ __forceinline__ void cursor_start(SlabCursor& c, int nlev, const int*
   cursor_settle<kFwd>(c, nlev, lev, items, warp);
 }
 
-template <bool kFwd>
+template <bool kFwd, int kCols>
 __device__ __forceinline__ void cursor_next(SlabCursor& c, int nlev, const int* lev, const BlockItem* items, int warp,
                                             int nw) {
-  c.j0 += kSlab;
+  c.j0 += kCols;
   if (c.j0 >= c.len) {
     c.it += nw;
     cursor_settle<kFwd>(c, nlev, lev, items, warp);
@@ -219,13 +220,14 @@ __device__ __forceinline__ void cursor_next(SlabCursor& c, int nlev, const int* 
 template <typename T, bool kFwd>
 __device__ __forceinline__ void issue_slab(const SlabCursor& c, const BlockItem* items, const T* W, const int* bidx,
                                            T* stage, int* istage, uint64_t* bar) {
+  constexpr int kCols = Stages<T>::kCols;
   const BlockItem I = items[c.it];
-  const int cnt = min(kSlab, c.len - c.j0);
+  const int cnt = min(kCols, c.len - c.j0);
   // forward: rows of the tile m, the slab = columns j0.. (column-major, m per
   // column); backward: columns of the tile mc, the slab = rows j0.. (mc per row)
   const int width = kFwd ? min(kTile, I.ns + I.nr - kTile * I.tile) : min(kTile, I.ns - kTile * I.tile);
   const uint32_t wbytes = round16((uint32_t)(width * cnt) * (uint32_t)sizeof(T));
-  const uint32_t ibytes = kFwd ? 0u : (uint32_t)(kSlab * sizeof(int));
+  const uint32_t ibytes = kFwd ? 0u : (uint32_t)(kCols * sizeof(int));
   mbar_expect_tx(bar, wbytes + ibytes);
   bulk_g2s(stage, W + I.off + (int64_t)width * c.j0, wbytes, bar);
   if (!kFwd) bulk_g2s(istage, bidx + I.idx0 + c.j0, ibytes, bar);
@@ -234,7 +236,7 @@ __device__ __forceinline__ void issue_slab(const SlabCursor& c, const BlockItem*
 // Shared-memory layout of the block kernels (the same computation on the
 // host in configure_solve): rings | index rings (backward) | mbarriers |
 // vector (3 planes of nc + next) | y slice (backward, 3 planes of nc) |
-// per-warp staging of 3 x kSlab vector entries (backward).
+// per-warp staging of 3 x kCols vector entries (backward).
 template <typename T>
 struct BlockSmem {
   T* ring;
@@ -254,16 +256,17 @@ __device__ __forceinline__ BlockSmem<T> block_smem(unsigned char* base, int nw, 
   size_t off = 0;
   s.ring = reinterpret_cast<T*>(base) + (size_t)warp * R * KE;
   off += (size_t)nw * R * KE * sizeof(T);
-  s.iring = reinterpret_cast<int*>(base + off) + (size_t)warp * R * kSlab;
-  if (!kFwd) off += (size_t)nw * R * kSlab * sizeof(int);
+  constexpr int kCols = Stages<T>::kCols;
+  s.iring = reinterpret_cast<int*>(base + off) + (size_t)warp * R * kCols;
+  if (!kFwd) off += (size_t)nw * R * kCols * sizeof(int);
   s.bar = reinterpret_cast<uint64_t*>(base + off) + warp * R;
   off += (size_t)nw * R * sizeof(uint64_t);
   s.sv = reinterpret_cast<T*>(base + off);
   off += 3 * (size_t)max_ld * sizeof(T);
   s.ys = reinterpret_cast<T*>(base + off);
   if (!kFwd) off += 3 * (size_t)max_cols * sizeof(T);
-  s.vstage = reinterpret_cast<T*>(base + off) + (size_t)warp * 3 * kSlab;
-  if (!kFwd) off += (size_t)nw * 3 * kSlab * sizeof(T);
+  s.vstage = reinterpret_cast<T*>(base + off) + (size_t)warp * 3 * kCols;
+  if (!kFwd) off += (size_t)nw * 3 * kCols * sizeof(T);
   s.items = reinterpret_cast<BlockItem*>(base + ((off + 15) & ~size_t(15)));
   return s;
 }
@@ -272,7 +275,8 @@ template <typename T, bool kFwd>
 size_t block_smem_bytes(int nw, int max_ld, int max_cols, int max_items, int R) {
   constexpr int KE = Stages<T>::kElems;
   size_t b = (size_t)nw * R * KE * sizeof(T) + (size_t)nw * R * sizeof(uint64_t) + 3 * (size_t)max_ld * sizeof(T);
-  if (!kFwd) b += (size_t)nw * R * kSlab * sizeof(int) + 3 * (size_t)max_cols * sizeof(T) + (size_t)nw * 3 * kSlab * sizeof(T);
+  constexpr int kCols = Stages<T>::kCols;
+  if (!kFwd) b += (size_t)nw * R * kCols * sizeof(int) + 3 * (size_t)max_cols * sizeof(T) + (size_t)nw * 3 * kCols * sizeof(T);
   return ((b + 15) & ~size_t(15)) + (size_t)max_items * sizeof(BlockItem);
 }
 
@@ -331,7 +335,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
       if (lane == 0) issue_slab<T, true>(pc, items, W, P.bidx, sm.ring + st * KE, nullptr, sm.bar + st);
       pending |= 1u << st;
       ++prod;
-      cursor_next<true>(pc, nlev, s_lev, items, warp, nw);
+      cursor_next<true, Stages<T>::kCols>(pc, nlev, s_lev, items, warp, nw);
     }
     for (int L = 0; L < nlev; ++L) {
       if (L == nlev - 1 && threadIdx.x == 0) next_ticket = atomicAdd(sy.queue + 2, 1);
@@ -347,7 +351,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
         const T* vx = sv + I.c0l;
         T ax = 0, ay = 0, az = 0;
 #pragma unroll 1
-        for (int j0 = I.a0; j0 < a1; j0 += kSlab) {
+        for (int j0 = I.a0; j0 < a1; j0 += Stages<T>::kCols) {
           const int st = cons % R;
           if (!failed && !mbar_wait_warp(sm.bar + st, (par >> st) & 1u, sy.max_spins)) {
             failed = true;
@@ -357,10 +361,10 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
             // nothing valid in this stage
           } else {
             const T* sp = sm.ring + st * KE;
-            const int cnt = min(kSlab, a1 - j0);
+            const int cnt = min(Stages<T>::kCols, a1 - j0);
             if (lane < m) {
 #pragma unroll
-              for (int u = 0; u < kSlab; ++u)
+              for (int u = 0; u < Stages<T>::kCols; ++u)
                 if (u < cnt) {
                   const T wv = sp[m * u + lane];
                   ax += wv * vx[j0 + u];
@@ -382,7 +386,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
             }
             pending |= 1u << st;
             ++prod;
-            cursor_next<true>(pc, nlev, s_lev, items, warp, nw);
+            cursor_next<true, Stages<T>::kCols>(pc, nlev, s_lev, items, warp, nw);
           }
         }
         if (row < I.ns) {
@@ -532,10 +536,10 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
     for (int k = 0; k < R && !pc.done(nlev) && !failed; ++k) {
       const int st = prod % R;
       if (lane == 0)
-        issue_slab<T, false>(pc, items, W, P.bidx, sm.ring + st * KE, sm.iring + st * kSlab, sm.bar + st);
+        issue_slab<T, false>(pc, items, W, P.bidx, sm.ring + st * KE, sm.iring + st * Stages<T>::kCols, sm.bar + st);
       pending |= 1u << st;
       ++prod;
-      cursor_next<false>(pc, nlev, s_lev, items, warp, nw);
+      cursor_next<false, Stages<T>::kCols>(pc, nlev, s_lev, items, warp, nw);
     }
     for (int L = 0; L < nlev; ++L) {
       if (L == nlev - 1 && threadIdx.x == 0) next_ticket = atomicAdd(sy.queue + 3, 1);
@@ -547,18 +551,18 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
         const int a1 = I.a1;
         T ax = 0, ay = 0, az = 0;
 #pragma unroll 1
-        for (int i0 = I.a0; i0 < a1; i0 += kSlab) {
+        for (int i0 = I.a0; i0 < a1; i0 += Stages<T>::kCols) {
           const int st = cons % R;
           if (!failed && !mbar_wait_warp(sm.bar + st, (par >> st) & 1u, sy.max_spins)) {
             failed = true;
             if (lane == 0) atomicOr(sy.err, 1);
           }
-          const int cnt = min(kSlab, a1 - i0);
+          const int cnt = min(Stages<T>::kCols, a1 - i0);
           const bool valid = (pending & (1u << st)) && !failed;
-          if (lane < kSlab) {
+          if (lane < Stages<T>::kCols) {
             T vx = 0, vy = 0, vz = 0;
             if (valid && lane < cnt) {
-              const int idx = sm.iring[st * kSlab + lane];
+              const int idx = sm.iring[st * Stages<T>::kCols + lane];
               if (idx < 0) {
                 const int k = -1 - idx;
                 vx = ys[k];
@@ -571,19 +575,19 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
               }
             }
             sm.vstage[lane] = vx;
-            sm.vstage[kSlab + lane] = vy;
-            sm.vstage[2 * kSlab + lane] = vz;
+            sm.vstage[Stages<T>::kCols + lane] = vy;
+            sm.vstage[2 * Stages<T>::kCols + lane] = vz;
           }
           __syncwarp();
           if (valid && lane < mc) {
             const T* sp = sm.ring + st * KE;
 #pragma unroll
-            for (int u = 0; u < kSlab; ++u)
+            for (int u = 0; u < Stages<T>::kCols; ++u)
               if (u < cnt) {
                 const T wv = sp[mc * u + lane];
                 ax += wv * sm.vstage[u];
-                ay += wv * sm.vstage[kSlab + u];
-                az += wv * sm.vstage[2 * kSlab + u];
+                ay += wv * sm.vstage[Stages<T>::kCols + u];
+                az += wv * sm.vstage[2 * Stages<T>::kCols + u];
               }
           }
           if (!failed) {
@@ -595,11 +599,11 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
           if (!pc.done(nlev) && !failed) {
             if (lane == 0) {
               fence_proxy_async();
-              issue_slab<T, false>(pc, items, W, P.bidx, sm.ring + st * KE, sm.iring + st * kSlab, sm.bar + st);
+              issue_slab<T, false>(pc, items, W, P.bidx, sm.ring + st * KE, sm.iring + st * Stages<T>::kCols, sm.bar + st);
             }
             pending |= 1u << st;
             ++prod;
-            cursor_next<false>(pc, nlev, s_lev, items, warp, nw);
+            cursor_next<false, Stages<T>::kCols>(pc, nlev, s_lev, items, warp, nw);
           }
         }
         if (lane < mc) {
