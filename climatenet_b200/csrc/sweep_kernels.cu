@@ -941,16 +941,26 @@ __global__ void k_solve_prep(int n, T* x, T* y, SweepSync sy) {
 
 // Persistent grid: as many CTAs as can be resident at once with this dynamic
 // shared memory (0 when the kernel does not fit).
+// The kernel's dynamic shared-memory limit is raised to the device's
+// opt-in maximum, not to this plan's need: the attribute belongs to the
+// kernel, shared by every handle of the process, and a later handle with a
+// smaller plan must not lower it under an earlier handle's launches (or the
+// launches captured in its graphs).
 template <typename K>
 int resident_ctas(K kernel, size_t smem, int threads = kSweepThreads) {
-  int dev = 0, sms = 148, per_sm = 0;
+  int dev = 0, sms = 148, per_sm = 0, optin = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if (smem > (size_t)optin) return 0;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
   return per_sm * sms;
 }
 

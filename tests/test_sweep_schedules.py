@@ -92,3 +92,22 @@ def test_schedule_rejects_values_outside_the_tuned_sets(oracle_run):
     q, v = g.state()
     assert rel_err(q, traj[3][0]) < REL and rel_err(v, traj[3][1]) < REL
     g.close()
+
+
+def test_handles_with_different_schedules_coexist(oracle_run):
+    """A kernel's shared-memory limit is process-wide: configuring a second
+    handle with a small plan must not break the first handle's larger one
+    (its direct launches and its captured graph)."""
+    s, traj, counts = oracle_run
+    p = abi.params(time_step=5e-3, iterations=20)
+    a = native.Simulation(s, p)
+    a.set_sweep_schedule(64, 7, 1, 0)  # one CTA of the largest blocks per SM
+    a.step(1)
+    b = native.Simulation(s, p)
+    b.set_sweep_schedule(64, 0, 1, 3)  # four CTAs of the smallest blocks per SM
+    b.step(1)
+    a.step(3)
+    q, v = a.state()
+    assert rel_err(q, traj[3][0]) < REL and rel_err(v, traj[3][1]) < REL
+    a.close()
+    b.close()
