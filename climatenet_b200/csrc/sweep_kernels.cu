@@ -952,8 +952,14 @@ int resident_ctas(K kernel, size_t smem, int threads = kSweepThreads) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  if (smem > (size_t)optin) return 0;
-  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, optin) != cudaSuccess) {
+  cudaFuncAttributes fa{};
+  if (cudaFuncGetAttributes(&fa, kernel) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  const int dyn_max = optin - (int)fa.sharedSizeBytes;  // static shared memory counts against the limit
+  if (smem > (size_t)dyn_max) return 0;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
