@@ -50,14 +50,15 @@ constexpr int kSweepThreads = 256;
 constexpr int kBlockMaxThreads = 512;  // block kernels: up to 16 warps per CTA (at most 128 registers a thread)
 
 // Bulk-copy stages per warp: one slab (32 rows x kCols columns, or kCols rows
-// x 32 columns; 4 KB in both precisions) each.  The deepest ring (at most
+// x 32 columns) each: 4 KB, except FP32 backward slabs of 16 rows (2 KB,
+// measured faster there: the per-row index staging is half as long).  The deepest ring (at most
 // kDeep stages) with which the launch shape's CTAs fit an SM
 // (DPlan::ring_f / ring_b, at least kMinRing).
-template <typename T>
+template <typename T, bool kFwd>
 struct Stages {
-  static constexpr int kCols = sizeof(T) == 8 ? kSlab : kSlabMax;
-  static constexpr int kDeep = 4;
+  static constexpr int kCols = (sizeof(T) == 4 && kFwd) ? kSlabMax : kSlab;
   static constexpr int kElems = kTile * kCols;
+  static constexpr int kDeep = kElems * sizeof(T) >= 4096 ? 4 : 8;
 };
 constexpr int kMinRing = 2;
 
@@ -220,7 +221,7 @@ __device__ __forceinline__ void cursor_next(SlabCursor& c, int nlev, const int* 
 template <typename T, bool kFwd>
 __device__ __forceinline__ void issue_slab(const SlabCursor& c, const BlockItem* items, const T* W, const int* bidx,
                                            T* stage, int* istage, uint64_t* bar) {
-  constexpr int kCols = Stages<T>::kCols;
+  constexpr int kCols = Stages<T, kFwd>::kCols;
   const BlockItem I = items[c.it];
   const int cnt = min(kCols, c.len - c.j0);
   // forward: rows of the tile m, the slab = columns j0.. (column-major, m per
@@ -251,12 +252,12 @@ struct BlockSmem {
 template <typename T, bool kFwd>
 __device__ __forceinline__ BlockSmem<T> block_smem(unsigned char* base, int nw, int warp, int max_ld, int max_cols,
                                                    int R) {
-  constexpr int KE = Stages<T>::kElems;
+  constexpr int KE = Stages<T, kFwd>::kElems;
   BlockSmem<T> s;
   size_t off = 0;
   s.ring = reinterpret_cast<T*>(base) + (size_t)warp * R * KE;
   off += (size_t)nw * R * KE * sizeof(T);
-  constexpr int kCols = Stages<T>::kCols;
+  constexpr int kCols = Stages<T, kFwd>::kCols;
   s.iring = reinterpret_cast<int*>(base + off) + (size_t)warp * R * kCols;
   if (!kFwd) off += (size_t)nw * R * kCols * sizeof(int);
   s.bar = reinterpret_cast<uint64_t*>(base + off) + warp * R;
@@ -273,9 +274,9 @@ __device__ __forceinline__ BlockSmem<T> block_smem(unsigned char* base, int nw, 
 
 template <typename T, bool kFwd>
 size_t block_smem_bytes(int nw, int max_ld, int max_cols, int max_items, int R) {
-  constexpr int KE = Stages<T>::kElems;
+  constexpr int KE = Stages<T, kFwd>::kElems;
   size_t b = (size_t)nw * R * KE * sizeof(T) + (size_t)nw * R * sizeof(uint64_t) + 3 * (size_t)max_ld * sizeof(T);
-  constexpr int kCols = Stages<T>::kCols;
+  constexpr int kCols = Stages<T, kFwd>::kCols;
   if (!kFwd) b += (size_t)nw * R * kCols * sizeof(int) + 3 * (size_t)max_cols * sizeof(T) + (size_t)nw * 3 * kCols * sizeof(T);
   return ((b + 15) & ~size_t(15)) + (size_t)max_items * sizeof(BlockItem);
 }
@@ -292,7 +293,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
                                                                     int n, SweepSync sy) {
   trace_stamp(sy.trace, DTrace::kSolve);
   griddep_launch_dependents();  // the first upper level may start on SMs this sweep leaves
-  constexpr int KE = Stages<T>::kElems;
+  constexpr int KE = Stages<T, true>::kElems;
   const int R = P.ring_f;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int s_ticket;
@@ -335,7 +336,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
       if (lane == 0) issue_slab<T, true>(pc, items, W, P.bidx, sm.ring + st * KE, nullptr, sm.bar + st);
       pending |= 1u << st;
       ++prod;
-      cursor_next<true, Stages<T>::kCols>(pc, nlev, s_lev, items, warp, nw);
+      cursor_next<true, Stages<T, true>::kCols>(pc, nlev, s_lev, items, warp, nw);
     }
     for (int L = 0; L < nlev; ++L) {
       if (L == nlev - 1 && threadIdx.x == 0) next_ticket = atomicAdd(sy.queue + 2, 1);
@@ -351,7 +352,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
         const T* vx = sv + I.c0l;
         T ax = 0, ay = 0, az = 0;
 #pragma unroll 1
-        for (int j0 = I.a0; j0 < a1; j0 += Stages<T>::kCols) {
+        for (int j0 = I.a0; j0 < a1; j0 += Stages<T, true>::kCols) {
           const int st = cons % R;
           if (!failed && !mbar_wait_warp(sm.bar + st, (par >> st) & 1u, sy.max_spins)) {
             failed = true;
@@ -361,10 +362,10 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
             // nothing valid in this stage
           } else {
             const T* sp = sm.ring + st * KE;
-            const int cnt = min(Stages<T>::kCols, a1 - j0);
+            const int cnt = min(Stages<T, true>::kCols, a1 - j0);
             if (lane < m) {
 #pragma unroll
-              for (int u = 0; u < Stages<T>::kCols; ++u)
+              for (int u = 0; u < Stages<T, true>::kCols; ++u)
                 if (u < cnt) {
                   const T wv = sp[m * u + lane];
                   ax += wv * vx[j0 + u];
@@ -386,7 +387,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
             }
             pending |= 1u << st;
             ++prod;
-            cursor_next<true, Stages<T>::kCols>(pc, nlev, s_lev, items, warp, nw);
+            cursor_next<true, Stages<T, true>::kCols>(pc, nlev, s_lev, items, warp, nw);
           }
         }
         if (row < I.ns) {
@@ -470,7 +471,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
                                                                      const T* __restrict__ y, const T* x, int n,
                                                                      SweepSync sy, WriteBack wb) {
   griddep_launch_dependents();
-  constexpr int KE = Stages<T>::kElems;
+  constexpr int KE = Stages<T, false>::kElems;
   const int R = P.ring_b;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   __shared__ int s_ticket;
@@ -536,10 +537,10 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
     for (int k = 0; k < R && !pc.done(nlev) && !failed; ++k) {
       const int st = prod % R;
       if (lane == 0)
-        issue_slab<T, false>(pc, items, W, P.bidx, sm.ring + st * KE, sm.iring + st * Stages<T>::kCols, sm.bar + st);
+        issue_slab<T, false>(pc, items, W, P.bidx, sm.ring + st * KE, sm.iring + st * Stages<T, false>::kCols, sm.bar + st);
       pending |= 1u << st;
       ++prod;
-      cursor_next<false, Stages<T>::kCols>(pc, nlev, s_lev, items, warp, nw);
+      cursor_next<false, Stages<T, false>::kCols>(pc, nlev, s_lev, items, warp, nw);
     }
     for (int L = 0; L < nlev; ++L) {
       if (L == nlev - 1 && threadIdx.x == 0) next_ticket = atomicAdd(sy.queue + 3, 1);
@@ -551,18 +552,18 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
         const int a1 = I.a1;
         T ax = 0, ay = 0, az = 0;
 #pragma unroll 1
-        for (int i0 = I.a0; i0 < a1; i0 += Stages<T>::kCols) {
+        for (int i0 = I.a0; i0 < a1; i0 += Stages<T, false>::kCols) {
           const int st = cons % R;
           if (!failed && !mbar_wait_warp(sm.bar + st, (par >> st) & 1u, sy.max_spins)) {
             failed = true;
             if (lane == 0) atomicOr(sy.err, 1);
           }
-          const int cnt = min(Stages<T>::kCols, a1 - i0);
+          const int cnt = min(Stages<T, false>::kCols, a1 - i0);
           const bool valid = (pending & (1u << st)) && !failed;
-          if (lane < Stages<T>::kCols) {
+          if (lane < Stages<T, false>::kCols) {
             T vx = 0, vy = 0, vz = 0;
             if (valid && lane < cnt) {
-              const int idx = sm.iring[st * Stages<T>::kCols + lane];
+              const int idx = sm.iring[st * Stages<T, false>::kCols + lane];
               if (idx < 0) {
                 const int k = -1 - idx;
                 vx = ys[k];
@@ -575,19 +576,19 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
               }
             }
             sm.vstage[lane] = vx;
-            sm.vstage[Stages<T>::kCols + lane] = vy;
-            sm.vstage[2 * Stages<T>::kCols + lane] = vz;
+            sm.vstage[Stages<T, false>::kCols + lane] = vy;
+            sm.vstage[2 * Stages<T, false>::kCols + lane] = vz;
           }
           __syncwarp();
           if (valid && lane < mc) {
             const T* sp = sm.ring + st * KE;
 #pragma unroll
-            for (int u = 0; u < Stages<T>::kCols; ++u)
+            for (int u = 0; u < Stages<T, false>::kCols; ++u)
               if (u < cnt) {
                 const T wv = sp[mc * u + lane];
                 ax += wv * sm.vstage[u];
-                ay += wv * sm.vstage[Stages<T>::kCols + u];
-                az += wv * sm.vstage[2 * Stages<T>::kCols + u];
+                ay += wv * sm.vstage[Stages<T, false>::kCols + u];
+                az += wv * sm.vstage[2 * Stages<T, false>::kCols + u];
               }
           }
           if (!failed) {
@@ -599,11 +600,11 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
           if (!pc.done(nlev) && !failed) {
             if (lane == 0) {
               fence_proxy_async();
-              issue_slab<T, false>(pc, items, W, P.bidx, sm.ring + st * KE, sm.iring + st * Stages<T>::kCols, sm.bar + st);
+              issue_slab<T, false>(pc, items, W, P.bidx, sm.ring + st * KE, sm.iring + st * Stages<T, false>::kCols, sm.bar + st);
             }
             pending |= 1u << st;
             ++prod;
-            cursor_next<false, Stages<T>::kCols>(pc, nlev, s_lev, items, warp, nw);
+            cursor_next<false, Stages<T, false>::kCols>(pc, nlev, s_lev, items, warp, nw);
           }
         }
         if (lane < mc) {
@@ -978,7 +979,7 @@ int ring_for(K kernel, const DPlan& P, int warps, int ctas, int* smem) {
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int max_ld = std::max(1, P.max_cols + P.max_ext);
-  for (int R = Stages<T>::kDeep; R >= kMinRing; --R) {
+  for (int R = Stages<T, kFwd>::kDeep; R >= kMinRing; --R) {
     const size_t b = block_smem_bytes<T, kFwd>(warps, max_ld, std::max(1, P.max_cols), std::max(1, P.max_items), R);
     if (resident_ctas(kernel, b, 32 * warps) >= ctas * sms) {
       *smem = (int)b;
