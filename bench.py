@@ -263,7 +263,12 @@ def train_warm_start(args, tolerance, candidates=4):
     return w, info
 
 
-def make_sim(s, pk, iterations, precision, weights=None, device=0, tolerance=0.0):
+# --schedule: solve schedules pinned per precision (profiler runs; otherwise
+# the autotuner at create chooses)
+SCHEDULE = {}
+
+
+def make_sim(s, pk, iterations, precision, weights=None, device=0, tolerance=0.0, pin=True):
     from climatenet_b200 import abi, native
     p = dict(pk)
     p["iterations"] = iterations
@@ -274,6 +279,8 @@ def make_sim(s, pk, iterations, precision, weights=None, device=0, tolerance=0.0
     prm = abi.params(**p)
     prm.device = device
     sim = native.Simulation(s, prm)
+    if pin and precision in SCHEDULE:
+        sim.set_sweep_schedule(*SCHEDULE[precision])
     if weights is not None:
         sim.mlp_set_weights(weights)
     return sim
@@ -351,11 +358,13 @@ def e2e_steps(sim, steps, barrier, dist, world, start):
     return whole_job_rate(world, steps, 1e3 * max_over_ranks(time.perf_counter() - t0, dist))
 
 
-# DRAM bytes (read + write) of one global solve of the 500 x 500 cloth,
-# forward + backward sweep, from ncu's dram__bytes_read.sum +
-# dram__bytes_write.sum (a profiler is needed to count them, so they cannot be
-# measured inside this run); None for other workloads.
-SOLVE_TRAFFIC_500 = {True: None, False: None}
+# DRAM bytes (read + write) of one global solve of the 500 x 500 cloth, all
+# launches of the forward and backward sweeps and the write-back, summed from
+# ncu's dram__bytes_read.sum + dram__bytes_write.sum (a profiler is needed to
+# count them, so they cannot be measured inside this run), with the
+# schedule the autotuner picks for this scene; None for other workloads.
+# Keyed by FP32 (True) / FP64 (False).
+SOLVE_TRAFFIC_500 = {True: 430255616, False: 832374272}
 
 
 def roofline(sim, fp32, n=None):
@@ -425,7 +434,7 @@ def batch_measurement(args, barrier, dist, rank, world, device):
     a = SimpleNamespace(**dict(vars(args), workload="batch"))
     t0 = time.time()
     s, pk = workload(a, rank, world)
-    sim = make_sim(s, pk, PLAIN_ITERATIONS, "fp32", device=device)
+    sim = make_sim(s, pk, PLAIN_ITERATIONS, "fp32", device=device, pin=False)
     setup_s = time.time() - t0
     start = stretch_start(s, pk, device)
     rec, ms, launches, clk, _, _ = run_arm(sim, args.steps, args.warmup, start, barrier, dist, 1, device)
@@ -450,7 +459,14 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-instance batch measurement")
+    ap.add_argument("--schedule", action="append", default=[],
+                    help="PREC=CHUNK,CUT,MODE,SHAPE (PREC fp64 or fp32): pin the cloth arms' solve schedule "
+                         "instead of autotuning it at create (for runs under a profiler, which distorts the "
+                         "autotuner's timings)")
     args = ap.parse_args()
+    for spec in args.schedule:
+        prec, vals = spec.split("=")
+        SCHEDULE[prec] = tuple(int(t) for t in vals.split(","))
     args.warmup = max(3, args.warmup)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
