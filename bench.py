@@ -381,12 +381,12 @@ def roofline(sim, fp32, n=None):
             "factor_elements_stored": st.factor_nnz, "nnz_L": st.factor_nnz_true}
 
 
-def stretch_start(s, pk, device):
-    """The state every arm's measured stretch starts from: PREROLL steps of
+def stretch_start(s, pk, device, preroll=PREROLL):
+    """The state every arm's measured stretch starts from: `preroll` steps of
     the reference's method (FP64, 20 PD iterations) from the scene's initial
     state.  Fixed, whatever --warmup is."""
     sim = make_sim(s, pk, PLAIN_ITERATIONS, "fp64", device=device)
-    sim.step(PREROLL)
+    sim.step(preroll)
     st = sim.state()
     sim.close()
     return st
@@ -447,6 +447,61 @@ def batch_measurement(args, barrier, dist, rank, world, device):
     return rec
 
 
+# the warm start's own workload starts 5 cm above the sphere: its stretch
+# begins once the layers lie on it (0.3 s)
+PREROLL5 = 150
+
+
+def warm_start_config5(args, barrier, dist, device):
+    """The learned warm start on its own workload: two 256 x 256 layers 1 mm
+    apart (1.2 m side) 5 cm above a sphere of radius 0.4 m rotating about z at
+    1 rad/s, mu 0.6, self-collision (1 mm), dt 2e-3 (131,072 vertices).  The
+    network is trained on contacts logged from the 64-instance batch scene
+    (300 steps, 60 PD iterations, cold start): another workload, as the
+    warm start is meant to be used.  Over a fixed stretch (PREROLL5 steps of
+    the reference's method from the initial state, so that the layers lie on
+    the sphere, then `steps` timed steps)
+    tau5 is the mean Alart-Curnier residual the reference's method (FP64, 20
+    PD iterations) reaches; the cold and the warm-started FP32 + refinement
+    solvers then iterate to tau5 (cap 60) over the same stretch.  The warm arm
+    is measured whatever the cold-start judge (10 steps from the stretch's
+    start) decides; its verdict is reported beside it."""
+    from climatenet_b200 import abi, scenes, warmstart
+    s5, pk5, _ = scenes.workload(5)
+    start = stretch_start(s5, pk5, device, preroll=PREROLL5)
+    sim = make_sim(s5, pk5, PLAIN_ITERATIONS, "fp64", device=device, pin=False)
+    rec_r = run_arm(sim, args.steps, args.warmup, start, barrier, dist, 1, device)[0]
+    sim.close()
+    tol = rec_r["mean_residual"]
+    cap = 3 * PLAIN_ITERATIONS if tol > 0 else PLAIN_ITERATIONS
+    sb, _, pkb = scenes.batch_scene(n_instances=64, seed=4)
+    pkb = dict(pkb)
+    pkb["iterations"] = 60
+    t0 = time.time()
+    X, T = warmstart.collect(sb, abi.params(**pkb), steps=300, capacity=12_000_000)
+    t1 = time.time()
+    w, tinfo = warmstart.train(X, T, epochs=10, batch=8192, lr=2e-3, seed=1)
+    t2 = time.time()
+    pj = dict(pk5)
+    pj["precision"] = abi.PDF_FP32_REFINE
+    verdict = warmstart.judge(s5, pj, w, tol, steps=10, warmup=args.warmup, cap=cap, start=start)
+    out = {"workload": "two 256x256 layers 1 mm apart over a sphere R=0.4 m rotating at 1 rad/s, mu=0.6, "
+                       "self-collision 1 mm, dt=2e-3 (131,072 vertices)",
+           "stretch": "steps %d-%d" % (PREROLL5 + 1, PREROLL5 + args.steps),
+           "reference_method_fp64_fixed20": {k: rec_r[k] for k in ("steps_per_s", "mean_residual")},
+           "tolerance": tol, "iteration_cap": cap,
+           "training": dict(tinfo, data="64-instance batch scene, 300 steps, 60 PD iterations, cold start",
+                            collect_s=t1 - t0, train_s=t2 - t1, epochs=10),
+           "judge": verdict}
+    for name, weights in (("cold", None), ("warm", w)):
+        sim = make_sim(s5, pk5, cap, "fp32", weights, device=device, tolerance=tol, pin=False)
+        rec = run_arm(sim, args.steps, args.warmup, start, barrier, dist, 1, device)[0]
+        sim.close()
+        out[name] = {k: rec[k] for k in ("steps_per_s", "ms_per_step", "mean_pd_iterations", "mean_residual")}
+    out["warm_over_cold_steps_per_s"] = out["warm"]["steps_per_s"] / out["cold"]["steps_per_s"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -459,6 +514,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the 64-instance batch measurement")
+    ap.add_argument("--no-warm-config", action="store_true",
+                    help="skip the learned warm start on its own workload (two 256 x 256 layers)")
     ap.add_argument("--schedule", action="append", default=[],
                     help="PREC=CHUNK,CUT,MODE,SHAPE (PREC fp64 or fp32): pin the cloth arms' solve schedule "
                          "instead of autotuning it at create (for runs under a profiler, which distorts the "
@@ -568,6 +625,10 @@ def main():
     batch = None
     if args.workload == "cloth" and not args.no_batch:
         batch = batch_measurement(args, barrier, dist, rank, world, local)
+    # the warm start's own workload: one GPU only (the scaling runs skip it)
+    warm5 = None
+    if args.workload == "cloth" and args.arm == "same-residual" and not args.no_warm_config and world == 1:
+        warm5 = warm_start_config5(args, barrier, dist, local)
     if dist is not None:
         dist.barrier()
     if rank == 0:
@@ -603,6 +664,8 @@ def main():
         line.update(line_extra)
         if batch is not None:
             line["batch"] = batch
+        if warm5 is not None:
+            line["warm_start_own_workload"] = warm5
         if not args.no_cpu and world == 1:
             line["cpu_baseline"] = cpu_baseline(args, args.cpu_steps, start)
         print(json.dumps(line), flush=True)

@@ -120,15 +120,23 @@ def cold_stretch(scene, params, tolerance, start, steps=10, cap=60):
 def train(X, T, epochs=30, batch=4096, lr=2e-3, seed=0, device=0):
     """Weights (raw features in, raw forces out) and the losses, trained on the GPU.
 
-    Returns (weights, info) with info = dict(train_loss, val_loss, variance):
-    the losses are those of the standardised problem (1.0 = predicting the
-    mean)."""
+    Returns (weights, info) with info = dict(train_loss, val_loss, samples,
+    dropped_nonfinite): the losses are those of the standardised problem (1.0
+    = predicting the mean); samples with a non-finite feature or target are
+    not trained on and are counted in dropped_nonfinite."""
+    X = np.asarray(X)
+    T = np.asarray(T)
+    # samples with a non-finite feature or target are left out (and counted)
+    keep = np.isfinite(X).all(1) & np.isfinite(T).all(1)
+    dropped = int(len(X) - keep.sum())
+    if dropped:
+        X, T = X[keep], T[keep]
     mu, sigma, nu, tau = normalisation(X, T)
     Xn = ((np.asarray(X, dtype=np.float64) - mu) / sigma).astype(np.float32)
     Tn = ((np.asarray(T, dtype=np.float64) - nu) / tau).astype(np.float32)
     w0 = native.mlp_init(seed)
     w, tl, vl = native.mlp_fit(w0, Xn, Tn, epochs=epochs, batch=batch, lr=lr, seed=seed, device=device)
-    return fold(w, mu, sigma, nu, tau), dict(train_loss=tl, val_loss=vl, samples=len(X))
+    return fold(w, mu, sigma, nu, tau), dict(train_loss=tl, val_loss=vl, samples=len(X), dropped_nonfinite=dropped)
 
 
 def judge(scene, params, weights, tolerance, steps=10, warmup=3, cap=60, start=None):
