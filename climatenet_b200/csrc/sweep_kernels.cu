@@ -47,20 +47,22 @@ namespace pdfb {
 
 constexpr int kTicketBatch = 2;
 constexpr int kSweepThreads = 256;
-constexpr int kBlockMaxThreads = 512;  // block kernels: up to 16 warps per CTA (at most 128 registers a thread)
+// block kernels: up to 17 warps per CTA (16 consumers and the producer), at
+// most 112 registers a thread, so that 2 CTAs of 9 warps fit an SM
+constexpr int kBlockMaxThreads = 576;
 
-// Bulk-copy stages per warp: one slab (32 rows x kCols columns, or kCols rows
-// x 32 columns) each: 4 KB, except FP32 backward slabs of 16 rows (2 KB,
-// measured faster there: the per-row index staging is half as long).  The deepest ring (at most
-// kDeep stages) with which the launch shape's CTAs fit an SM
-// (DPlan::ring_f / ring_b, at least kMinRing).
+// A slab (one bulk copy) is 32 rows x kCols columns (forward) or kCols rows
+// x 32 columns (backward): 4 KB, except FP32 backward slabs of 16 rows (2 KB,
+// measured faster there: the per-row index staging is half as long).  A
+// block kernel's CTA has a ring of R slots (DPlan::ring_f / ring_b): the
+// largest in [kMinSlots, kMaxSlots] with which the launch shape's CTAs fit an
+// SM.
 template <typename T, bool kFwd>
 struct Stages {
   static constexpr int kCols = (sizeof(T) == 4 && kFwd) ? kSlabMax : kSlab;
   static constexpr int kElems = kTile * kCols;
-  static constexpr int kDeep = kElems * sizeof(T) >= 4096 ? 4 : 8;
 };
-constexpr int kMinRing = 2;
+constexpr int kMinSlots = 4, kMaxSlots = 64;
 
 __device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long* p) {
   return *reinterpret_cast<const volatile unsigned long long*>(p);
@@ -175,117 +177,132 @@ __device__ __forceinline__ void stage_items(BlockItem* dst, const BlockItem* src
 // end, after every thread has read the current one.
 
 // ---------------------------------------------------------------- blocks
+//
+// A block kernel's CTA is `ncw` consumer warps and one producer warp.  The
+// producer's lane 0 streams the block's factor, slab by slab in item order
+// (the items are stored level by level), into a ring of R slots shared by
+// the CTA: slot q % R holds the block's slab number q (counted over the CTA's
+// lifetime), its `full` mbarrier completes when the copy lands, its `empty`
+// mbarrier when the consuming warp has read it.  Consumer warps take the
+// items of each level round-robin, wait for each slab's `full` barrier, and
+// release it; levels are separated by a barrier among the consumers only, so
+// the producer keeps copying the next levels' slabs while a level finishes.
+// A slab is only copied into a slot whose previous slab (issued R slabs
+// earlier, so of the same or an earlier level) was read, which its consumer
+// reaches without waiting on anything issued later: the pipeline cannot
+// stall on itself.  Every wait is bounded.
 
-// Walks one warp's slabs of a block in the order the warp consumes them: the
-// items of level L taken round-robin by warp (item0 + lev[L] + warp, + nw,
-// ...), the slabs of an item in order.  Every lane holds the same cursor.
-struct SlabCursor {
-  int L, it, j0, len;  // j0: next slab's first column (forward) / row (backward); len: the item's end
-  __device__ __forceinline__ bool done(int nlev) const { return L >= nlev; }
-};
-
-// items and lev are the block's item descriptors and level offsets staged in
-// shared memory (indices relative to the block's first item)
-template <bool kFwd>
-__device__ __forceinline__ void cursor_settle(SlabCursor& c, int nlev, const int* lev, const BlockItem* items,
-                                              int warp) {
-  while (c.L < nlev && c.it >= lev[c.L + 1]) {
-    ++c.L;
-    if (c.L < nlev) c.it = lev[c.L] + warp;
-  }
-  if (c.L < nlev) {
-    c.j0 = items[c.it].a0;
-    c.len = items[c.it].a1;
-  }
-}
-
-template <bool kFwd>
-__device__ __forceinline__ void cursor_start(SlabCursor& c, int nlev, const int* lev, const BlockItem* items,
-                                             int warp) {
-  c.L = 0;
-  c.it = lev[0] + warp;
-  cursor_settle<kFwd>(c, nlev, lev, items, warp);
-}
-
-template <bool kFwd, int kCols>
-__device__ __forceinline__ void cursor_next(SlabCursor& c, int nlev, const int* lev, const BlockItem* items, int warp,
-                                            int nw) {
-  c.j0 += kCols;
-  if (c.j0 >= c.len) {
-    c.it += nw;
-    cursor_settle<kFwd>(c, nlev, lev, items, warp);
-  }
-}
-
-// lane 0: the bulk copy of the slab at cursor c into stage `st`
-template <typename T, bool kFwd>
-__device__ __forceinline__ void issue_slab(const SlabCursor& c, const BlockItem* items, const T* W, const int* bidx,
-                                           T* stage, int* istage, uint64_t* bar) {
-  constexpr int kCols = Stages<T, kFwd>::kCols;
-  const BlockItem I = items[c.it];
-  const int cnt = min(kCols, c.len - c.j0);
-  // forward: rows of the tile m, the slab = columns j0.. (column-major, m per
-  // column); backward: columns of the tile mc, the slab = rows j0.. (mc per row)
-  const int width = kFwd ? min(kTile, I.ns + I.nr - kTile * I.tile) : min(kTile, I.ns - kTile * I.tile);
-  const uint32_t wbytes = round16((uint32_t)(width * cnt) * (uint32_t)sizeof(T));
-  const uint32_t ibytes = kFwd ? 0u : (uint32_t)(kCols * sizeof(int));
-  mbar_expect_tx(bar, wbytes + ibytes);
-  bulk_g2s(stage, W + I.off + (int64_t)width * c.j0, wbytes, bar);
-  if (!kFwd) bulk_g2s(istage, bidx + I.idx0 + c.j0, ibytes, bar);
-}
-
-// Shared-memory layout of the block kernels (the same computation on the
-// host in configure_solve): rings | index rings (backward) | mbarriers |
-// vector (3 planes of nc + next) | y slice (backward, 3 planes of nc) |
-// per-warp staging of 3 x kCols vector entries (backward).
+// the ring's parts in shared memory
 template <typename T>
 struct BlockSmem {
-  T* ring;
-  int* iring;
-  uint64_t* bar;
+  T* ring;          // R slots of Stages::kElems
+  int* iring;       // backward: R slots of kCols row indices
+  uint64_t* full;   // R
+  uint64_t* empty;  // R
   T* sv;
   T* ys;
-  T* vstage;
+  T* vstage;        // this consumer warp's 3 x kCols vector entries (backward)
   BlockItem* items;
+  int* slab0;       // first slab of each item, relative to the block
 };
 
 template <typename T, bool kFwd>
-__device__ __forceinline__ BlockSmem<T> block_smem(unsigned char* base, int nw, int warp, int max_ld, int max_cols,
-                                                   int R) {
-  constexpr int KE = Stages<T, kFwd>::kElems;
+__device__ __forceinline__ BlockSmem<T> block_smem(unsigned char* base, int ncw, int warp, int max_ld, int max_cols,
+                                                   int max_items, int R) {
+  constexpr int KE = Stages<T, kFwd>::kElems, kCols = Stages<T, kFwd>::kCols;
   BlockSmem<T> s;
   size_t off = 0;
-  s.ring = reinterpret_cast<T*>(base) + (size_t)warp * R * KE;
-  off += (size_t)nw * R * KE * sizeof(T);
-  constexpr int kCols = Stages<T, kFwd>::kCols;
-  s.iring = reinterpret_cast<int*>(base + off) + (size_t)warp * R * kCols;
-  if (!kFwd) off += (size_t)nw * R * kCols * sizeof(int);
-  s.bar = reinterpret_cast<uint64_t*>(base + off) + warp * R;
-  off += (size_t)nw * R * sizeof(uint64_t);
+  s.ring = reinterpret_cast<T*>(base);
+  off += (size_t)R * KE * sizeof(T);
+  s.iring = reinterpret_cast<int*>(base + off);
+  if (!kFwd) off += (size_t)R * kCols * sizeof(int);
+  s.full = reinterpret_cast<uint64_t*>(base + off);
+  s.empty = s.full + R;
+  off += 2 * (size_t)R * sizeof(uint64_t);
   s.sv = reinterpret_cast<T*>(base + off);
   off += 3 * (size_t)max_ld * sizeof(T);
   s.ys = reinterpret_cast<T*>(base + off);
   if (!kFwd) off += 3 * (size_t)max_cols * sizeof(T);
-  s.vstage = reinterpret_cast<T*>(base + off) + (size_t)warp * 3 * kCols;
-  if (!kFwd) off += (size_t)nw * 3 * kCols * sizeof(T);
-  s.items = reinterpret_cast<BlockItem*>(base + ((off + 15) & ~size_t(15)));
+  s.vstage = reinterpret_cast<T*>(base + off) + (size_t)min(warp, ncw - 1) * 3 * kCols;
+  if (!kFwd) off += (size_t)ncw * 3 * kCols * sizeof(T);
+  off = (off + 15) & ~size_t(15);
+  s.items = reinterpret_cast<BlockItem*>(base + off);
+  off += (size_t)max_items * sizeof(BlockItem);
+  s.slab0 = reinterpret_cast<int*>(base + off);
   return s;
 }
 
 template <typename T, bool kFwd>
-size_t block_smem_bytes(int nw, int max_ld, int max_cols, int max_items, int R) {
-  constexpr int KE = Stages<T, kFwd>::kElems;
-  size_t b = (size_t)nw * R * KE * sizeof(T) + (size_t)nw * R * sizeof(uint64_t) + 3 * (size_t)max_ld * sizeof(T);
-  constexpr int kCols = Stages<T, kFwd>::kCols;
-  if (!kFwd) b += (size_t)nw * R * kCols * sizeof(int) + 3 * (size_t)max_cols * sizeof(T) + (size_t)nw * 3 * kCols * sizeof(T);
-  return ((b + 15) & ~size_t(15)) + (size_t)max_items * sizeof(BlockItem);
+size_t block_smem_bytes(int ncw, int max_ld, int max_cols, int max_items, int R) {
+  constexpr int KE = Stages<T, kFwd>::kElems, kCols = Stages<T, kFwd>::kCols;
+  size_t b = (size_t)R * KE * sizeof(T) + 2 * (size_t)R * sizeof(uint64_t) + 3 * (size_t)max_ld * sizeof(T);
+  if (!kFwd) b += (size_t)R * kCols * sizeof(int) + 3 * (size_t)max_cols * sizeof(T) + (size_t)ncw * 3 * kCols * sizeof(T);
+  return ((b + 15) & ~size_t(15)) + (size_t)max_items * (sizeof(BlockItem) + sizeof(int));
 }
 
-// After an mbarrier wait gave up: wait (bounded) for every copy this warp
-// still has in flight, so that none lands after the CTA exits.
-__device__ __forceinline__ void drain_stages(uint64_t* bar, uint32_t pending, uint32_t par, int R, int max_spins) {
-  for (int k = 0; k < R; ++k)
-    if (pending & (1u << k)) mbar_wait(bar + k, (par >> k) & 1u, max_spins);
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+// barrier 1 among the consumer warps only (the producer does not take part)
+__device__ __forceinline__ void consumers_sync(int nthreads) {
+  asm volatile("bar.sync 1, %0;" ::"r"(nthreads) : "memory");
+}
+
+// Warp 0: slab0[k] = the number of slabs of items [0, k) (kCols columns /
+// rows each, from a0); returns the total (every lane).
+template <int kCols>
+__device__ __forceinline__ int scan_slabs(const BlockItem* items, int nitems, int* slab0, int lane) {
+  int total = 0;
+  for (int k0 = 0; k0 < nitems; k0 += 32) {
+    const int k = k0 + lane;
+    const int c = k < nitems ? (items[k].a1 - items[k].a0 + kCols - 1) / kCols : 0;
+    int incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (k < nitems) slab0[k] = total + incl - c;
+    total += __shfl_sync(0xffffffffu, incl, 31);
+  }
+  return total;
+}
+
+// Producer lane: copies the block's slabs, numbered from q_base, into the
+// ring in item order; returns the number after the last one issued and sets
+// ok false when a wait for a free slot gave up.
+template <typename T, bool kFwd>
+__device__ __forceinline__ int produce_block(const BlockSmem<T>& sm, const BlockItem* items, int nitems, int q_base,
+                                             int R, const T* W, const int* bidx, int max_spins, bool& ok) {
+  constexpr int KE = Stages<T, kFwd>::kElems, kCols = Stages<T, kFwd>::kCols;
+  int q = q_base;
+  for (int it = 0; it < nitems; ++it) {
+    const BlockItem I = items[it];
+    // forward: rows of the tile m, a slab = columns j0.. (column-major, m per
+    // column); backward: columns of the tile mc, a slab = rows j0.. (mc per row)
+    const int width = kFwd ? min(kTile, I.ns + I.nr - kTile * I.tile) : min(kTile, I.ns - kTile * I.tile);
+    for (int j0 = I.a0; j0 < I.a1; j0 += kCols, ++q) {
+      const int slot = q % R, use = q / R;
+      if (use > 0 && !mbar_wait(sm.empty + slot, (use - 1) & 1, max_spins)) {
+        ok = false;
+        return q;
+      }
+      fence_proxy_async();  // the consumer's reads of the slot before the copy over it
+      const int cnt = min(kCols, I.a1 - j0);
+      const uint32_t wbytes = round16((uint32_t)(width * cnt) * (uint32_t)sizeof(T));
+      const uint32_t ibytes = kFwd ? 0u : (uint32_t)(kCols * sizeof(int));
+      mbar_expect_tx(sm.full + slot, wbytes + ibytes);
+      bulk_g2s(sm.ring + (size_t)slot * KE, W + I.off + (int64_t)width * j0, wbytes, sm.full + slot);
+      if (!kFwd) bulk_g2s(sm.iring + (size_t)slot * kCols, bidx + I.idx0 + j0, ibytes, sm.full + slot);
+    }
+  }
+  return q;
+}
+
+// After a wait gave up: the producer waits (bounded) for the copies it
+// issued into each slot's last use, so that none lands after the CTA exits.
+__device__ __forceinline__ void drain_ring(uint64_t* full, int q_end, int R, int max_spins) {
+  for (int q = max(0, q_end - R); q < q_end; ++q) mbar_wait(full + q % R, (q / R) & 1, max_spins);
 }
 
 template <typename T>
@@ -293,22 +310,30 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
                                                                     int n, SweepSync sy) {
   trace_stamp(sy.trace, DTrace::kSolve);
   griddep_launch_dependents();  // the first upper level may start on SMs this sweep leaves
-  constexpr int KE = Stages<T, true>::kElems;
+  constexpr int KE = Stages<T, true>::kElems, kCols = Stages<T, true>::kCols;
   const int R = P.ring_f;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ int s_ticket;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const BlockSmem<T> sm = block_smem<T, true>(smem_raw, nw, warp, P.max_cols + P.max_ext, P.max_cols, R);
+  __shared__ int s_ticket, s_nslab, s_failed;
   __shared__ int s_lev[kMaxBlockLevels + 1];
-  if (lane == 0)
-    for (int k = 0; k < R; ++k) mbar_init(sm.bar + k, 1);
-  fence_mbar_init();
-  __syncwarp();
-  uint32_t par = 0, pending = 0;  // per stage: wait parity, fill in flight
-  int prod = 0, cons = 0;         // slabs issued / consumed by this warp
-  bool failed = false;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, ncw = (blockDim.x >> 5) - 1;
+  const bool producer = warp == ncw;
+  const BlockSmem<T> sm =
+      block_smem<T, true>(smem_raw, ncw, warp, P.max_cols + P.max_ext, P.max_cols, P.max_items, R);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < R; ++k) {
+      mbar_init(sm.full + k, 1);
+      mbar_init(sm.empty + k, 1);
+    }
+    fence_mbar_init();
+  }
+  int q_base = 0;       // the CTA's slabs before this block
+  int q_issued = 0;     // producer lane 0: slabs issued
+  bool failed = false;  // a bounded wait gave up (this thread's view)
   int next_ticket = 0;  // thread 0
-  if (threadIdx.x == 0) s_ticket = atomicAdd(sy.queue + 2, 1);
+  if (threadIdx.x == 0) {
+    s_ticket = atomicAdd(sy.queue + 2, 1);
+    s_failed = 0;
+  }
   __syncthreads();
   for (;;) {
     const int bi = s_ticket;
@@ -328,87 +353,88 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
     if (threadIdx.x <= nlev) s_lev[threadIdx.x] = B.lev[threadIdx.x];
     cp_async_wait_all();
     __syncthreads();
-    const BlockItem* items = sm.items;
-    SlabCursor pc;
-    cursor_start<true>(pc, nlev, s_lev, items, warp);
-    for (int k = 0; k < R && !pc.done(nlev) && !failed; ++k) {
-      const int st = prod % R;
-      if (lane == 0) issue_slab<T, true>(pc, items, W, P.bidx, sm.ring + st * KE, nullptr, sm.bar + st);
-      pending |= 1u << st;
-      ++prod;
-      cursor_next<true, Stages<T, true>::kCols>(pc, nlev, s_lev, items, warp, nw);
+    if (warp == 0) {
+      const int t = scan_slabs<kCols>(sm.items, nitems, sm.slab0, lane);
+      if (lane == 0) s_nslab = t;
     }
-    for (int L = 0; L < nlev; ++L) {
-      if (L == nlev - 1 && threadIdx.x == 0) next_ticket = atomicAdd(sy.queue + 2, 1);
-      const int i1 = s_lev[L + 1];
-#pragma unroll 1
-      for (int it = s_lev[L] + warp; it < i1; it += nw) {
-        const BlockItem I = items[it];
-        const int m = min(kTile, I.ns + I.nr - kTile * I.tile);
-        const int w = min((int)I.ns, kTile * I.tile + kTile);
-        const int a1 = I.a1;
-        const int row = kTile * I.tile + lane;
-        const int loc = (row >= I.ns && row < I.ns + I.nr) ? P.rows_loc[I.roff + row - I.ns] : -1;
-        const T* vx = sv + I.c0l;
-        T ax = 0, ay = 0, az = 0;
-#pragma unroll 1
-        for (int j0 = I.a0; j0 < a1; j0 += Stages<T, true>::kCols) {
-          const int st = cons % R;
-          if (!failed && !mbar_wait_warp(sm.bar + st, (par >> st) & 1u, sy.max_spins)) {
-            failed = true;
-            if (lane == 0) atomicOr(sy.err, 1);
-          }
-          if (!(pending & (1u << st)) || failed) {
-            // nothing valid in this stage
-          } else {
-            const T* sp = sm.ring + st * KE;
-            const int cnt = min(Stages<T, true>::kCols, a1 - j0);
-            if (lane < m) {
-#pragma unroll
-              for (int u = 0; u < Stages<T, true>::kCols; ++u)
-                if (u < cnt) {
-                  const T wv = sp[m * u + lane];
-                  ax += wv * vx[j0 + u];
-                  ay += wv * vx[ld + j0 + u];
-                  az += wv * vx[2 * ld + j0 + u];
-                }
-            }
-          }
-          if (!failed) {
-            par ^= 1u << st;
-            pending &= ~(1u << st);
-          }
-          __syncwarp();
-          ++cons;
-          if (!pc.done(nlev) && !failed) {
-            if (lane == 0) {
-              fence_proxy_async();
-              issue_slab<T, true>(pc, items, W, P.bidx, sm.ring + st * KE, nullptr, sm.bar + st);
-            }
-            pending |= 1u << st;
-            ++prod;
-            cursor_next<true, Stages<T, true>::kCols>(pc, nlev, s_lev, items, warp, nw);
-          }
-        }
-        if (row < I.ns) {
-          const int64_t o = (int64_t)c0b + I.c0l + row;
-          if (I.a0 == 0 && a1 == w) {
-            y[o] = ax;
-            y[o + n] = ay;
-            y[o + 2 * (int64_t)n] = az;
-          } else {  // one span of a split tile (y starts at zero)
-            atomicAdd(y + o, ax);
-            atomicAdd(y + o + n, ay);
-            atomicAdd(y + o + 2 * (int64_t)n, az);
-          }
-        } else if (loc >= 0) {
-          atomicAdd(sv + loc, -ax);
-          atomicAdd(sv + ld + loc, -ay);
-          atomicAdd(sv + 2 * ld + loc, -az);
+    __syncthreads();
+    const BlockItem* items = sm.items;
+    if (producer) {
+      int q_end = q_base;
+      bool ok = !failed;
+      if (lane == 0 && ok) {
+        q_end = produce_block<T, true>(sm, items, nitems, q_base, R, W, P.bidx, sy.max_spins, ok);
+        q_issued = q_end;
+        if (!ok) {
+          atomicOr(sy.err, 1);
+          s_failed = 1;
         }
       }
-      __syncthreads();
+      failed = failed || !__shfl_sync(0xffffffffu, ok, 0);
+    } else {
+      for (int L = 0; L < nlev; ++L) {
+        if (L == nlev - 1 && threadIdx.x == 0) next_ticket = atomicAdd(sy.queue + 2, 1);
+        const int i1 = s_lev[L + 1];
+#pragma unroll 1
+        for (int it = s_lev[L] + warp; it < i1; it += ncw) {
+          const BlockItem I = items[it];
+          const int m = min(kTile, I.ns + I.nr - kTile * I.tile);
+          const int w = min((int)I.ns, kTile * I.tile + kTile);
+          const int a1 = I.a1;
+          const int row = kTile * I.tile + lane;
+          const int loc = (row >= I.ns && row < I.ns + I.nr) ? P.rows_loc[I.roff + row - I.ns] : -1;
+          const T* vx = sv + I.c0l;
+          T ax = 0, ay = 0, az = 0;
+          int q = q_base + sm.slab0[it];
+#pragma unroll 1
+          for (int j0 = I.a0; j0 < a1; j0 += kCols, ++q) {
+            const int slot = q % R;
+            if (!failed && !mbar_wait_warp(sm.full + slot, (q / R) & 1, sy.max_spins)) {
+              failed = true;
+              if (lane == 0) {
+                atomicOr(sy.err, 1);
+                s_failed = 1;
+              }
+            }
+            if (!failed) {
+              const T* sp = sm.ring + (size_t)slot * KE;
+              const int cnt = min(kCols, a1 - j0);
+              if (lane < m) {
+#pragma unroll
+                for (int u = 0; u < kCols; ++u)
+                  if (u < cnt) {
+                    const T wv = sp[m * u + lane];
+                    ax += wv * vx[j0 + u];
+                    ay += wv * vx[ld + j0 + u];
+                    az += wv * vx[2 * ld + j0 + u];
+                  }
+              }
+              __syncwarp();
+              if (lane == 0) mbar_arrive(sm.empty + slot);  // the slot is read
+            }
+          }
+          if (row < I.ns) {
+            const int64_t o = (int64_t)c0b + I.c0l + row;
+            if (I.a0 == 0 && a1 == w) {
+              y[o] = ax;
+              y[o + n] = ay;
+              y[o + 2 * (int64_t)n] = az;
+            } else {  // one span of a split tile (y starts at zero)
+              atomicAdd(y + o, ax);
+              atomicAdd(y + o + n, ay);
+              atomicAdd(y + o + 2 * (int64_t)n, az);
+            }
+          } else if (loc >= 0) {
+            atomicAdd(sv + loc, -ax);
+            atomicAdd(sv + ld + loc, -ay);
+            atomicAdd(sv + 2 * ld + loc, -az);
+          }
+        }
+        consumers_sync(ncw * 32);
+      }
     }
+    q_base += s_nslab;
+    __syncthreads();  // every level done, every slab of the block issued
     // the ext rows' updates, once per block
     for (int e = threadIdx.x; e < B.next; e += blockDim.x) {
       const int64_t r = P.rows[B.ext0 + e];
@@ -416,11 +442,13 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
       atomicAdd(b + r + n, sv[ld + nc + e]);
       atomicAdd(b + r + 2 * (int64_t)n, sv[2 * ld + nc + e]);
     }
-    __syncthreads();  // the shared vector is free, every thread has read s_ticket
+    __syncthreads();  // the shared vector is free, every thread has read s_ticket and s_nslab
     if (threadIdx.x == 0) s_ticket = next_ticket;
     __syncthreads();
   }
-  if (failed) drain_stages(sm.bar, pending, par, R, sy.max_spins);
+  // a wait gave up somewhere: every copy the producer issued lands before
+  // the CTA exits
+  if (s_failed && producer && lane == 0) drain_ring(sm.full, q_issued, R, sy.max_spins);
 }
 
 // v[perm[k]] = x_k (mode 0) or += x_k (mode 1) and q^k = q_n + dt v for the
@@ -428,7 +456,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
 // thread takes kWbCols columns a pass and issues every load of the pass
 // before its stores, so that a pass costs two dependent memory round trips
 // (the permutation, then the vertex gathers) instead of several per column.
-constexpr int kWbCols = 4;
+constexpr int kWbCols = 2;
 constexpr int kExtBatch = 4;  // ext rows per thread whose indices are loaded together
 template <typename T>
 __device__ __forceinline__ void write_back_columns(const T* sv, int ld, int nc, const int* __restrict__ perm,
@@ -471,22 +499,29 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
                                                                      const T* __restrict__ y, const T* x, int n,
                                                                      SweepSync sy, WriteBack wb) {
   griddep_launch_dependents();
-  constexpr int KE = Stages<T, false>::kElems;
+  constexpr int KE = Stages<T, false>::kElems, kCols = Stages<T, false>::kCols;
   const int R = P.ring_b;
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  __shared__ int s_ticket;
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  const BlockSmem<T> sm = block_smem<T, false>(smem_raw, nw, warp, P.max_cols + P.max_ext, P.max_cols, R);
+  __shared__ int s_ticket, s_nslab, s_failed;
   __shared__ int s_lev[kMaxBlockLevels + 1];
-  if (lane == 0)
-    for (int k = 0; k < R; ++k) mbar_init(sm.bar + k, 1);
-  fence_mbar_init();
-  __syncwarp();
-  uint32_t par = 0, pending = 0;
-  int prod = 0, cons = 0;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, ncw = (blockDim.x >> 5) - 1;
+  const bool producer = warp == ncw;
+  const BlockSmem<T> sm =
+      block_smem<T, false>(smem_raw, ncw, warp, P.max_cols + P.max_ext, P.max_cols, P.max_items, R);
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < R; ++k) {
+      mbar_init(sm.full + k, 1);
+      mbar_init(sm.empty + k, 1);
+    }
+    fence_mbar_init();
+  }
+  int q_base = 0, q_issued = 0;
   bool failed = false;
   int next_ticket = 0;  // thread 0
-  if (threadIdx.x == 0) s_ticket = atomicAdd(sy.queue + 3, 1);
+  if (threadIdx.x == 0) {
+    s_ticket = atomicAdd(sy.queue + 3, 1);
+    s_failed = 0;
+  }
   __syncthreads();
   for (;;) {
     const int bi = s_ticket;
@@ -531,103 +566,103 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
     for (int k = threadIdx.x; k < nc; k += blockDim.x) sv[k] = sv[ld + k] = sv[2 * ld + k] = T(0);
     cp_async_wait_all();
     __syncthreads();
-    const BlockItem* items = sm.items;
-    SlabCursor pc;
-    cursor_start<false>(pc, nlev, s_lev, items, warp);
-    for (int k = 0; k < R && !pc.done(nlev) && !failed; ++k) {
-      const int st = prod % R;
-      if (lane == 0)
-        issue_slab<T, false>(pc, items, W, P.bidx, sm.ring + st * KE, sm.iring + st * Stages<T, false>::kCols, sm.bar + st);
-      pending |= 1u << st;
-      ++prod;
-      cursor_next<false, Stages<T, false>::kCols>(pc, nlev, s_lev, items, warp, nw);
+    if (warp == 0) {
+      const int t = scan_slabs<kCols>(sm.items, nitems, sm.slab0, lane);
+      if (lane == 0) s_nslab = t;
     }
-    for (int L = 0; L < nlev; ++L) {
-      if (L == nlev - 1 && threadIdx.x == 0) next_ticket = atomicAdd(sy.queue + 3, 1);
-      const int i1 = s_lev[L + 1];
-#pragma unroll 1
-      for (int it = s_lev[L] + warp; it < i1; it += nw) {
-        const BlockItem I = items[it];
-        const int j0t = kTile * I.tile, nd = I.ns - j0t, mc = min(kTile, nd), h = nd + I.nr;
-        const int a1 = I.a1;
-        T ax = 0, ay = 0, az = 0;
-#pragma unroll 1
-        for (int i0 = I.a0; i0 < a1; i0 += Stages<T, false>::kCols) {
-          const int st = cons % R;
-          if (!failed && !mbar_wait_warp(sm.bar + st, (par >> st) & 1u, sy.max_spins)) {
-            failed = true;
-            if (lane == 0) atomicOr(sy.err, 1);
-          }
-          const int cnt = min(Stages<T, false>::kCols, a1 - i0);
-          const bool valid = (pending & (1u << st)) && !failed;
-          if (lane < Stages<T, false>::kCols) {
-            T vx = 0, vy = 0, vz = 0;
-            if (valid && lane < cnt) {
-              const int idx = sm.iring[st * Stages<T, false>::kCols + lane];
-              if (idx < 0) {
-                const int k = -1 - idx;
-                vx = ys[k];
-                vy = ys[nc + k];
-                vz = ys[2 * nc + k];
-              } else {
-                vx = -sv[idx];
-                vy = -sv[ld + idx];
-                vz = -sv[2 * ld + idx];
-              }
-            }
-            sm.vstage[lane] = vx;
-            sm.vstage[Stages<T, false>::kCols + lane] = vy;
-            sm.vstage[2 * Stages<T, false>::kCols + lane] = vz;
-          }
-          __syncwarp();
-          if (valid && lane < mc) {
-            const T* sp = sm.ring + st * KE;
-#pragma unroll
-            for (int u = 0; u < Stages<T, false>::kCols; ++u)
-              if (u < cnt) {
-                const T wv = sp[mc * u + lane];
-                ax += wv * sm.vstage[u];
-                ay += wv * sm.vstage[Stages<T, false>::kCols + u];
-                az += wv * sm.vstage[2 * Stages<T, false>::kCols + u];
-              }
-          }
-          if (!failed) {
-            par ^= 1u << st;
-            pending &= ~(1u << st);
-          }
-          __syncwarp();
-          ++cons;
-          if (!pc.done(nlev) && !failed) {
-            if (lane == 0) {
-              fence_proxy_async();
-              issue_slab<T, false>(pc, items, W, P.bidx, sm.ring + st * KE, sm.iring + st * Stages<T, false>::kCols, sm.bar + st);
-            }
-            pending |= 1u << st;
-            ++prod;
-            cursor_next<false, Stages<T, false>::kCols>(pc, nlev, s_lev, items, warp, nw);
-          }
-        }
-        if (lane < mc) {
-          T* s = sv + I.c0l + j0t + lane;
-          if (I.a0 == 0 && a1 == h) {
-            s[0] = ax;
-            s[ld] = ay;
-            s[2 * ld] = az;
-          } else {  // one span of a split tile
-            atomicAdd(s, ax);
-            atomicAdd(s + ld, ay);
-            atomicAdd(s + 2 * ld, az);
-          }
+    __syncthreads();
+    const BlockItem* items = sm.items;
+    if (producer) {
+      bool ok = !failed;
+      if (lane == 0 && ok) {
+        q_issued = produce_block<T, false>(sm, items, nitems, q_base, R, W, P.bidx, sy.max_spins, ok);
+        if (!ok) {
+          atomicOr(sy.err, 1);
+          s_failed = 1;
         }
       }
-      __syncthreads();
+      failed = failed || !__shfl_sync(0xffffffffu, ok, 0);
+    } else {
+      for (int L = 0; L < nlev; ++L) {
+        if (L == nlev - 1 && threadIdx.x == 0) next_ticket = atomicAdd(sy.queue + 3, 1);
+        const int i1 = s_lev[L + 1];
+#pragma unroll 1
+        for (int it = s_lev[L] + warp; it < i1; it += ncw) {
+          const BlockItem I = items[it];
+          const int j0t = kTile * I.tile, nd = I.ns - j0t, mc = min(kTile, nd), h = nd + I.nr;
+          const int a1 = I.a1;
+          T ax = 0, ay = 0, az = 0;
+          int q = q_base + sm.slab0[it];
+#pragma unroll 1
+          for (int i0 = I.a0; i0 < a1; i0 += kCols, ++q) {
+            const int slot = q % R;
+            if (!failed && !mbar_wait_warp(sm.full + slot, (q / R) & 1, sy.max_spins)) {
+              failed = true;
+              if (lane == 0) {
+                atomicOr(sy.err, 1);
+                s_failed = 1;
+              }
+            }
+            if (failed) continue;
+            const int cnt = min(kCols, a1 - i0);
+            if (lane < kCols) {
+              T vx = 0, vy = 0, vz = 0;
+              if (lane < cnt) {
+                const int idx = sm.iring[(size_t)slot * kCols + lane];
+                if (idx < 0) {
+                  const int k = -1 - idx;
+                  vx = ys[k];
+                  vy = ys[nc + k];
+                  vz = ys[2 * nc + k];
+                } else {
+                  vx = -sv[idx];
+                  vy = -sv[ld + idx];
+                  vz = -sv[2 * ld + idx];
+                }
+              }
+              sm.vstage[lane] = vx;
+              sm.vstage[kCols + lane] = vy;
+              sm.vstage[2 * kCols + lane] = vz;
+            }
+            __syncwarp();
+            if (lane < mc) {
+              const T* sp = sm.ring + (size_t)slot * KE;
+#pragma unroll
+              for (int u = 0; u < kCols; ++u)
+                if (u < cnt) {
+                  const T wv = sp[mc * u + lane];
+                  ax += wv * sm.vstage[u];
+                  ay += wv * sm.vstage[kCols + u];
+                  az += wv * sm.vstage[2 * kCols + u];
+                }
+            }
+            __syncwarp();  // the slot and the staged entries are read
+            if (lane == 0) mbar_arrive(sm.empty + slot);
+          }
+          if (lane < mc) {
+            T* s = sv + I.c0l + j0t + lane;
+            if (I.a0 == 0 && a1 == h) {
+              s[0] = ax;
+              s[ld] = ay;
+              s[2 * ld] = az;
+            } else {  // one span of a split tile
+              atomicAdd(s, ax);
+              atomicAdd(s + ld, ay);
+              atomicAdd(s + 2 * ld, az);
+            }
+          }
+        }
+        consumers_sync(ncw * 32);
+      }
     }
+    q_base += s_nslab;
+    __syncthreads();  // every level done, every slab of the block issued
     if (!failed) write_back_columns(sv, ld, nc, P.perm + c0b, wb);
-    __syncthreads();  // the shared vectors are free, every thread has read s_ticket
+    __syncthreads();  // the shared vectors are free, every thread has read s_ticket and s_nslab
     if (threadIdx.x == 0) s_ticket = next_ticket;
     __syncthreads();
   }
-  if (failed) drain_stages(sm.bar, pending, par, R, sy.max_spins);
+  if (s_failed && producer && lane == 0) drain_ring(sm.full, q_issued, R, sy.max_spins);
   griddep_wait();  // a CTA without a block completes after the launch before it too
 }
 
@@ -979,17 +1014,18 @@ int resident_ctas(K kernel, size_t smem, int threads = kSweepThreads) {
   return per_sm * sms;
 }
 
-// The deepest ring (kMinRing .. kDeep stages per warp) with which `ctas`
-// CTAs of `warps` warps of this block kernel are resident per SM; 0 if none.
+// The largest ring (kMinSlots .. kMaxSlots slots per CTA) with which `ctas`
+// CTAs of `warps` consumer warps and the producer warp of this block kernel
+// are resident per SM; 0 if none.
 template <typename T, bool kFwd, typename K>
 int ring_for(K kernel, const DPlan& P, int warps, int ctas, int* smem) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int max_ld = std::max(1, P.max_cols + P.max_ext);
-  for (int R = Stages<T, kFwd>::kDeep; R >= kMinRing; --R) {
+  for (int R = kMaxSlots; R >= kMinSlots; --R) {
     const size_t b = block_smem_bytes<T, kFwd>(warps, max_ld, std::max(1, P.max_cols), std::max(1, P.max_items), R);
-    if (resident_ctas(kernel, b, 32 * warps) >= ctas * sms) {
+    if (resident_ctas(kernel, b, 32 * (warps + 1)) >= ctas * sms) {
       *smem = (int)b;
       return R;
     }
@@ -1007,8 +1043,8 @@ bool configure_solve(DPlan& P, int shape) {
   P.ring_f = ring_for<T, true>(k_block_forward<T>, P, warps, ctas, &P.smem_f);
   P.ring_b = ring_for<T, false>(k_block_backward<T>, P, warps, ctas, &P.smem_b);
   if (!P.ring_f || !P.ring_b) return false;
-  const int rf = resident_ctas(k_block_forward<T>, P.smem_f, 32 * warps);
-  const int rb = resident_ctas(k_block_backward<T>, P.smem_b, 32 * warps);
+  const int rf = resident_ctas(k_block_forward<T>, P.smem_f, 32 * (warps + 1));
+  const int rb = resident_ctas(k_block_backward<T>, P.smem_b, 32 * (warps + 1));
   P.grid_bf = std::max(1, std::min(rf, std::max(1, P.nblk)));
   P.grid_bb = std::max(1, std::min(rb, std::max(1, P.nblk)));
   P.grid_uf = std::max(1, resident_ctas(k_upper_forward<T>, 0));
@@ -1041,7 +1077,7 @@ template <typename T>
 void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* Wb, T* b, T* y, T* x, int n,
                          SweepSync sy, WriteBack wb, cudaEvent_t* marks) {
   // marks (optional): 4 events recorded between the five launches
-  k_block_forward<T><<<P.grid_bf, 32 * P.block_warps, P.smem_f, st>>>(P, Wf, b, y, n, sy);
+  k_block_forward<T><<<P.grid_bf, 32 * (P.block_warps + 1), P.smem_f, st>>>(P, Wf, b, y, n, sy);
   if (marks) cudaEventRecord(marks[0], st);
   if (P.upper_mode == 1) {
     const int wpc = kSweepThreads / 32;
@@ -1066,7 +1102,7 @@ void launch_solve_sweeps(cudaStream_t st, const DPlan& P, const T* Wf, const T* 
     k_upper_backward<T><<<P.grid_ub, kSweepThreads, 0, st>>>(P, Wb, y, x, n, sy);
   }
   if (marks) cudaEventRecord(marks[2], st);
-  launch_dependent(k_block_backward<T>, P.grid_bb, 32 * P.block_warps, (size_t)P.smem_b, st, P, Wb,
+  launch_dependent(k_block_backward<T>, P.grid_bb, 32 * (P.block_warps + 1), (size_t)P.smem_b, st, P, Wb,
                    static_cast<const T*>(y), static_cast<const T*>(x), n, sy, wb);
   if (marks) cudaEventRecord(marks[3], st);
   launch_dependent(k_solve_post<T>, std::max(1, std::min(148 * 4, (P.n_upper + 255) / 256)), 256, 0, st, P, x, y, n,
