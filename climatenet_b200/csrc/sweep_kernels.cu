@@ -190,7 +190,12 @@ __device__ __forceinline__ void stage_items(BlockItem* dst, const BlockItem* src
 // A slab is only copied into a slot whose previous slab (issued R slabs
 // earlier, so of the same or an earlier level) was read, which its consumer
 // reaches without waiting on anything issued later: the pipeline cannot
-// stall on itself.  Every wait is bounded.
+// stall on itself.  A consumer may reach a slot two uses ahead of the copy
+// in it (its slab belongs to a warp that is ahead of the one reading the
+// slot's previous slab), where a parity wait on `full` would mistake an
+// earlier phase for its own; so the producer posts the use number of each
+// slot (`use`) before the copy, and a consumer waits for its use number
+// first, then for `full`.  Every wait is bounded.
 
 // the ring's parts in shared memory
 template <typename T>
@@ -199,6 +204,7 @@ struct BlockSmem {
   int* iring;       // backward: R slots of kCols row indices
   uint64_t* full;   // R
   uint64_t* empty;  // R
+  int* use;         // R: the use number of the copy issued into each slot (-1: none yet)
   T* sv;
   T* ys;
   T* vstage;        // this consumer warp's 3 x kCols vector entries (backward)
@@ -219,6 +225,8 @@ __device__ __forceinline__ BlockSmem<T> block_smem(unsigned char* base, int ncw,
   s.full = reinterpret_cast<uint64_t*>(base + off);
   s.empty = s.full + R;
   off += 2 * (size_t)R * sizeof(uint64_t);
+  s.use = reinterpret_cast<int*>(base + off);
+  off += (size_t)R * sizeof(uint64_t);
   s.sv = reinterpret_cast<T*>(base + off);
   off += 3 * (size_t)max_ld * sizeof(T);
   s.ys = reinterpret_cast<T*>(base + off);
@@ -235,9 +243,26 @@ __device__ __forceinline__ BlockSmem<T> block_smem(unsigned char* base, int ncw,
 template <typename T, bool kFwd>
 size_t block_smem_bytes(int ncw, int max_ld, int max_cols, int max_items, int R) {
   constexpr int KE = Stages<T, kFwd>::kElems, kCols = Stages<T, kFwd>::kCols;
-  size_t b = (size_t)R * KE * sizeof(T) + 2 * (size_t)R * sizeof(uint64_t) + 3 * (size_t)max_ld * sizeof(T);
+  size_t b = (size_t)R * KE * sizeof(T) + 3 * (size_t)R * sizeof(uint64_t) + 3 * (size_t)max_ld * sizeof(T);
   if (!kFwd) b += (size_t)R * kCols * sizeof(int) + 3 * (size_t)max_cols * sizeof(T) + (size_t)ncw * 3 * kCols * sizeof(T);
   return ((b + 15) & ~size_t(15)) + (size_t)max_items * (sizeof(BlockItem) + sizeof(int));
+}
+
+// A consumer warp's wait for slab q: its slot's use number posted, then the
+// slot's `full` barrier (bounded; false when either wait gave up).
+__device__ __forceinline__ bool wait_slab(const int* use, uint64_t* full, int q, int R, int max_spins) {
+  const int slot = q % R, u = q / R;
+  int ok = 1;
+  if ((threadIdx.x & 31) == 0) {
+    ok = 0;
+    for (int k = 0; k < max_spins; ++k)
+      if (*reinterpret_cast<const volatile int*>(use + slot) == u) {
+        ok = 1;
+        break;
+      }
+  }
+  if (!__shfl_sync(0xffffffffu, ok, 0)) return false;
+  return mbar_wait_warp(full + slot, u & 1, max_spins);
 }
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
@@ -288,6 +313,8 @@ __device__ __forceinline__ int produce_block(const BlockSmem<T>& sm, const Block
         return q;
       }
       fence_proxy_async();  // the consumer's reads of the slot before the copy over it
+      // the slot's `full` barrier has completed every phase before this use
+      *reinterpret_cast<volatile int*>(sm.use + slot) = use;
       const int cnt = min(kCols, I.a1 - j0);
       const uint32_t wbytes = round16((uint32_t)(width * cnt) * (uint32_t)sizeof(T));
       const uint32_t ibytes = kFwd ? 0u : (uint32_t)(kCols * sizeof(int));
@@ -323,6 +350,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
     for (int k = 0; k < R; ++k) {
       mbar_init(sm.full + k, 1);
       mbar_init(sm.empty + k, 1);
+      sm.use[k] = -1;
     }
     fence_mbar_init();
   }
@@ -389,7 +417,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_forward(DPlan P, 
 #pragma unroll 1
           for (int j0 = I.a0; j0 < a1; j0 += kCols, ++q) {
             const int slot = q % R;
-            if (!failed && !mbar_wait_warp(sm.full + slot, (q / R) & 1, sy.max_spins)) {
+            if (!failed && !wait_slab(sm.use, sm.full, q, R, sy.max_spins)) {
               failed = true;
               if (lane == 0) {
                 atomicOr(sy.err, 1);
@@ -512,6 +540,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
     for (int k = 0; k < R; ++k) {
       mbar_init(sm.full + k, 1);
       mbar_init(sm.empty + k, 1);
+      sm.use[k] = -1;
     }
     fence_mbar_init();
   }
@@ -596,7 +625,7 @@ __global__ void __launch_bounds__(kBlockMaxThreads, 1) k_block_backward(DPlan P,
 #pragma unroll 1
           for (int i0 = I.a0; i0 < a1; i0 += kCols, ++q) {
             const int slot = q % R;
-            if (!failed && !mbar_wait_warp(sm.full + slot, (q / R) & 1, sy.max_spins)) {
+            if (!failed && !wait_slab(sm.use, sm.full, q, R, sy.max_spins)) {
               failed = true;
               if (lane == 0) {
                 atomicOr(sy.err, 1);
