@@ -65,6 +65,9 @@ constexpr int kRecords = 64;  // step records in flight before the oldest is har
 constexpr int kChunkCandidates[3] = {32, 64, 128};
 constexpr int kCutCandidates = 8;  // cut levels 0 .. 7
 constexpr int kBlockShape = 1;     // block kernels: 2 CTAs of 8 warps per SM
+// the launch shapes tried at every cut level and mode (2 CTAs of 8 consumer
+// warps, 4 CTAs of 4 per SM); the others only at the best of those
+constexpr int kStageOneShapes[2] = {1, 3};
 // polls of a dependency counter before a sweep gives up (each poll sleeps
 // about 32 ns): far above any legitimate wait
 constexpr int kMaxSpins = 1 << 22;
@@ -567,9 +570,9 @@ void launch_solve_with(pdf_handle* h, const SweepSync& sy, T* b, T* y, T* x, con
 
 // Schedule autotuner: times the global solve of this scene's factor with
 // each candidate cut level and both upper modes (work-item width 64, block
-// kernels at 2 CTAs of 8 warps per SM where they fit), then with each launch
-// shape of the block kernels at the best cut level and mode, then with each
-// work-item width, and keeps the fastest.  The right-hand side is
+// kernels at 2 CTAs of 8 or 4 CTAs of 4 consumer warps per SM where they
+// fit), then with each launch shape of the block kernels at the best cut
+// level and mode, then with each work-item width, and keeps the fastest.  The right-hand side is
 // zero (the sweeps read the same data and wait on the same dependencies
 // whatever the values); v and q^k, which the solve writes, are restored.
 void autotune_schedule(pdf_handle* h) {
@@ -614,16 +617,32 @@ void autotune_schedule(pdf_handle* h) {
   double cut_ms[2][kCutCandidates] = {};
   int cut_shape[2][kCutCandidates] = {};
   for (int cut = 0; cut < kCutCandidates; ++cut)
-    for (int mode = 0; mode < 2; ++mode) {
-      const double ms = time_plan(kChunk, cut, mode, kBlockShape, false);
-      cut_ms[mode][cut] = ms;
-      cut_shape[mode][cut] = h->d.plan.block_shape;
-      if (ms > 0. && ms < best) {
-        best = ms;
-        best_cut = cut;
-        best_mode = mode;
+    for (int mode = 0; mode < 2; ++mode)
+      for (int sh : kStageOneShapes) {
+        const double ms = time_plan(kChunk, cut, mode, sh, true);
+        if (ms > 0. && (cut_ms[mode][cut] == 0. || ms < cut_ms[mode][cut])) {
+          cut_ms[mode][cut] = ms;
+          cut_shape[mode][cut] = sh;
+        }
+        if (ms > 0. && ms < best) {
+          best = ms;
+          best_cut = cut;
+          best_mode = mode;
+        }
       }
-    }
+  if (best == 1e300) {  // neither first-stage shape fits any cut: one CTA of 8 warps
+    for (int cut = 0; cut < kCutCandidates; ++cut)
+      for (int mode = 0; mode < 2; ++mode) {
+        const double ms = time_plan(kChunk, cut, mode, 0, false);
+        cut_ms[mode][cut] = ms;
+        cut_shape[mode][cut] = h->d.plan.block_shape;
+        if (ms > 0. && ms < best) {
+          best = ms;
+          best_cut = cut;
+          best_mode = mode;
+        }
+      }
+  }
   for (int cut = 0; cut < kCutCandidates; ++cut) {
     h->stats.sweep_cut_ms[cut] = cut_ms[0][cut];
     h->stats.sweep_cut_level_ms[cut] = cut_ms[1][cut];
