@@ -364,7 +364,7 @@ def e2e_steps(sim, steps, barrier, dist, world, start):
 # count them, so they cannot be measured inside this run), with the
 # schedule the autotuner picks for this scene; None for other workloads.
 # Keyed by FP32 (True) / FP64 (False).
-SOLVE_TRAFFIC_500 = {True: 430255616, False: 832374272}
+SOLVE_TRAFFIC_500 = {True: 439347456, False: 838375424}
 
 
 def roofline(sim, fp32, n=None):
