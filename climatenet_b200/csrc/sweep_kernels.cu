@@ -6,35 +6,42 @@
 // W_s = [D^-1 ; L_R D^-1] (see factor.hpp) in 32-lane tiles:
 //   forward : y_s = D^-1 b_s ; b_R -= (L_R D^-1) b_s
 //   backward: x_s = W_s^T [y_s ; -x_R]
-// One solve is five launches (factor.hpp, SweepPlan):
+// One solve, in launch order (factor.hpp, SweepPlan):
 //  1. k_block_forward — the lower levels of the elimination tree, cut into
-//     subtrees with contiguous columns ("blocks"), one CTA per block: the
-//     block's slice of b and its rows outside the block ("ext" rows, the row
-//     set of the block's root) sit in shared memory, the block's levels are
-//     separated by CTA barriers, each tile of each supernode (each span of
-//     kBlockSpanF columns / kBlockSpanB rows of a longer tile, the spans
-//     meeting in atomics) is one warp's item, and the factor streams in through bulk asynchronous copies
-//     (cp.async.bulk, global -> shared, completion on an mbarrier) into a ring
-//     of stages per warp, kept several slabs ahead of the warp's arithmetic
-//     (across level barriers too: the factor does not depend on the data).
-//     The ext rows' updates are added to b with one atomic each per block.
-//  2. k_upper_forward — the supernodes above the blocks, split into 32-row
-//     tiles x column chunks, taken by warps from a queue in elimination-tree
-//     order; a warp waits (bounded spin) only until every work item of the
-//     supernode's upper children is counted (the blocks finished in launch 1);
-//     each item counts itself without reading the counter back.  Partial sums
-//     land in y / b_R with atomics.
-//  3. k_upper_backward — the same supernodes top-down in 32-column tiles x row
-//     chunks; an item waits until its parent is complete; sums land in x.
+//     subtrees with contiguous columns ("blocks"), one CTA per block at a
+//     time: the block's slice of b and its rows outside the block ("ext"
+//     rows, the row set of the block's root) sit in shared memory, the
+//     block's levels are separated by a barrier among the consumer warps,
+//     each tile of each supernode (each span of kBlockSpanF columns /
+//     kBlockSpanB rows of a longer tile, the spans meeting in atomics) is one
+//     consumer warp's item, and a producer warp streams the factor through
+//     bulk asynchronous copies (cp.async.bulk, global -> shared, completion
+//     on an mbarrier) into a ring of slots shared by the CTA, ahead of the
+//     consumers and across their level barriers (the factor does not depend
+//     on the data).  The ext rows' updates are added to b with one atomic
+//     each per block.
+//  2. the supernodes above the blocks, forward, split into 32-row tiles x
+//     column chunks: either k_upper_level_forward, one launch per
+//     elimination-tree level (items spread over all warps, the launch
+//     boundary ordering the levels), or k_upper_forward, one launch whose
+//     warps take items from a queue in elimination-tree order and wait
+//     (bounded spin) until every work item of the supernode's upper children
+//     is counted (each item counts itself without reading the counter back).
+//     Partial sums land in y / b_R with atomics.
+//  3. the same supernodes backward, top-down, in 32-column tiles x row
+//     chunks (k_upper_level_backward per level, or k_upper_backward with an
+//     item waiting until its parent is complete); sums land in x.
 //  4. k_block_backward — the blocks top-down: their y slice and the final x
 //     of their ext rows are loaded into shared memory, the factor and, per
 //     slab, the row-index list of the tile stream in as in launch 1, and x of
 //     the block's columns is written back into v and q^k directly.
 //  5. k_solve_post — the write-back of the upper supernodes' columns.
-// Completion counters are cumulative over solves: supernode s has finished
-// solve number e when its counter reaches e * (its work items).  Every wait
-// (counter or mbarrier) gives up after SweepSync::max_spins polls, sets the
-// error flag and returns instead of hanging.
+// The launches after the first are programmatic dependents of the one before
+// them (griddepcontrol).  Completion counters are cumulative over solves:
+// supernode s has finished solve number e when its counter reaches e * (its
+// work items).  Every wait (counter or mbarrier) gives up after
+// SweepSync::max_spins polls, sets the error flag and returns instead of
+// hanging.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -100,8 +107,6 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 __device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-// orders this thread's (and, after __syncwarp, the warp's) generic-proxy
-// reads of a stage before the bulk copy that overwrites it
 // Programmatic dependent launch: a kernel launched with the programmatic
 // stream serialization attribute may start while the kernel before it in the
 // stream still runs; griddep_wait() returns once that kernel has completed
@@ -112,6 +117,8 @@ __device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wa
 __device__ __forceinline__ void griddep_launch_dependents() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
+// orders generic-proxy accesses of shared memory before the bulk copies that
+// follow (a slot's earlier reads before the copy that overwrites it)
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
