@@ -83,7 +83,7 @@ __global__ void k_bend_proj(DModel m, const double* __restrict__ qk, double* __r
 // w (x0 - q_i) — the same quantity without the A^T A product, each term a
 // small force instead of a difference of large ones; f = r + M v.
 template <typename T>
-__global__ void k_vertex_rhs(DModel m, const double* __restrict__ qk, const double* __restrict__ v,
+__global__ void __launch_bounds__(256, 4) k_vertex_rhs(DModel m, const double* __restrict__ qk, const double* __restrict__ v,
                              const double* __restrict__ cstep, const double* __restrict__ bp,
                              double air_damping, const int* __restrict__ slot_of,
                              double* __restrict__ fslot, T* __restrict__ b, double dt, int residual_mode) {
