@@ -55,9 +55,6 @@ __global__ void k_bend_proj(DModel m, const double* __restrict__ qk, double* __r
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= m.B) return;
   double3 lb = make_double3(0., 0., 0.);
-  // unrolled so that the stencil's gathers are in flight together (the sum
-  // keeps its order)
-#pragma unroll 4
   for (int k = m.bend_ptr[b]; k < m.bend_ptr[b + 1]; ++k) lb = lb + m.bend_coef[k] * ld3(qk, m.bend_idx[k]);
   const double n = sqrt(dot3(lb, lb));
   const double w = m.bend_w[b];
@@ -98,7 +95,6 @@ __global__ void __launch_bounds__(256, 4) k_vertex_rhs(DModel m, const double* _
   const int bo = m.bend_of[i];
   if (bo >= 0) acc = acc + m.self_bend[i] * ld3(bp, bo);
   const double ks = residual_mode ? m.spring_k[i] : 0.;
-#pragma unroll 2
   for (int s = m.ring_ptr[i]; s < m.ring_ptr[i + 1]; ++s) {
     const int j = m.ring_idx[s];
     const double3 d = qi - ld3(qk, j);
