@@ -154,7 +154,6 @@ void build_schedule(pdf_handle* h, int chunk, int cut_level, int upper_mode = 0,
     sy.queue = dalloc<int>(4);
     sy.epoch = dalloc<unsigned long long>(1);
     sy.fdone = dalloc<unsigned long long>(f.n_sn);
-    sy.fchild = dalloc<unsigned long long>(f.n_sn);
     sy.bdone = dalloc<unsigned long long>(f.n_sn);
     sy.err = dalloc<int>(1);
     sy.max_spins = kMaxSpins;
@@ -163,7 +162,6 @@ void build_schedule(pdf_handle* h, int chunk, int cut_level, int upper_mode = 0,
   const unsigned long long one = 1ULL;
   CK(cudaMemcpy(sy.epoch, &one, sizeof(one), cudaMemcpyHostToDevice));
   CK(cudaMemset(sy.fdone, 0, f.n_sn * sizeof(unsigned long long)));
-  CK(cudaMemset(sy.fchild, 0, f.n_sn * sizeof(unsigned long long)));
   CK(cudaMemset(sy.bdone, 0, f.n_sn * sizeof(unsigned long long)));
   CK(cudaMemset(sy.err, 0, sizeof(int)));
   sy.trace = DTrace{h->d.iter, h->d.stamps, std::max(1, h->prm.local_global_iterations)};
@@ -1027,7 +1025,7 @@ void free_handle(pdf_handle* h) {
                   d.bend_idx, d.bend_coef, d.bend_w, d.bend_rest, d.pin_term, d.ata_ptr, d.ata_col, d.ata_val,
                   d.perm, d.iperm, d.vmat, d.friction, d.tris, d.obstacles, d.vmesh, d.q, d.v, d.tn, d.qk,
                   d.cstep, d.bp, d.sn, d.rows, d.Wf64, d.Wb64, d.Wf32, d.Wb32, d.sync.queue, d.sync.epoch,
-                  d.sync.fdone, d.sync.fchild, d.sync.bdone, d.sync.err, d.b64, d.y64, d.x64, d.b32, d.y32,
+                  d.sync.fdone, d.sync.bdone, d.sync.err, d.b64, d.y64, d.x64, d.b32, d.y32,
                   d.x32, d.flags, d.sel_idx, d.cub_tmp, d.newf, d.ac_hist, d.c.n_contacts, d.c.c_vertex,
                   d.c.c_normal, d.c.c_speed, d.c.c_mu, d.c.c_basis, d.c.c_force, d.c.c_ac, d.c.c_slot, d.c.n_self,
                   d.c.s_vertex, d.c.s_partner, d.c.s_face, d.c.s_normal, d.c.s_mu, d.c.s_basis, d.c.s_force,

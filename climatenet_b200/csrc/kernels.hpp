@@ -14,7 +14,6 @@ struct SweepSync {
   int* queue;
   unsigned long long* epoch;
   unsigned long long* fdone;   // per supernode: forward work items finished
-  unsigned long long* fchild;  // per supernode: children whose forward finished
   unsigned long long* bdone;   // per supernode: backward work items finished
   int* err;                    // set when a dependency wait gives up
   int max_spins;               // polls of a dependency counter before giving up
